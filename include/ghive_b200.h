@@ -1,0 +1,318 @@
+/*
+ * ghive_b200.h — C ABI of the B200 (sm_100a) relational-operator library.
+ *
+ * This is the drop-in boundary for the path GHive offloads from Hive's
+ * Filter / GroupBy / MapJoin / ReduceSink operators: filter, hash group-by
+ * aggregation, hash equi-join (build + probe) and ORDER BY sort over Hive
+ * columnar batches.  Every entry point takes plain pointers and sizes; no
+ * C++ or torch type crosses it.  The C++ adapters that keep GHive's operator
+ * classes (`FilterPredicate::process`, `GroupByPredicate::gpu_execute`,
+ * `BaseJoinPredicate::process`, the Sink sort) sit on top of this header in
+ * ghive_b200/csrc/host/ghive_ops.hpp, and the JNI shim that keeps
+ * `JNIInterface.GPUProcess` sits on top of those.
+ *
+ * Reference interfaces replaced (paths inside the GHive project):
+ *   gpu_impl/inc/DataFlow/Column.hpp:5-35       ColumnType, Column
+ *   gpu_impl/inc/DataFlow/Table.hpp:29-52        in-band NULL sentinels
+ *   gpu_impl/inc/Operator/FilterPredicate.hpp:17-58   PredicateMode
+ *   gpu_impl/src/Operator/FilterPredicate.cu:434-571  FilterPredicate::process
+ *   gpu_impl/src/Operator/FilterOperator.cu:36-93     FilterOperator::clean_data
+ *   gpu_impl/inc/Operator/AggregationDesc.hpp:6-37    AggregationType / AggregationDesc
+ *   gpu_impl/src/Operator/GroupByPredicate.cu:19-359  GroupByPredicate::gpu_execute
+ *   gpu_impl/inc/Operator/BaseJoinPredicate.hpp:11-25 BaseJoinType
+ *   gpu_impl/src/Operator/SortMergeJoinPredicate.cu:8-461  join process
+ *   gpu_impl/src/Operator/BaseJoinPredicate.cu:4-97   generate_result (payload gather)
+ *   gpu_impl/src/Operator/SinkOperator.cu:98-306      Sink ORDER BY sort
+ *
+ * Conventions
+ *   - Every function returns GHB_OK (0) or a GHB_ERR_* code; the message of
+ *     the last failure on a context is ghb_last_error(ctx).
+ *   - Device entry points are asynchronous on the given stream (a
+ *     cudaStream_t passed as void*; NULL = legacy default stream).  Row counts
+ *     produced on the device are written to a caller-provided DEVICE int64.
+ *     ghb_sync() waits for the stream and reports any device-side error
+ *     (look-back timeout, output capacity exceeded) raised since the last sync.
+ *   - Entry points suffixed _host take HOST buffers, copy them to the device,
+ *     run the operator and copy the result back before returning.
+ *   - Row counts are int64 (the reference used uint32, Column.hpp:18).
+ */
+#ifndef GHIVE_B200_H
+#define GHIVE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GHB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define GHB_OK               0
+#define GHB_ERR_INVALID      1   /* bad argument or descriptor; nothing launched */
+#define GHB_ERR_OOM          2   /* device scratch could not be allocated        */
+#define GHB_ERR_CUDA         3   /* a CUDA runtime call failed                   */
+#define GHB_ERR_TIMEOUT      4   /* a bounded device-side wait gave up           */
+#define GHB_ERR_CAPACITY     5   /* output buffer too small; required rows known */
+#define GHB_ERR_UNSUPPORTED  6   /* valid request outside what the kernels do    */
+
+/* ---- column types: same values as GHive's ColumnType (Column.hpp:5-11) -- */
+#define GHB_LONG    0   /* int64  (Hive LongColumnVector.vector)   */
+#define GHB_DOUBLE  1   /* double (Hive DoubleColumnVector.vector) */
+#define GHB_INT     2   /* int32  (GHive INT column)               */
+#define GHB_STRING  3   /* UTF-8 blob + int32 [start,end) pairs in aux; oracle only */
+
+/* ---- NULL conventions ---------------------------------------------------- */
+#define GHB_NULLS_NONE      0  /* Hive noNulls == true                                   */
+#define GHB_NULLS_SENTINEL  1  /* GHive in-band: INT64_MAX / NaN / INT32_MAX (Table.hpp:29-52) */
+#define GHB_NULLS_BYTEMAP   2  /* Hive ColumnVector.isNull[]: one byte per row, nonzero = NULL */
+
+/* ---- predicate modes: same values as GHive's PredicateMode
+ *      (FilterPredicate.hpp:17-58); semantics of the leaves follow Hive's
+ *      FilterColumnCompareScalar / FilterColumnBetween templates: a NULL
+ *      operand never passes. ------------------------------------------------ */
+#define GHB_FILTER_EQ            0   /* x == a            */
+#define GHB_FILTER_LE            1   /* x <= a            */
+#define GHB_FILTER_GE            2   /* x >= a            */
+#define GHB_FILTER_LT            3   /* x <  a            */
+#define GHB_FILTER_GT            4   /* x >  a            */
+#define GHB_FILTER_RANGE         5   /* a <  x <  b       */
+#define GHB_FILTER_EQ_RANGE      6   /* a <= x <= b (BETWEEN) */
+#define GHB_FILTER_NOT_EQ        7   /* x != a            */
+#define GHB_FILTER_NOT_RANGE     8   /* x < a || x > b (NOT BETWEEN) */
+#define GHB_FILTER_NOT_EQ_RANGE  9   /* x <= a || x >= b  */
+#define GHB_FILTER_NOT_NULL     10   /* x IS NOT NULL     */
+#define GHB_FILTER_AND          11
+#define GHB_FILTER_OR           12
+
+/* ---- aggregation types: same values as GHive's AggregationType
+ *      (AggregationDesc.hpp:6-25).  Result types follow Hive's UDAFs:
+ *      SUM(int/long) -> int64 with silent wrap; SUM(double) -> double;
+ *      AVG -> double (sum kept in double, VectorUDAFAvg.txt:56-71);
+ *      MIN/MAX -> input type; CNT -> int64 (COUNT(*) when col < 0). ------- */
+#define GHB_AGG_SUM  0
+#define GHB_AGG_MAX  1
+#define GHB_AGG_MIN  2
+#define GHB_AGG_AVG  3
+#define GHB_AGG_CNT  4
+
+/* ---- join types: same values as GHive's BaseJoinType (BaseJoinPredicate.hpp:11-25) */
+#define GHB_INNER_JOIN       0
+#define GHB_LEFT_OUTER_JOIN  1   /* probe side is the left (preserved) side */
+#define GHB_LEFT_SEMI_JOIN   4
+
+/* ---- sort orders (SinkOperator "sort order: +-"; null order 'a'/'z') ---- */
+#define GHB_ASC   0
+#define GHB_DESC  1
+#define GHB_NULLS_DEFAULT 0  /* Hive default: ASC -> NULLS FIRST, DESC -> NULLS LAST */
+#define GHB_NULLS_FIRST   1
+#define GHB_NULLS_LAST    2
+
+/* An input column.  `data` holds n values of `type`.  For GHB_STRING, `data`
+ * is the char blob and `aux` the int32 [start,end) pair array (GHive's
+ * Column::data_ptr_aux); -1,-1 is NULL. */
+typedef struct ghb_column {
+  int32_t type;
+  int32_t null_mode;
+  const void* data;
+  const uint8_t* is_null;   /* used when null_mode == GHB_NULLS_BYTEMAP */
+  const void* aux;          /* GHB_STRING only */
+  int64_t n;
+} ghb_column;
+
+/* An output column with room for the capacity the call states.  `is_null`
+ * may be NULL when the caller knows no output value can be NULL; an
+ * aggregate that can be NULL (SUM/AVG/MIN/MAX over an all-NULL group)
+ * then writes the GHive sentinel of its type instead. */
+typedef struct ghb_out_column {
+  int32_t type;
+  int32_t reserved;
+  void* data;
+  uint8_t* is_null;
+} ghb_out_column;
+
+/* One node of a predicate tree (GHive FilterPredicate, FilterPredicate.hpp:60-117).
+ * Leaves compare column `col` with the literals, or with column `col2` when
+ * col2 >= 0 (column-vs-column; only the binary compare modes).  A literal is
+ * read as double when lit_is_double != 0, else as int64; the comparison runs
+ * in double when either side is double (Java binary numeric promotion), else
+ * in int64.  AND/OR nodes name two children by node index. */
+typedef struct ghb_pred_node {
+  int32_t mode;
+  int32_t col;
+  int32_t col2;
+  int32_t lit_is_double;
+  int32_t child[2];
+  int64_t lit_i[2];
+  double lit_d[2];
+} ghb_pred_node;
+
+typedef struct ghb_predicate {
+  int32_t n_nodes;   /* <= GHB_MAX_PRED_NODES */
+  int32_t root;
+  const ghb_pred_node* nodes;
+} ghb_predicate;
+#define GHB_MAX_PRED_NODES 32
+
+/* GHive AggregationDesc{type, index}; col < 0 with GHB_AGG_CNT is COUNT(*). */
+typedef struct ghb_agg_desc {
+  int32_t type;
+  int32_t col;
+} ghb_agg_desc;
+
+/* Tuning knobs (zero = library default / autotuned choice). */
+typedef struct ghb_groupby_cfg {
+  int32_t block_threads;      /* threads per CTA                              */
+  int32_t smem_slots;         /* shared-memory pre-aggregation slots per CTA;
+                                 -1 disables the shared stage                 */
+  int32_t global_slots_log2;  /* log2 of the global table size (0 = from max_groups) */
+  int32_t ctas_per_sm;        /* persistent CTAs per SM                       */
+  int64_t max_groups;         /* capacity hint = output capacity              */
+} ghb_groupby_cfg;
+
+typedef struct ghb_join_cfg {
+  float load_factor;          /* build table fill, default 0.5               */
+  int32_t l2_persist;         /* 1: pin the table in L2 with an access-policy window */
+  int32_t block_threads;
+} ghb_join_cfg;
+
+typedef struct ghb_sort_cfg {
+  int32_t digit_bits;         /* radix digit width (8..12), 0 = default      */
+  int32_t block_threads;
+  int32_t items_per_thread;
+} ghb_sort_cfg;
+
+typedef struct ghb_ctx ghb_ctx;
+typedef struct ghb_join_table ghb_join_table;
+
+/* ---- context ---------------------------------------------------------- */
+/* Creates a context on `device`.  The context owns a growable device scratch
+ * arena (hash tables, look-back state); `arena_bytes` pre-reserves it
+ * (0 = grow on demand).  Replaces the process-global state GHive keeps in
+ * Parser.cu:16-20; contexts are independent and may be used from different
+ * host threads (one thread per context at a time). */
+int32_t ghb_ctx_create(int32_t device, int64_t arena_bytes, ghb_ctx** out);
+int32_t ghb_ctx_destroy(ghb_ctx* ctx);
+const char* ghb_last_error(const ghb_ctx* ctx);
+int32_t ghb_abi_version(void);
+/* Waits for `stream` and returns the first device-side error recorded on the
+ * context since the previous ghb_sync (GHB_OK if none), then clears it. */
+int32_t ghb_sync(ghb_ctx* ctx, void* stream);
+/* Number of kernels the context launched since creation. */
+int64_t ghb_kernel_launches(const ghb_ctx* ctx);
+
+/* ---- filter (F1) -------------------------------------------------------
+ * Replaces FilterPredicate::process (FilterPredicate.cu:434-571) followed by
+ * FilterOperator::clean_data (FilterOperator.cu:36-93): evaluates the
+ * predicate tree on `cols` and writes the selected rows of the columns listed
+ * in `proj` (indices into cols) to `out[0..nproj)`, in input order.  The
+ * inputs are not modified (the reference compacted them in place).
+ * d_out_rows (device int64) receives the number of selected rows.  Rows
+ * beyond out_capacity are counted but not written; ghb_sync then returns
+ * GHB_ERR_CAPACITY. */
+int32_t ghb_filter(ghb_ctx* ctx, const ghb_predicate* pred,
+                   const ghb_column* cols, int32_t ncols,
+                   const int32_t* proj, int32_t nproj,
+                   ghb_out_column* out, int64_t out_capacity,
+                   int64_t* d_out_rows, void* stream);
+
+/* ---- fused filter + hash group-by (G1/G2) -----------------------------
+ * Replaces GroupByPredicate::gpu_execute (GroupByPredicate.cu:19-359) fed by
+ * the filter above; the predicate (nullable) is evaluated inside the
+ * aggregation kernel so no filtered table is materialised.  Output columns:
+ * out[0..nkeys) = group keys, out[nkeys..nkeys+naggs) = aggregates, one row
+ * per group in unspecified order (Hive's HashMap order is unspecified too).
+ * With nkeys == 0 the result is one row (Hive's global aggregate, also on an
+ * empty input).  d_out_groups (device int64) receives the group count. */
+int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred,
+                           const ghb_column* cols, int32_t ncols,
+                           const int32_t* key_cols, int32_t nkeys,
+                           const ghb_agg_desc* aggs, int32_t naggs,
+                           ghb_out_column* out, int64_t out_capacity,
+                           int64_t* d_out_groups,
+                           const ghb_groupby_cfg* cfg, void* stream);
+
+/* ---- hash join (J1 build, J2 probe) ------------------------------------
+ * Replaces the sort + CPU merge of SortMergeJoinPredicate::process
+ * (SortMergeJoinPredicate.cu:8-461) and the host gather of
+ * BaseJoinPredicate::generate_result (BaseJoinPredicate.cu:4-97) with a
+ * device hash join on one LONG or INT key.  The table keeps build row ids;
+ * it stays resident on the device until ghb_join_table_free, so one build
+ * serves many probes (a broadcast map-join small table).  NULL build keys
+ * are not inserted; NULL probe keys never match. */
+int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key,
+                       const ghb_join_cfg* cfg, ghb_join_table** out,
+                       void* stream);
+int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table);
+/* Rows stored and the largest number of build rows sharing one key
+ * (valid after ghb_sync of the build stream). */
+int32_t ghb_join_table_info(ghb_ctx* ctx, const ghb_join_table* table,
+                            int64_t* rows, int64_t* max_dup, int64_t* slots);
+
+/* Probes `probe_key` against `table` (join_type GHB_INNER_JOIN,
+ * GHB_LEFT_SEMI_JOIN or GHB_LEFT_OUTER_JOIN).  Each output row is one
+ * (probe row, build row) pair, in probe-row order.  Written per output row,
+ * each optional (NULL to skip):
+ *   out_probe_rowid[i]  probe row index (int32)
+ *   out_build_rowid[i]  build row index (int32; -1 for an outer-join miss)
+ *   out_build[j]        build_payload[j] gathered at the build row
+ *                       (NULL in is_null / sentinel for an outer miss)
+ *   out_probe[j]        probe_payload[j] gathered at the probe row
+ * d_out_rows (device int64) receives the number of output rows. */
+int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table,
+                       const ghb_column* probe_key, int32_t join_type,
+                       const ghb_column* build_payload, int32_t n_build_payload,
+                       ghb_out_column* out_build,
+                       const ghb_column* probe_payload, int32_t n_probe_payload,
+                       ghb_out_column* out_probe,
+                       int32_t* out_probe_rowid, int32_t* out_build_rowid,
+                       int64_t out_capacity, int64_t* d_out_rows, void* stream);
+
+/* ---- ORDER BY sort (S1) -------------------------------------------------
+ * Replaces the Sink sort (SinkOperator.cu:153-286): a stable sort of n rows
+ * by the key columns in Hive's BinarySortable order (BinarySortableSerDe.java:
+ * 921-960: signed integers and IEEE doubles in numeric order, per-key ASC/DESC
+ * and NULLS FIRST/LAST).  Writes the sorted key columns to out_keys and the
+ * payload columns, permuted the same way, to out_payload; out_rowid (nullable,
+ * int32) receives the permutation.  Ties keep input order. */
+int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
+                 const int32_t* null_orders, int32_t nkeys,
+                 const ghb_column* payload, int32_t npayload,
+                 ghb_out_column* out_keys, ghb_out_column* out_payload,
+                 int32_t* out_rowid, const ghb_sort_cfg* cfg, void* stream);
+
+/* ---- host-buffer entry points (end-to-end) -------------------------------
+ * Same operators with every column in HOST memory (pageable or pinned).
+ * These copy the inputs in, run the operator, copy the result out and
+ * synchronise, like one GHive operator call on host `Column`s.  The row
+ * count is returned through the host int64 *out_rows. */
+int32_t ghb_filter_host(ghb_ctx* ctx, const ghb_predicate* pred,
+                        const ghb_column* cols, int32_t ncols,
+                        const int32_t* proj, int32_t nproj,
+                        ghb_out_column* out, int64_t out_capacity,
+                        int64_t* out_rows);
+int32_t ghb_filter_groupby_host(ghb_ctx* ctx, const ghb_predicate* pred,
+                                const ghb_column* cols, int32_t ncols,
+                                const int32_t* key_cols, int32_t nkeys,
+                                const ghb_agg_desc* aggs, int32_t naggs,
+                                ghb_out_column* out, int64_t out_capacity,
+                                int64_t* out_groups, const ghb_groupby_cfg* cfg);
+int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key,
+                           const ghb_column* probe_key, int32_t join_type,
+                           const ghb_column* build_payload, int32_t n_build_payload,
+                           ghb_out_column* out_build,
+                           const ghb_column* probe_payload, int32_t n_probe_payload,
+                           ghb_out_column* out_probe,
+                           int32_t* out_probe_rowid, int32_t* out_build_rowid,
+                           int64_t out_capacity, int64_t* out_rows,
+                           const ghb_join_cfg* cfg);
+int32_t ghb_sort_host(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
+                      const int32_t* null_orders, int32_t nkeys,
+                      const ghb_column* payload, int32_t npayload,
+                      ghb_out_column* out_keys, ghb_out_column* out_payload,
+                      int32_t* out_rowid, const ghb_sort_cfg* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GHIVE_B200_H */
