@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: GHive's offloaded relational operators on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (one GPU's worth, weak-scaled over N ranks): the inner hash
+equi-join of a 1.5M-row build side (unique int64 keys, int64 + double
+payloads) with a 60M-row probe side (int64 foreign key, 5% misses, int32
+payload), emitting every (probe row id, build int64 payload, build double
+payload) match.  One step = build the table + probe all 60M rows.  The fused
+filter + group-by (6M-row fact table) and the 60M-row (d, k) sort are timed
+too and reported under "ops".
+
+Timing: CUDA events on the launching stream, W untimed warm-up steps, then K
+timed steps between a barrier + device synchronise on both sides; the
+reported time is the max over ranks.  The join's probe key column (480 MB)
+and the sort's columns are larger than the 126 MB L2; the group-by step flushes
+L2 (a 256 MB write) before each timed launch.  Inputs are seeded PCG64
+synthetic data of the workload shapes.
+
+`--impl reference` times the CPU restatement of Hive's vectorized map-join
+(the oracle port: HashCodeUtil hash, triangular probing, load factor 0.75)
+on all host threads over a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BUILD = 1_500_000
+N_PROBE = 60_000_000
+N_FACT = 6_000_000
+N_SORT = 60_000_000
+METRIC = "GPU rows/s (inner hash join: probe rows per second, build + probe per step)"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded in a committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_init(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v, device):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- CPU arm
+def cpu_join_sample(threads, probe_rows, seed_idx=1):
+    """Oracle port of Hive's map-join on a sample: full build, probe_rows rows."""
+    from ghive_b200 import workloads
+    from oracle import oracle
+    (bkey, bpay), (fk, _) = workloads.join_tables(N_BUILD, probe_rows, seed_idx=seed_idx)
+    t0 = time.perf_counter()
+    prow, outs = oracle.hash_join_mt(threads, bkey, fk, bpay)
+    dt = time.perf_counter() - t0
+    return probe_rows / dt, dt, len(prow)
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sample = 6_000_000
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, dt, rows = cpu_join_sample(threads, sample)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sample / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded PCG64)",
+            "config": {"workload": "inner hash join, build 1.5M unique int64 keys + int64/double "
+                                   "payloads, probe 60M int64 keys (5% miss)",
+                       "build_rows": N_BUILD, "probe_rows": N_PROBE,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                             "sample": "build 1.5M rows + probe %d of the 60M probe rows per step "
+                                       "(Hive VectorMapJoinFastLongHashTable restated, C++)" % sample},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU arm
+def run_ours(args, world, rank, local):
+    import torch
+
+    from ghive_b200 import abi, workloads
+    from ghive_b200.ops import Context
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = Context(local)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = load_peaks()
+
+    # ---------------- headline: hash join, data resident in HBM
+    (bkey, bpay), (fk, ppay) = workloads.join_tables(N_BUILD, N_PROBE, seed_idx=1 + 17 * rank)
+    d_bkey = torch.from_numpy(bkey).to(dev)
+    d_bpay = [torch.from_numpy(c).to(dev) for c in bpay]
+    d_fk = torch.from_numpy(fk).to(dev)
+    cap = N_PROBE
+    outs = None
+
+    def join_step(ev=None):
+        nonlocal outs
+        t = ctx.join_build(d_bkey)
+        if ev:
+            ev[0].record(stream)
+        outs = ctx.join_probe(t, d_fk, abi.INNER_JOIN, build_payload=d_bpay, capacity=cap,
+                              rowids=False, sync=False, outs=outs)
+        if ev:
+            ev[1].record(stream)
+        t.free()
+        return outs
+
+    # probe output: probe row id (int32) is written through the rowid slot
+    from ghive_b200.ops import _Outs
+    ob = _Outs([abi.LONG, abi.DOUBLE], cap, dev, with_nulls=False)
+    op = _Outs([], cap, dev)
+    prow = torch.empty(cap, dtype=torch.int32, device=dev)
+    d_rows = torch.zeros(1, dtype=torch.int64, device=dev)
+    outs = (ob, op, prow, None, d_rows)
+
+    for _ in range(args.warmup):
+        join_step()
+    ctx.sync()
+    rows_out = int(d_rows.item())
+    probe_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = ctx.launches
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for i in range(args.steps):
+            join_step(probe_ev[i])
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = ctx.launches - l0
+    ctx.sync()
+    step_ms = start.elapsed_time(end) / args.steps
+    step_ms = max_over_ranks(world, step_ms, dev)
+    probe_ms = statistics.mean(a.elapsed_time(b) for a, b in probe_ev)
+    value = world * N_PROBE / (step_ms / 1e3)
+    probe_bytes = N_PROBE * 8 + rows_out * 20 + N_BUILD * 16
+    achieved = probe_bytes / (probe_ms / 1e3) / 1e9
+
+    # ---------------- e2e: host buffers through the C ABI entry point
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    h_bkey, h_bpay, h_fk = pin(bkey), [pin(c) for c in bpay], pin(fk)
+    from ghive_b200.ops import _Outs as HOuts
+    hob = HOuts([abi.LONG, abi.DOUBLE], cap, None, with_nulls=False)
+    hprow = torch.empty(cap, dtype=torch.int32).pin_memory().numpy()
+    hob_pinned = []  # pinned output columns: the D2H copies run at DMA speed
+    for j, t in enumerate((abi.LONG, abi.DOUBLE)):
+        buf = torch.empty(cap, dtype=torch.int64 if t == abi.LONG else torch.float64).pin_memory()
+        hob.cols[j] = (buf.numpy(), None)
+        hob.arr[j].data = buf.data_ptr()
+        hob_pinned.append(buf)
+    hop = HOuts([], cap, None)
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(1):
+        ctx.hash_join_host(h_bkey, h_fk, abi.INNER_JOIN, build_payload=h_bpay, capacity=cap,
+                           outs=(hob, hop, hprow, None))
+    dstream = torch.cuda.default_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(dstream)
+    for _ in range(e2e_steps):
+        r = ctx.hash_join_host(h_bkey, h_fk, abi.INNER_JOIN, build_payload=h_bpay, capacity=cap,
+                               outs=(hob, hop, hprow, None))
+    e1.record(dstream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / e2e_steps, dev)
+    assert r["rows"] == rows_out
+    e2e = {"value": world * N_PROBE / (e2e_ms / 1e3), "unit": "rows/s",
+           "h2d_bytes_per_step": int(bkey.nbytes + sum(c.nbytes for c in bpay) + fk.nbytes),
+           "d2h_bytes_per_step": int(rows_out * 20 + 8), "ms_per_step": e2e_ms,
+           "api": "ghb_hash_join_host (pinned host columns)"}
+    del d_fk, outs, ob, prow
+    torch.cuda.empty_cache()
+
+    ops = {}
+    if not args.headline_only:
+        ops["filter_groupby"] = bench_groupby(ctx, args, dev, stream, peak)
+        ops["sort"] = bench_sort(ctx, args, dev, stream, peak)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt, _ = cpu_join_sample(threads, 12_000_000)
+        cpu = {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": "build 1.5M rows + probe 12M of the 60M probe rows "
+                         "(Hive VectorMapJoinFastLongHashTable restated, C++), %.1f s" % dt}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded PCG64)",
+                "config": {"workload": "inner hash join, build 1.5M unique int64 keys + int64/double "
+                                       "payloads, probe 60M int64 keys (5% miss), output (probe row, "
+                                       "int64 payload, double payload) per match",
+                           "build_rows": N_BUILD, "probe_rows": N_PROBE, "output_rows": rows_out,
+                           "parallelism": "dp%d (replicated build, sharded probe, no collective)" % world,
+                           "l2": "inputs larger than L2 (probe key column 480 MB)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "kernel": "join_probe_kernel",
+                             "bytes_per_launch": probe_bytes, "ms_per_launch": probe_ms,
+                             "traffic": profile_traffic("join_probe_60M.md")},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary(), "ops": ops}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def flush_l2(buf):
+    buf.add_(1)
+
+
+def bench_groupby(ctx, args, dev, stream, peak):
+    import torch
+
+    from ghive_b200 import workloads
+    cols = workloads.fact_table(N_FACT, seed_idx=0)
+    dcols = [torch.from_numpy(c).to(dev) for c in cols]
+    pred = workloads.fact_predicate()
+    flush = torch.zeros(64 << 20, dtype=torch.float32, device=dev)  # 256 MB
+    res = None
+    for _ in range(args.warmup):
+        res = ctx.filter_groupby(pred, dcols, [0], workloads.AGGS_FACT, capacity=1000,
+                                 max_groups=1000, sync=False)
+    ctx.sync()
+    times = []
+    for _ in range(max(args.steps, 10)):
+        flush_l2(flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        res = ctx.filter_groupby(pred, dcols, [0], workloads.AGGS_FACT, capacity=1000,
+                                 max_groups=1000, sync=False)
+        b.record(stream)
+        times.append((a, b))
+    ctx.sync()
+    groups = int(res[1].item())
+    ms = statistics.median(x.elapsed_time(y) for x, y in times)
+    nbytes = N_FACT * 24 + groups * 48
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"workload": "filter d<1263 + GROUP BY k (1000 groups): COUNT(*), SUM(qty), SUM(price), "
+                        "AVG(price), MIN(d), MAX(d) over 6M rows",
+            "rows_per_s": N_FACT / (ms / 1e3), "ms": ms, "groups": groups,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "bytes": nbytes, "l2": "flushed before each launch"}}
+
+
+def bench_sort(ctx, args, dev, stream, peak):
+    import torch
+
+    from ghive_b200 import workloads
+    out = {}
+    for zipf in (False, True):
+        d, k, rowid = workloads.sort_table(N_SORT, zipf=zipf, seed_idx=2)
+        dd, dk, dr = (torch.from_numpy(x).to(dev) for x in (d, k, rowid))
+        for _ in range(max(1, args.warmup)):
+            ctx.sort([dd, dk], payload=[dr], sync=False)
+        ctx.sync()
+        times = []
+        for _ in range(max(3, min(args.steps, 10))):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.sort([dd, dk], payload=[dr], sync=False)
+            b.record(stream)
+            times.append((a, b))
+        ctx.sync()
+        ms = statistics.median(x.elapsed_time(y) for x, y in times)
+        nbytes = N_SORT * 32
+        ach = nbytes / (ms / 1e3) / 1e9
+        out["zipf" if zipf else "uniform"] = {
+            "rows_per_s": N_SORT / (ms / 1e3), "ms": ms,
+            "roofline_lower_bound_32B_per_row": {"achieved": ach, "peak": peak, "frac": ach / peak}}
+        del dd, dk, dr
+        torch.cuda.empty_cache()
+    out["workload"] = "ORDER BY (d int32, k int64) ASC, stable, int32 row-id payload, 60M rows"
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--headline-only", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_init(args.gpus)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

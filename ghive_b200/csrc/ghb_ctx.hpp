@@ -1,0 +1,104 @@
+// ghb_ctx.hpp — the context object behind ghb_ctx* and host-side helpers.
+//
+// A context owns: a device status word that kernels raise errors into, a
+// growable device scratch arena, the look-back tile-status array (tagged
+// with a launch epoch so it is never cleared per launch), the group-by table
+// (left zeroed by the finalize kernel, so each call starts clean without a
+// memset), and the kernel-launch counter.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ghive_b200.h"
+#include "ghb_internal.cuh"
+
+struct ghb_ctx {
+  int device = 0;
+  int num_sms = 148;
+  int32_t* d_status = nullptr;            // device error word
+  std::string last_error;
+  int64_t launches = 0;
+
+  // scratch arena (bump allocated per operator call)
+  char* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  size_t scratch_used = 0;
+
+  // decoupled look-back tile status
+  uint64_t* lb_status = nullptr;
+  int64_t lb_tiles = 0;
+  uint32_t epoch = 0;
+
+  // self-resetting counters: [0] tile claim, [1] finished CTAs, ...
+  unsigned long long* d_counters = nullptr;
+
+  // group-by global table, zeroed after each finalize
+  void* gb_table = nullptr;
+  size_t gb_bytes = 0;
+  bool gb_dirty = false;
+
+  // pinned staging for the host-buffer entry points
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+};
+
+struct ghb_join_table {
+  uint64_t* keys = nullptr;   // stored key (flip_i64), 0 = empty
+  int32_t* head = nullptr;    // first build row of the key
+  int32_t* count = nullptr;   // build rows sharing the key
+  int32_t* next = nullptr;    // chain of build rows (duplicates)
+  int64_t slots = 0;          // power of two
+  int64_t build_rows = 0;
+  int32_t key_type = GHB_LONG;
+  unsigned long long* d_stats = nullptr;  // [0] rows stored, [1] max dup, [2] side-slot rows
+  int32_t side_head = -1;     // unused (INT64_MIN key lives in the side slot)
+  void* alloc = nullptr;
+  size_t alloc_bytes = 0;
+  cudaStream_t stream = 0;    // build stream; the table is released in its order
+  bool l2_window = false;
+};
+
+namespace ghb {
+
+int32_t set_error(ghb_ctx* ctx, int32_t code, const char* fmt, ...);
+
+#define GHB_CUDA_TRY(ctx, expr)                                                        \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess)                                                             \
+      return ::ghb::set_error((ctx), GHB_ERR_CUDA, "%s failed: %s", #expr,            \
+                              cudaGetErrorString(_e));                                 \
+  } while (0)
+
+#define GHB_LAUNCH_CHECK(ctx)                                                          \
+  do {                                                                                 \
+    (ctx)->launches++;                                                                 \
+    cudaError_t _e = cudaGetLastError();                                               \
+    if (_e != cudaSuccess)                                                             \
+      return ::ghb::set_error((ctx), GHB_ERR_CUDA, "kernel launch failed: %s",         \
+                              cudaGetErrorString(_e));                                 \
+  } while (0)
+
+// Reserves `bytes` (256-aligned) from the scratch arena; grows it when too
+// small (a cudaFree + cudaMalloc after syncing the device).  Resets with
+// scratch_reset at the start of an operator call.
+int32_t scratch_reset(ghb_ctx* ctx);
+int32_t scratch_alloc(ghb_ctx* ctx, size_t bytes, void** out, cudaStream_t stream);
+int32_t scratch_reserve(ghb_ctx* ctx, size_t total, cudaStream_t stream);
+
+// Look-back status array with room for `tiles` tiles, and a fresh epoch.
+int32_t lookback_prepare(ghb_ctx* ctx, int64_t tiles, uint32_t* epoch, cudaStream_t stream);
+
+int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, int64_t* n);
+int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, PredProg* prog);
+
+inline size_t type_width(int32_t t) { return t == GHB_INT ? 4 : 8; }
+
+}  // namespace ghb

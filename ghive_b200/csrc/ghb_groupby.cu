@@ -1,0 +1,606 @@
+// ghb_groupby.cu — fused filter + hash group-by aggregation (G1 + G2).
+//
+// Replaces GroupByPredicate::gpu_execute (gpu_impl/src/Operator/
+// GroupByPredicate.cu:19-359), which sorted row indices with a comparison
+// sort and then ran one H2D + reduce_by_key + D2H pass per aggregate
+// (:506-720).  Here one pass over the rows evaluates the filter predicate in
+// registers and folds every aggregate of the row into a hash table:
+//
+//   G1  persistent CTAs; each folds its rows into a shared-memory open-
+//       addressing table (keys + one 64-bit accumulator per aggregate state);
+//       rows whose key does not fit go straight to the global table; at the
+//       end the CTA merges its shared table into the global one.
+//   G2  finalize: walks the global table, emits one output row per group
+//       (COUNT, SUM, AVG = sum/count, MIN, MAX with Hive's NULL rules) and
+//       zeroes every slot it read, so the next call needs no memset.
+//
+// Semantics follow Hive's UDAFs (VectorUDAFSum.txt:59-71, VectorUDAFAvg.txt:
+// 56-71, VectorUDAFMinMax.txt:65-72): SUM over integers wraps silently, SUM
+// and AVG over doubles are double sums, an aggregate that saw only NULLs is
+// NULL, COUNT(*) counts rows, COUNT(col) counts non-NULL values.  Double sums
+// are accumulated with an error-free transformation: every atomicAdd returns
+// the old value, so the adding thread knows the exact rounding error of that
+// addition (Knuth's TwoSum) and adds it to a companion compensation word;
+// sum + compensation is then accurate to ~1 ulp whatever the order.
+#include <algorithm>
+
+#include "ghb_ctx.hpp"
+
+namespace ghb {
+
+enum AccKind : int8_t {
+  A_CNT_STAR = 0,  // rows in the group (always accumulator 0: also the "slot used" flag)
+  A_CNT_NN = 1,    // non-NULL values of a column
+  A_SUM_I = 2,     // int64 wrapping sum
+  A_SUM_F = 3,     // double sum; accumulator a+1 is its compensation
+  A_COMP_F = 4,
+  A_MAX_O = 5,     // atomicMax of the order-preserving unsigned image
+  A_MIN_O = 6,     // atomicMax of the complemented image
+};
+constexpr int kMaxAcc = 16;
+constexpr int kMaxAggs = 16;
+
+struct AccPlan {
+  int32_t n_acc;
+  int8_t kind[kMaxAcc];
+  int8_t col[kMaxAcc];
+};
+
+struct OutAgg {
+  int8_t type;       // GHB_AGG_*
+  int8_t in_type;    // input column type
+  int8_t acc_val;
+  int8_t acc_cnt;    // accumulator that says "saw a non-NULL value"
+};
+
+struct GbParams {
+  ColSet cols;
+  PredProg pred;
+  AccPlan acc;
+  int32_t key_col;       // -1: global aggregate (all rows in one group)
+  int32_t smem_slots;    // power of two, 0 = no shared stage
+  int32_t warp_agg;      // combine equal keys within a warp before the atomics
+  int64_t n;
+  uint64_t* gkeys;       // [C + 2] stored keys (flip_i64 of the raw key), 0 = empty
+  uint64_t* gacc;        // [n_acc][C + 2]
+  int64_t C;             // power of two
+  int32_t gprobe;        // probe limit in the global table
+  int32_t* status;
+  int64_t* d_out_groups;
+};
+
+struct FinParams {
+  const uint64_t* gkeys_ro;
+  uint64_t* gkeys;
+  uint64_t* gacc;
+  int64_t C;
+  int32_t n_acc;
+  int32_t key_type;      // -1: global aggregate
+  ghb_out_column key_out;
+  int32_t naggs;
+  OutAgg agg[kMaxAggs];
+  ghb_out_column out[kMaxAggs];
+  int64_t cap;
+  int64_t* d_out_groups;
+  int32_t* status;
+};
+
+// ---------------------------------------------------------------- device
+__device__ __forceinline__ double two_sum_err(double a, double b, double s) {
+  double bb = __dsub_rn(s, a);
+  return __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+
+// Compensated atomic add of x into (sum, comp).
+__device__ __forceinline__ void atomic_add_comp(uint64_t* sum, uint64_t* comp, double x) {
+  if (x == 0.0) return;
+  double old = atomicAdd((double*)sum, x);
+  double e = two_sum_err(old, x, __dadd_rn(old, x));
+  if (e != 0.0) atomicAdd((double*)comp, e);
+}
+
+__device__ __forceinline__ uint64_t order_image(int type, int64_t raw) {
+  return type == GHB_DOUBLE ? flip_f64_bits((uint64_t)raw) : flip_i64(raw);
+}
+
+// Open-addressing find-or-insert of a non-zero stored key.  Linear probing;
+// returns the slot or -1 after max_probe probes.
+__device__ __forceinline__ int64_t table_insert(uint64_t* keys, int64_t mask, uint64_t u,
+                                                int max_probe) {
+  int64_t h = (int64_t)(mix64(u) & (uint64_t)mask);
+  for (int p = 0; p < max_probe; p++) {
+    uint64_t cur = keys[h];
+    if (cur == u) return h;
+    if (cur == 0) {
+      unsigned long long prev = atomicCAS((unsigned long long*)&keys[h], 0ull, (unsigned long long)u);
+      if (prev == 0 || prev == u) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+// Folds row r into the accumulators at `slot` (stride = slots per accumulator).
+__device__ __forceinline__ void acc_row(const GbParams& p, uint64_t* acc, int64_t stride,
+                                        int64_t slot, int64_t r) {
+  for (int a = 0; a < p.acc.n_acc; a++) {
+    uint64_t* cell = acc + a * stride + slot;
+    int8_t kind = p.acc.kind[a];
+    if (kind == A_CNT_STAR) { atomicAdd((unsigned long long*)cell, 1ull); continue; }
+    if (kind == A_COMP_F) continue;
+    const ghb_column& c = p.cols.c[p.acc.col[a]];
+    int64_t v = ld_raw(c, r);
+    if (raw_is_null(c, v, r)) continue;
+    switch (kind) {
+      case A_CNT_NN: atomicAdd((unsigned long long*)cell, 1ull); break;
+      case A_SUM_I: atomicAdd((unsigned long long*)cell, (unsigned long long)v); break;
+      case A_SUM_F: atomic_add_comp(cell, cell + stride, raw_to_f64(c.type, v)); break;
+      case A_MAX_O: atomicMax((unsigned long long*)cell, (unsigned long long)order_image(c.type, v)); break;
+      case A_MIN_O: atomicMax((unsigned long long*)cell, (unsigned long long)~order_image(c.type, v)); break;
+    }
+  }
+}
+
+// Row contribution of accumulator a as a 64-bit word (0 = no contribution).
+__device__ __forceinline__ uint64_t acc_contrib(const GbParams& p, int a, int64_t r, bool live) {
+  if (!live) return 0;
+  int8_t kind = p.acc.kind[a];
+  if (kind == A_CNT_STAR) return 1;
+  if (kind == A_COMP_F) return 0;
+  const ghb_column& c = p.cols.c[p.acc.col[a]];
+  int64_t v = ld_raw(c, r);
+  if (raw_is_null(c, v, r)) return 0;
+  switch (kind) {
+    case A_CNT_NN: return 1;
+    case A_SUM_I: return (uint64_t)v;
+    case A_SUM_F: return (uint64_t)__double_as_longlong(raw_to_f64(c.type, v));
+    case A_MAX_O: return order_image(c.type, v);
+    case A_MIN_O: return ~order_image(c.type, v);
+  }
+  return 0;
+}
+
+// Merges one partial accumulator word `w` (and its compensation `wc`) into a cell.
+__device__ __forceinline__ void acc_merge(int8_t kind, uint64_t* cell, int64_t stride, uint64_t w,
+                                          uint64_t wc) {
+  switch (kind) {
+    case A_CNT_STAR:
+    case A_CNT_NN:
+    case A_SUM_I:
+      if (w) atomicAdd((unsigned long long*)cell, (unsigned long long)w);
+      break;
+    case A_SUM_F:
+      atomic_add_comp(cell, cell + stride, __longlong_as_double(w));
+      if (wc && __longlong_as_double(wc) != 0.0) atomicAdd((double*)(cell + stride), __longlong_as_double(wc));
+      break;
+    case A_MAX_O:
+    case A_MIN_O:
+      if (w) atomicMax((unsigned long long*)cell, (unsigned long long)w);
+      break;
+    default: break;
+  }
+}
+
+// Warp-cooperative fold: lanes holding the same slot combine their row
+// contributions through a per-warp staging row, then the lowest such lane
+// applies one atomic per accumulator.
+__device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, int64_t stride,
+                                             int64_t slot, int64_t r, bool live,
+                                             uint64_t* stage) {
+  const int lane = threadIdx.x & 31;
+  unsigned peers = __match_any_sync(0xffffffffu, live ? slot : -1);
+  int leader = __ffs(peers) - 1;
+  for (int a = 0; a < p.acc.n_acc; a++) {
+    int8_t kind = p.acc.kind[a];
+    if (kind == A_COMP_F) continue;
+    uint64_t w = acc_contrib(p, a, r, live);
+    stage[lane] = w;
+    __syncwarp();
+    if (live && lane == leader) {
+      uint64_t tot = 0, comp = 0;
+      double s = 0.0, c = 0.0;
+      for (unsigned m = peers; m; m &= m - 1) {
+        uint64_t x = stage[__ffs(m) - 1];
+        switch (kind) {
+          case A_CNT_STAR:
+          case A_CNT_NN:
+          case A_SUM_I: tot += x; break;
+          case A_SUM_F: {
+            double xv = __longlong_as_double(x);
+            double t = __dadd_rn(s, xv);
+            c = __dadd_rn(c, two_sum_err(s, xv, t));
+            s = t;
+            break;
+          }
+          default: tot = max(tot, x); break;
+        }
+      }
+      if (kind == A_SUM_F) {
+        tot = (uint64_t)__double_as_longlong(s);
+        comp = (uint64_t)__double_as_longlong(c);
+      }
+      acc_merge(kind, acc + a * stride + slot, stride, tot, comp);
+    }
+    __syncwarp();
+  }
+}
+
+template <bool KEYED>
+__global__ void __launch_bounds__(1024) gb_fold_kernel(GbParams p) {
+  extern __shared__ uint64_t smem[];
+  const int S = p.smem_slots;
+  const int64_t sstride = S + 2;
+  uint64_t* skeys = smem;
+  uint64_t* sacc = smem + sstride;
+  uint64_t* stage = sacc + (int64_t)p.acc.n_acc * sstride + (threadIdx.x >> 5) * 32;
+  const int64_t gstride = p.C + 2;
+
+  for (int64_t i = threadIdx.x; i < sstride * (1 + p.acc.n_acc); i += blockDim.x) smem[i] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *p.d_out_groups = 0;
+  __syncthreads();
+
+  // Warp-uniform trip count so the warp-cooperative path can use all lanes.
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t iters = (p.n + nthreads - 1) / nthreads;
+  for (int64_t it = 0; it < iters; it++) {
+    int64_t r = first + it * nthreads;
+    bool live = r < p.n && eval_pred(p.pred, p.cols, r);
+    uint64_t u = 0;
+    int side = -1;  // 0: key INT64_MIN, 1: NULL key / global aggregate
+    if (live) {
+      if (KEYED) {
+        const ghb_column& kc = p.cols.c[p.key_col];
+        int64_t raw = ld_raw(kc, r);
+        if (raw_is_null(kc, raw, r)) side = 1;
+        else {
+          u = flip_i64(raw);
+          if (u == 0) side = 0;
+        }
+      } else {
+        side = 1;
+      }
+    }
+    int64_t sslot = -1;
+    if (live && S > 0) {
+      sslot = side >= 0 ? S + side : table_insert(skeys, S - 1, u, 8);
+    }
+    if (p.warp_agg) {
+      bool in_smem = live && sslot >= 0;
+      if (__any_sync(0xffffffffu, in_smem))
+        acc_row_warp(p, sacc, sstride, in_smem ? sslot : 0, r, in_smem, stage);
+    } else if (live && sslot >= 0) {
+      acc_row(p, sacc, sstride, sslot, r);
+    }
+    if (live && sslot < 0) {
+      int64_t g = side >= 0 ? p.C + side : table_insert(p.gkeys, p.C - 1, u, p.gprobe);
+      if (g < 0) {
+        raise_status(p.status, kDevCapacity);
+        continue;
+      }
+      acc_row(p, p.gacc, gstride, g, r);
+    }
+  }
+  __syncthreads();
+
+  // merge the shared table into the global one
+  for (int64_t s = threadIdx.x; s < sstride && S > 0; s += blockDim.x) {
+    if (sacc[s] == 0) continue;  // accumulator 0 is COUNT(*): empty slot
+    int64_t g;
+    if (s < S) {
+      g = table_insert(p.gkeys, p.C - 1, skeys[s], p.gprobe);
+      if (g < 0) {
+        raise_status(p.status, kDevCapacity);
+        continue;
+      }
+    } else {
+      g = p.C + (s - S);
+    }
+    for (int a = 0; a < p.acc.n_acc; a++) {
+      int8_t kind = p.acc.kind[a];
+      if (kind == A_COMP_F) continue;
+      uint64_t w = sacc[a * sstride + s];
+      uint64_t wc = kind == A_SUM_F ? sacc[(a + 1) * sstride + s] : 0;
+      acc_merge(kind, p.gacc + a * gstride + g, gstride, w, wc);
+    }
+  }
+}
+
+__device__ __forceinline__ void write_out(const ghb_out_column& o, int64_t row, bool null,
+                                          int64_t iv, double dv) {
+  if (o.is_null) o.is_null[row] = null ? 1 : 0;
+  switch (o.type) {
+    case GHB_LONG: ((int64_t*)o.data)[row] = null ? INT64_MAX : iv; break;
+    case GHB_INT: ((int32_t*)o.data)[row] = null ? INT32_MAX : (int32_t)iv; break;
+    case GHB_DOUBLE: ((double*)o.data)[row] = null ? __longlong_as_double(0x7ff8000000000000ll) : dv; break;
+  }
+}
+
+__device__ __forceinline__ int64_t decode_order(int type, uint64_t img) {
+  return type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(img) : (int64_t)(img ^ 0x8000000000000000ull);
+}
+
+__global__ void gb_finalize_kernel(FinParams f) {
+  const int64_t stride = f.C + 2;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < stride;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t cnt = f.gacc[s];
+    bool emit = cnt != 0 || (f.key_type < 0 && s == f.C + 1);
+    if (emit && (f.key_type >= 0 || s == f.C + 1)) {
+      int64_t row = (int64_t)atomicAdd((unsigned long long*)f.d_out_groups, 1ull);
+      if (row < f.cap) {
+        if (f.key_type >= 0) {
+          bool knull = s == f.C + 1;
+          int64_t raw = s == f.C ? INT64_MIN : (int64_t)(f.gkeys_ro[s] ^ 0x8000000000000000ull);
+          write_out(f.key_out, row, knull, raw, __longlong_as_double(raw));
+        }
+        for (int a = 0; a < f.naggs; a++) {
+          const OutAgg& d = f.agg[a];
+          uint64_t v = f.gacc[d.acc_val * stride + s];
+          bool null = f.gacc[d.acc_cnt * stride + s] == 0;
+          int64_t iv = 0;
+          double dv = 0.0;
+          switch (d.type) {
+            case GHB_AGG_CNT: null = false; iv = (int64_t)v; break;
+            case GHB_AGG_SUM:
+              if (d.in_type == GHB_DOUBLE)
+                dv = __longlong_as_double(v) + __longlong_as_double(f.gacc[(d.acc_val + 1) * stride + s]);
+              else
+                iv = (int64_t)v;
+              break;
+            case GHB_AGG_AVG: {
+              double sum = __longlong_as_double(v) + __longlong_as_double(f.gacc[(d.acc_val + 1) * stride + s]);
+              uint64_t c = f.gacc[d.acc_cnt * stride + s];
+              dv = c ? sum / (double)c : 0.0;
+              break;
+            }
+            case GHB_AGG_MIN:
+            case GHB_AGG_MAX: {
+              uint64_t img = d.type == GHB_AGG_MIN ? ~v : v;
+              iv = decode_order(d.in_type, img);
+              dv = __longlong_as_double(iv);
+              break;
+            }
+          }
+          write_out(f.out[a], row, null, iv, dv);
+        }
+      } else {
+        raise_status(f.status, kDevCapacity);
+      }
+    }
+    // leave the slot zeroed for the next call
+    if (cnt != 0 || s >= f.C) {
+      f.gkeys[s] = 0;
+      for (int a = 0; a < f.n_acc; a++) f.gacc[a * stride + s] = 0;
+    } else if (f.gkeys[s] != 0) {
+      f.gkeys[s] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- host
+struct GbPlan {
+  AccPlan acc;
+  FinParams fin;
+};
+
+// Index of accumulator (k, col), adding it (and its compensation word for a
+// double sum) when absent; -1 when the plan has no room left.
+static int add_acc(AccPlan& ap, AccKind k, int col) {
+  for (int a = 0; a < ap.n_acc; a++)
+    if (ap.kind[a] == k && ap.col[a] == col) return a;
+  if (ap.n_acc + (k == A_SUM_F ? 2 : 1) > kMaxAcc) return -1;
+  int a = ap.n_acc++;
+  ap.kind[a] = k;
+  ap.col[a] = (int8_t)col;
+  if (k == A_SUM_F) {
+    ap.kind[ap.n_acc] = A_COMP_F;
+    ap.col[ap.n_acc] = (int8_t)col;
+    ap.n_acc++;
+  }
+  return a;
+}
+
+static int32_t plan_aggs(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols,
+                         const ghb_agg_desc* aggs, int32_t naggs, const ghb_out_column* out,
+                         int32_t nkeys, GbPlan* plan) {
+  if (naggs < 0 || naggs > kMaxAggs)
+    return set_error(ctx, GHB_ERR_INVALID, "naggs=%d outside [0,%d]", naggs, kMaxAggs);
+  AccPlan& ap = plan->acc;
+  ap.n_acc = 0;
+  add_acc(ap, A_CNT_STAR, -1);
+  for (int i = 0; i < naggs; i++) {
+    const ghb_agg_desc& d = aggs[i];
+    OutAgg& o = plan->fin.agg[i];
+    o.type = (int8_t)d.type;
+    bool star = d.type == GHB_AGG_CNT && d.col < 0;
+    if (!star && (d.col < 0 || d.col >= ncols))
+      return set_error(ctx, GHB_ERR_INVALID, "aggregate %d: column %d out of range", i, d.col);
+    const ghb_column* c = star ? nullptr : &cols[d.col];
+    o.in_type = (int8_t)(c ? c->type : GHB_LONG);
+    int cnt = 0;
+    if (c && c->null_mode != GHB_NULLS_NONE) cnt = add_acc(ap, A_CNT_NN, d.col);
+    o.acc_cnt = (int8_t)cnt;
+    int32_t want_out;
+    switch (d.type) {
+      case GHB_AGG_CNT:
+        o.acc_val = (int8_t)cnt;
+        want_out = GHB_LONG;
+        break;
+      case GHB_AGG_SUM:
+        if (c->type == GHB_DOUBLE) {
+          o.acc_val = (int8_t)add_acc(ap, A_SUM_F, d.col);
+          want_out = GHB_DOUBLE;
+        } else {
+          o.acc_val = (int8_t)add_acc(ap, A_SUM_I, d.col);
+          want_out = GHB_LONG;
+        }
+        break;
+      case GHB_AGG_AVG:
+        o.acc_val = (int8_t)add_acc(ap, A_SUM_F, d.col);
+        want_out = GHB_DOUBLE;
+        break;
+      case GHB_AGG_MIN:
+        o.acc_val = (int8_t)add_acc(ap, A_MIN_O, d.col);
+        want_out = c->type;
+        break;
+      case GHB_AGG_MAX:
+        o.acc_val = (int8_t)add_acc(ap, A_MAX_O, d.col);
+        want_out = c->type;
+        break;
+      default:
+        return set_error(ctx, GHB_ERR_UNSUPPORTED, "aggregate %d: type %d not supported", i, d.type);
+    }
+    if (cnt < 0 || o.acc_val < 0)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "more than %d accumulator words per group", kMaxAcc);
+    const ghb_out_column& oc = out[nkeys + i];
+    if (oc.type != want_out)
+      return set_error(ctx, GHB_ERR_INVALID, "aggregate %d: output column type %d, expected %d", i,
+                       oc.type, want_out);
+    if (!oc.data) return set_error(ctx, GHB_ERR_INVALID, "aggregate %d: output data is NULL", i);
+    plan->fin.out[i] = oc;
+  }
+  plan->fin.naggs = naggs;
+  plan->fin.n_acc = ap.n_acc;
+  return GHB_OK;
+}
+
+static int64_t next_pow2(int64_t v) {
+  int64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+// Shared implementation; `table` (nullable) overrides the context's table.
+int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
+                            int32_t ncols, const int32_t* key_cols, int32_t nkeys,
+                            const ghb_agg_desc* aggs, int32_t naggs, ghb_out_column* out,
+                            int64_t out_capacity, int64_t* d_out_groups,
+                            const ghb_groupby_cfg* cfg, cudaStream_t stream,
+                            void* fixed_table, size_t fixed_table_bytes) {
+  if (!ctx) return GHB_ERR_INVALID;
+  int64_t n = 0;
+  int32_t st = validate_columns(ctx, cols, ncols, &n);
+  if (st) return st;
+  if (nkeys < 0 || nkeys > 1)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "nkeys=%d: the device group-by takes 0 or 1 key column", nkeys);
+  if (nkeys == 1 && (!key_cols || key_cols[0] < 0 || key_cols[0] >= ncols))
+    return set_error(ctx, GHB_ERR_INVALID, "key column out of range");
+  if (naggs > 0 && !aggs) return set_error(ctx, GHB_ERR_INVALID, "aggs is NULL");
+  if ((nkeys + naggs) > 0 && !out) return set_error(ctx, GHB_ERR_INVALID, "out is NULL");
+  if (!d_out_groups) return set_error(ctx, GHB_ERR_INVALID, "d_out_groups is NULL");
+  if (out_capacity < 1) return set_error(ctx, GHB_ERR_INVALID, "out_capacity must be >= 1");
+
+  GbParams p;
+  std::memset(&p, 0, sizeof(p));
+  GbPlan plan;
+  std::memset(&plan, 0, sizeof(plan));
+  st = plan_aggs(ctx, cols, ncols, aggs, naggs, out, nkeys, &plan);
+  if (st) return st;
+  st = build_pred_prog(ctx, pred, ncols, &p.pred);
+  if (st) return st;
+  for (int i = 0; i < ncols; i++) p.cols.c[i] = cols[i];
+  p.cols.n = ncols;
+  p.acc = plan.acc;
+  p.n = n;
+  p.key_col = nkeys ? key_cols[0] : -1;
+  if (nkeys) {
+    if (out[0].type != cols[key_cols[0]].type)
+      return set_error(ctx, GHB_ERR_INVALID, "key output column type %d, expected %d", out[0].type,
+                       cols[key_cols[0]].type);
+    if (!out[0].data) return set_error(ctx, GHB_ERR_INVALID, "key output data is NULL");
+  }
+
+  int64_t max_groups = (cfg && cfg->max_groups > 0) ? cfg->max_groups : out_capacity;
+  if (nkeys == 0) max_groups = 1;
+  max_groups = std::min<int64_t>(max_groups, std::max<int64_t>(n, 1));
+  int64_t C = (cfg && cfg->global_slots_log2 > 0) ? (1ll << cfg->global_slots_log2)
+                                                   : next_pow2(std::max<int64_t>(2 * max_groups, 64));
+  int S;
+  if (cfg && cfg->smem_slots < 0) S = 0;
+  else if (cfg && cfg->smem_slots > 0) S = (int)next_pow2(cfg->smem_slots);
+  else S = (int)std::min<int64_t>(4096, next_pow2(std::max<int64_t>(2 * max_groups, 64)));
+  if (nkeys == 0) S = 64;
+  int threads = (cfg && cfg->block_threads > 0) ? cfg->block_threads : 1024;
+  threads = std::max(64, std::min(1024, threads / 32 * 32));
+  size_t smem = (size_t)(S + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8;
+  while (smem > 200 * 1024 && S > 64) {
+    S /= 2;
+    smem = (size_t)(S + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8;
+  }
+  p.smem_slots = S;
+  p.warp_agg = (nkeys == 0 || max_groups <= 64) ? 1 : 0;
+
+  size_t table_bytes = (size_t)(C + 2) * 8 * (1 + p.acc.n_acc);
+  if (fixed_table) {
+    if (table_bytes > fixed_table_bytes)
+      return set_error(ctx, GHB_ERR_CAPACITY, "group-by table needs %zu bytes, %zu available",
+                       table_bytes, fixed_table_bytes);
+    p.gkeys = (uint64_t*)fixed_table;
+  } else {
+    if (table_bytes > ctx->gb_bytes || ctx->gb_dirty || !ctx->gb_table) {
+      if (table_bytes > ctx->gb_bytes) {
+        GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+        if (ctx->gb_table) cudaFree(ctx->gb_table);
+        ctx->gb_table = nullptr;
+        ctx->gb_bytes = 0;
+        size_t want = std::max(table_bytes, (size_t)1 << 20);
+        if (cudaMalloc(&ctx->gb_table, want) != cudaSuccess) {
+          cudaGetLastError();
+          return set_error(ctx, GHB_ERR_OOM, "cannot allocate a %zu-byte group-by table", want);
+        }
+        ctx->gb_bytes = want;
+      }
+      GHB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->gb_table, 0, ctx->gb_bytes, stream));
+      ctx->gb_dirty = false;
+    }
+    p.gkeys = (uint64_t*)ctx->gb_table;
+  }
+  p.gacc = p.gkeys + (C + 2);
+  p.C = C;
+  p.gprobe = (int32_t)std::min<int64_t>(C, 1 << 20);
+  p.status = ctx->d_status;
+  p.d_out_groups = d_out_groups;
+
+  int blocks_per_sm = 0;
+  auto kfn = nkeys ? gb_fold_kernel<true> : gb_fold_kernel<false>;
+  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kfn, threads, smem));
+  blocks_per_sm = std::max(1, blocks_per_sm);
+  if (cfg && cfg->ctas_per_sm > 0) blocks_per_sm = std::min(blocks_per_sm, cfg->ctas_per_sm);
+  int64_t want_blocks = (n + threads - 1) / threads;
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * blocks_per_sm, want_blocks));
+  kfn<<<grid, threads, smem, stream>>>(p);
+  GHB_LAUNCH_CHECK(ctx);
+
+  FinParams& f = plan.fin;
+  f.gkeys_ro = p.gkeys;
+  f.gkeys = p.gkeys;
+  f.gacc = p.gacc;
+  f.C = C;
+  f.key_type = nkeys ? cols[key_cols[0]].type : -1;
+  if (nkeys) f.key_out = out[0];
+  f.cap = out_capacity;
+  f.d_out_groups = d_out_groups;
+  f.status = ctx->d_status;
+  int fthreads = 256;
+  int fgrid = (int)std::min<int64_t>((C + 2 + fthreads - 1) / fthreads, (int64_t)ctx->num_sms * 8);
+  gb_finalize_kernel<<<fgrid, fthreads, 0, stream>>>(f);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
+                                      int32_t ncols, const int32_t* key_cols, int32_t nkeys,
+                                      const ghb_agg_desc* aggs, int32_t naggs, ghb_out_column* out,
+                                      int64_t out_capacity, int64_t* d_out_groups,
+                                      const ghb_groupby_cfg* cfg, void* stream) {
+  if (!ctx) return GHB_ERR_INVALID;
+  scratch_reset(ctx);
+  return filter_groupby_impl(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, out_capacity,
+                             d_out_groups, cfg, (cudaStream_t)stream, nullptr, 0);
+}

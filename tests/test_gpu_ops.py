@@ -1,0 +1,489 @@
+"""GPU parity: every operator through the C ABI against the CPU oracle.
+
+Bit-exact for keys, counts, integer sums, MIN/MAX, filter rows, join pairs
+(as sorted multisets) and sort order; DOUBLE SUM/AVG within 1e-12 relative
+of the oracle's Hive-order sequential sum (REL_TOL below).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ghive_b200 import abi, workloads
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+EDGE_SIZES = [0, 1, 31, 32, 33, 1023, 1024, 1025, 2047, 2049, 4095, 4097, 100_003]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from ghive_b200.ops import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def devcol(c):
+    from ghive_b200.ops import Sentinel
+    if isinstance(c, Sentinel):
+        return Sentinel(dev(c.values))
+    if isinstance(c, tuple):
+        return (dev(c[0]), dev(c[1].astype(np.uint8)))
+    return dev(c)
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def oracle_col(c):
+    from ghive_b200.ops import Sentinel
+    return c.values if isinstance(c, Sentinel) else c
+
+
+# ----------------------------------------------------------------- filter
+def _check_filter(ctx, pred, cols, sentinel=False):
+    ocols = [oracle_col(c) for c in cols]
+    sel = oracle.filter_rows(pred, ocols) if not sentinel else \
+        oracle.filter_rows(pred, ocols, n=None)
+    outs, k = ctx.filter(pred, [devcol(c) for c in cols])
+    assert k == len(sel)
+    for c, (v, nl) in zip(cols, outs):
+        vals = oracle_col(c)
+        vals = vals[0] if isinstance(vals, tuple) else vals
+        got = host(v)
+        exp = vals[sel]
+        assert np.array_equal(got.view(np.uint8), exp.view(np.uint8)) if exp.dtype == np.float64 \
+            else np.array_equal(got, exp)
+        if isinstance(c, tuple):
+            assert np.array_equal(host(nl), c[1][sel].astype(bool))
+
+
+@pytest.mark.parametrize("n", EDGE_SIZES)
+def test_filter_edge_sizes(ctx, n):
+    g = np.random.default_rng(n + 1)
+    cols = [g.integers(0, 2526, n, dtype=np.int32), g.integers(-50, 50, n, dtype=np.int64),
+            g.random(n)]
+    _check_filter(ctx, abi.Pred.leaf(abi.FILTER_LT, 0, a=1263), cols)
+
+
+def test_filter_every_mode_and_type(ctx):
+    g = np.random.default_rng(5)
+    n = 50_000
+    cols = [g.integers(-100, 100, n, dtype=np.int32), g.integers(-100, 100, n, dtype=np.int64),
+            np.round(g.normal(0, 50, n), 1)]
+    for col in range(3):
+        for mode in range(abi.FILTER_NOT_NULL + 1):
+            lit = (-10.5, 20.0) if col == 2 or mode % 2 else (-10, 20)
+            p = abi.Pred.leaf(mode, col, a=lit[0], b=lit[1])
+            _check_filter(ctx, p, cols)
+
+
+def test_filter_tree_and_column_compare(ctx):
+    g = np.random.default_rng(6)
+    n = 70_001
+    cols = [g.integers(0, 100, n, dtype=np.int64), g.integers(0, 100, n, dtype=np.int64),
+            g.integers(0, 3, n, dtype=np.int32), g.random(n) * 100]
+    p = abi.Pred.or_(abi.Pred.and_(abi.Pred.leaf(abi.FILTER_GT, 0, col2=1),
+                                   abi.Pred.leaf(abi.FILTER_EQ, 2, a=0.0)),
+                     abi.Pred.leaf(abi.FILTER_EQ_RANGE, 3, a=10.0, b=12.5))
+    _check_filter(ctx, p, cols)
+    p2 = abi.Pred.leaf(abi.FILTER_LE, 3, col2=0)  # double vs long column
+    _check_filter(ctx, p2, cols)
+
+
+def test_filter_nulls_bytemap_and_sentinel(ctx):
+    from ghive_b200.ops import Sentinel
+    g = np.random.default_rng(7)
+    n = 33_333
+    v = g.integers(0, 1000, n, dtype=np.int64)
+    isnull = g.random(n) < 0.2
+    _check_filter(ctx, abi.Pred.leaf(abi.FILTER_GE, 0, a=500), [(v, isnull)])
+    _check_filter(ctx, abi.Pred.leaf(abi.FILTER_NOT_NULL, 0), [(v, isnull)])
+    s = v.copy()
+    s[isnull] = np.iinfo(np.int64).max
+    out, k = ctx.filter(abi.Pred.leaf(abi.FILTER_NOT_NULL, 0), [Sentinel(dev(s))])
+    assert k == int((~isnull).sum())
+    d = np.where(isnull, np.nan, g.random(n))
+    out, k = ctx.filter(abi.Pred.leaf(abi.FILTER_LT, 0, a=0.5), [Sentinel(dev(d))])
+    assert k == int(((d < 0.5) & ~np.isnan(d)).sum())
+
+
+def test_filter_ghive_golden_rows(ctx):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ghive_filter.json")) as f:
+        case = json.load(f)["cases"][0]
+    cols = [np.array(c[1], dtype={"long": np.int64, "double": np.float64, "int": np.int32}[c[0]])
+            for c in case["columns"]]
+    pred = abi.Pred.leaf(getattr(abi, case["mode"]), case["col"], a=float(case["literal"]))
+    outs, k = ctx.filter(pred, [dev(c) for c in cols])
+    rows = [tuple(("%f" % host(v)[i]) if t == abi.DOUBLE else str(host(v)[i])
+                  for (v, _), t in zip(outs, case["expected_types"])) for i in range(k)]
+    assert rows == [tuple(r) for r in case["expected_rows"]]
+
+
+def test_filter_capacity_error_reports_required_rows(ctx):
+    from ghive_b200._lib import GhbError
+    n = 10_000
+    cols = [np.arange(n, dtype=np.int64)]
+    with pytest.raises(GhbError) as e:
+        ctx.filter(abi.Pred.leaf(abi.FILTER_LT, 0, a=5000), [dev(cols[0])], capacity=100)
+    assert e.value.code == abi.ERR_CAPACITY
+    outs, k = ctx.filter(abi.Pred.leaf(abi.FILTER_LT, 0, a=5000), [dev(cols[0])])
+    assert k == 5000  # the context stays usable after the error
+
+
+# --------------------------------------------------------------- group-by
+def _norm_rows(keys, aggs):
+    """Rows as tuples sorted by key (NULL first)."""
+    n = len(aggs[0][0]) if aggs else len(keys[0][0])
+    rows = []
+    for i in range(n):
+        r = []
+        for v, nl in keys + aggs:
+            r.append(None if nl[i] else v[i].item())
+        rows.append(tuple(r))
+    nk = len(keys)
+    return sorted(rows, key=lambda r: tuple((x is not None, x if x is not None else 0) for x in r[:nk]))
+
+
+def _coltype(c):
+    v = oracle_col(c)
+    v = v[0] if isinstance(v, tuple) else v
+    return abi.TYPE_OF_DTYPE[np.dtype(v.dtype)]
+
+
+def _check_groupby(ctx, pred, cols, keys, aggs, max_groups=None):
+    ocols = [oracle_col(c) for c in cols]
+    ok, oa = oracle.filter_groupby(pred, ocols, keys, aggs)
+    exp = _norm_rows(ok, oa)
+    gk, ga, g = ctx.filter_groupby(pred, [devcol(c) for c in cols], keys, aggs,
+                                   capacity=max(len(exp), 1) + 16, max_groups=max_groups)
+    got = _norm_rows([(host(v), host(nl)) for v, nl in gk], [(host(v), host(nl)) for v, nl in ga])
+    assert g == len(exp)
+    types = [abi.agg_out_type(t, _coltype(cols[c]) if c >= 0 else abi.LONG) for t, c in aggs]
+    for re_, rg in zip(exp, got):
+        assert re_[:len(keys)] == rg[:len(keys)]
+        for j, (e, x) in enumerate(zip(re_[len(keys):], rg[len(keys):])):
+            if e is None or x is None:
+                assert e is None and x is None
+            elif types[j] == abi.DOUBLE:
+                assert abs(x - e) <= REL_TOL * max(abs(e), 1e-300), (e, x)
+            else:
+                assert x == e
+    return g
+
+
+@pytest.mark.parametrize("n", EDGE_SIZES)
+def test_groupby_fact_shape_edge_sizes(ctx, n):
+    cols = workloads.fact_table(n, seed_idx=100 + n % 97, groups=1000)
+    _check_groupby(ctx, workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT, max_groups=1000)
+
+
+def test_groupby_fact_shape_300k(ctx):
+    cols = workloads.fact_table(300_000, seed_idx=7)
+    g = _check_groupby(ctx, workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT, max_groups=1000)
+    assert g == 1000
+
+
+@pytest.mark.parametrize("groups", [1, 7, 64, 5000, 200_000])
+def test_groupby_cardinalities_and_skew(ctx, groups):
+    g = np.random.default_rng(groups)
+    n = 400_000
+    keys = workloads.zipf_ranks(g, n, groups, 1.1) * 7919 - 1000
+    cols = [keys, g.integers(1, 51, n, dtype=np.int64),
+            g.integers(90000, 10500001, n) / 100.0, g.integers(0, 2526, n, dtype=np.int32)]
+    _check_groupby(ctx, workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT, max_groups=groups)
+
+
+def test_groupby_no_keys_and_empty(ctx):
+    cols = workloads.fact_table(123_457, seed_idx=9)
+    _check_groupby(ctx, workloads.fact_predicate(), cols, [], workloads.AGGS_FACT)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_LT, 3, a=-1), cols, [], workloads.AGGS_FACT)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_LT, 3, a=-1), cols, [0], workloads.AGGS_FACT)
+
+
+def test_groupby_nulls_keys_and_values(ctx):
+    from ghive_b200.ops import Sentinel
+    g = np.random.default_rng(11)
+    n = 80_000
+    k = g.integers(-5, 40, n, dtype=np.int64)
+    kn = g.random(n) < 0.1
+    v = g.integers(-1000, 1000, n, dtype=np.int64)
+    vn = g.random(n) < 0.3
+    vn[k == 3] = True  # an all-NULL group: SUM/AVG/MIN/MAX NULL, COUNT(col) 0
+    dv = g.random(n) * 100
+    dn = g.random(n) < 0.3
+    aggs = [(abi.CNT, -1), (abi.CNT, 1), (abi.SUM, 1), (abi.AVG, 1), (abi.MIN, 1), (abi.MAX, 1),
+            (abi.SUM, 2), (abi.AVG, 2), (abi.MIN, 2), (abi.MAX, 2)]
+    _check_groupby(ctx, None, [(k, kn), (v, vn), (dv, dn)], [0], aggs, max_groups=64)
+    ks = k.copy()
+    ks[kn] = np.iinfo(np.int64).max
+    # sentinel keys: NULL group holds the same rows
+    ok, oa = oracle.filter_groupby(None, [(k, kn), v], [0], [(abi.SUM, 1)])
+    gk, ga, gg = ctx.filter_groupby(None, [Sentinel(dev(ks)), dev(v)], [0], [(abi.SUM, 1)],
+                                    capacity=128, max_groups=64)
+    assert gg == len(ok[0][0])
+    assert sum(host(nl).sum() for _, nl in gk) == 1
+
+
+def test_groupby_key_types_and_extremes(ctx):
+    g = np.random.default_rng(12)
+    n = 50_000
+    i64 = np.iinfo(np.int64)
+    k = g.choice(np.array([i64.min, i64.min + 1, -1, 0, 1, i64.max - 1], dtype=np.int64), n)
+    v = g.choice(np.array([i64.max, i64.min, 1, -1], dtype=np.int64), n)  # SUM wraps
+    _check_groupby(ctx, None, [k, v], [0], [(abi.SUM, 1), (abi.MIN, 1), (abi.MAX, 1), (abi.CNT, -1)],
+                   max_groups=8)
+    kd = g.choice(np.array([-0.5, 0.0, 2.25, 1e300, -1e-300]), n)
+    _check_groupby(ctx, None, [kd, v], [0], [(abi.SUM, 1), (abi.CNT, -1)], max_groups=8)
+    ki = g.integers(np.iinfo(np.int32).min, np.iinfo(np.int32).max, n, dtype=np.int32) % 1000
+    _check_groupby(ctx, None, [ki, v], [0], [(abi.MAX, 1)], max_groups=1000)
+
+
+def test_groupby_hive_golden_cases(ctx):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hive_groupby.json")) as f:
+        cases = json.load(f)["cases"]
+    ran = 0
+    for case in cases:
+        if case.get("key_type") == "string":
+            continue
+        vals = case["values"] * case.get("repeat", 1)
+        vdt = np.float64 if case["value_type"] == "double" else np.int64
+        v = np.array([0 if x is None else x for x in vals], dtype=vdt)
+        vn = np.array([x is None for x in vals], dtype=bool)
+        spec = (abi.CNT, -1) if case["agg"] == "count(*)" else \
+            (abi.AGG_NAMES[case["agg"]], 1 if "keys" in case else 0)
+        if "keys" not in case:
+            gk, ga, g = ctx.filter_groupby(None, [(dev(v), dev(vn.astype(np.uint8)))], [], [spec],
+                                           capacity=1)
+            val, nl = ga[0]
+            got = None if host(nl)[0] else host(val)[0].item()
+            assert got == case["expected"], (case["test"], got, case["expected"])
+        else:
+            ks = case["keys"]
+            k = np.array([0 if x is None else x for x in ks], dtype=np.int64)
+            kn = np.array([x is None for x in ks], dtype=bool)
+            gk, ga, g = ctx.filter_groupby(None, [(dev(k), dev(kn.astype(np.uint8))),
+                                                  (dev(v), dev(vn.astype(np.uint8)))], [0], [spec],
+                                           capacity=16, max_groups=8)
+            got = sorted([(None if host(gk[0][1])[i] else host(gk[0][0])[i].item(),
+                           None if host(ga[0][1])[i] else host(ga[0][0])[i].item())
+                          for i in range(g)], key=lambda r: (r[0] is not None, r[0] or 0))
+            exp = sorted([tuple(p) for p in case["expected"]], key=lambda r: (r[0] is not None, r[0] or 0))
+            assert got == exp, case["test"]
+        ran += 1
+    assert ran >= 50
+
+
+def test_groupby_ghive_golden_numeric(ctx):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ghive_groupby.json")) as f:
+        cases = json.load(f)["cases"]
+    for case in cases:
+        if any(case["columns"][k][0] == "string" for k in case["keys"]):
+            continue
+        cols = [np.array(c[1], dtype={"long": np.int64, "double": np.float64, "int": np.int32}[c[0]])
+                for c in case["columns"]]
+        aggs = [(abi.AGG_NAMES[t.lower()], c) for t, c in case["aggs"]]
+        gk, ga, g = ctx.filter_groupby(None, [dev(c) for c in cols], case["keys"], aggs, capacity=64,
+                                       max_groups=32)
+        rows = sorted(tuple(("%f" % host(v)[i]) if t == abi.DOUBLE else str(host(v)[i])
+                            for (v, _), t in zip(gk + ga, case["expected_types"])) for i in range(g))
+        assert rows == sorted(tuple(r) for r in case["expected_rows"]), case["test"]
+
+
+def test_groupby_repeat_is_stable(ctx):
+    cols = workloads.fact_table(200_000, seed_idx=13)
+    dc = [dev(c) for c in cols]
+    first = None
+    for _ in range(20):
+        gk, ga, g = ctx.filter_groupby(workloads.fact_predicate(), dc, [0], workloads.AGGS_FACT,
+                                       capacity=1000, max_groups=1000)
+        rows = _norm_rows([(host(v), host(nl)) for v, nl in gk], [(host(v), host(nl)) for v, nl in ga])
+        if first is None:
+            first = rows
+        else:
+            for a, b in zip(first, rows):
+                assert a[:3] == b[:3] and a[5:] == b[5:]
+                assert abs(a[3] - b[3]) <= REL_TOL * abs(a[3])
+
+
+# ------------------------------------------------------------------- join
+def _check_join(ctx, bkey, pkey, jt=abi.INNER_JOIN, bpay=(), ppay=()):
+    pr, br = oracle.hash_join(bkey, pkey, jt)
+    t = ctx.join_build(dev(bkey))
+    r = ctx.join_probe(t, dev(pkey), jt, build_payload=[dev(c) for c in bpay],
+                       probe_payload=[dev(c) for c in ppay])
+    assert r["rows"] == len(pr)
+    gp, gb = host(r["probe_rowid"]), host(r["build_rowid"])
+    assert np.all(np.diff(gp) >= 0)  # probe-row order
+    assert sorted(zip(gp.tolist(), gb.tolist())) == sorted(zip(pr.tolist(), br.tolist()))
+    for c, (v, nl) in zip(bpay, r["build"]):
+        hv, hn = host(v), host(nl)
+        ok = gb >= 0
+        assert np.array_equal(hv[ok], c[gb[ok]])
+        assert np.all(hn[~ok])
+    for c, (v, _) in zip(ppay, r["probe"]):
+        assert np.array_equal(host(v), c[gp])
+    t.free()
+    return r
+
+
+@pytest.mark.parametrize("n", EDGE_SIZES)
+def test_join_edge_sizes(ctx, n):
+    g = np.random.default_rng(n + 3)
+    nb = max(1, n // 3)
+    bkey = g.permutation(np.arange(1, nb + 1, dtype=np.int64))
+    pkey = g.integers(0, 2 * nb + 2, n, dtype=np.int64)
+    _check_join(ctx, bkey, pkey, bpay=[g.integers(0, 1 << 62, nb, dtype=np.int64), g.random(nb)])
+
+
+def test_join_config_shape_small(ctx):
+    (bkey, bpay), (fk, ppay) = workloads.join_tables(15_000, 600_000, seed_idx=21)
+    _check_join(ctx, bkey, fk, bpay=bpay, ppay=[ppay])
+
+
+def test_join_duplicates_semi_outer_nulls(ctx):
+    g = np.random.default_rng(22)
+    bkey = g.integers(-50, 50, 5000, dtype=np.int64)  # heavy duplicates
+    pkey = g.integers(-80, 80, 40_000, dtype=np.int64)
+    pay = g.integers(0, 1000, 5000, dtype=np.int64)
+    for jt in (abi.INNER_JOIN, abi.LEFT_SEMI_JOIN, abi.LEFT_OUTER_JOIN):
+        _check_join(ctx, bkey, pkey, jt, bpay=[pay] if jt != abi.LEFT_SEMI_JOIN else ())
+    i64 = np.iinfo(np.int64)
+    bkey2 = np.array([i64.min, 5, i64.max - 1, 7, i64.min], dtype=np.int64)
+    pkey2 = np.array([i64.min, 7, 8, i64.max - 1, i64.min, 5], dtype=np.int64)
+    _check_join(ctx, bkey2, pkey2)
+
+
+def test_join_null_keys_never_match(ctx):
+    g = np.random.default_rng(23)
+    bkey = np.arange(1000, dtype=np.int64)
+    bnull = g.random(1000) < 0.2
+    pkey = g.integers(0, 1000, 20_000, dtype=np.int64)
+    pnull = g.random(20_000) < 0.2
+    pr, br = oracle.hash_join((bkey, bnull), (pkey, pnull))
+    t = ctx.join_build((dev(bkey), dev(bnull.astype(np.uint8))))
+    r = ctx.join_probe(t, (dev(pkey), dev(pnull.astype(np.uint8))))
+    assert r["rows"] == len(pr)
+    assert sorted(zip(host(r["probe_rowid"]).tolist(), host(r["build_rowid"]).tolist())) == \
+        sorted(zip(pr.tolist(), br.tolist()))
+
+
+def test_join_ghive_semi_outer_chain(ctx):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ghive_join.json")) as f:
+        case = json.load(f)["cases"][0]
+    tabs = [np.array(t, dtype=np.int64) for t in case["tables"]]
+    jt_map = {"LEFT_SEMI_JOIN": abi.LEFT_SEMI_JOIN, "LEFT_OUTER_JOIN": abi.LEFT_OUTER_JOIN}
+    tuples = [(i,) for i in range(len(tabs[0]))]
+    for name, left, right in case["join_types"]:
+        rows = np.array([t[0] for t in tuples], dtype=np.int64)
+        t = ctx.join_build(dev(tabs[right]))
+        r = ctx.join_probe(t, dev(tabs[0][rows]), jt_map[name])
+        pr, br = host(r["probe_rowid"]), host(r["build_rowid"])
+        if jt_map[name] == abi.LEFT_SEMI_JOIN:
+            tuples = [tuples[p] for p in pr]
+        else:
+            tuples = [tuples[p] + (int(b),) for p, b in zip(pr, br)]
+        t.free()
+    exp = case["expected_offsets"]
+    w = len(tuples[0])
+    assert sorted(tuples) == sorted(tuple(exp[i:i + w]) for i in range(0, len(exp), w))
+
+
+# ------------------------------------------------------------------- sort
+def _check_sort(ctx, keys, orders=None, null_orders=None, payload=(), rowid=True):
+    perm = oracle.sort_perm([oracle_col(k) for k in keys], orders, null_orders)
+    ok, op, rid = ctx.sort([devcol(k) for k in keys], orders, null_orders,
+                           payload=[dev(p) for p in payload], rowid=rowid)
+    if rowid:
+        assert np.array_equal(host(rid), perm)
+    for k, (v, nl) in zip(keys, ok):
+        vals, isnull = (k if isinstance(k, tuple) else (k, None))
+        hv = host(v)
+        if isnull is not None:
+            assert np.array_equal(host(nl), isnull[perm])
+            m = ~isnull[perm]
+            assert np.array_equal(hv[m].view(np.uint8) if hv.dtype == np.float64 else hv[m],
+                                  vals[perm][m].view(np.uint8) if hv.dtype == np.float64 else vals[perm][m])
+        else:
+            assert np.array_equal(hv.view(np.uint8) if hv.dtype == np.float64 else hv,
+                                  vals[perm].view(np.uint8) if hv.dtype == np.float64 else vals[perm])
+    for p, (v, _) in zip(payload, op):
+        assert np.array_equal(host(v), p[perm])
+
+
+@pytest.mark.parametrize("n", EDGE_SIZES[1:])
+def test_sort_edge_sizes(ctx, n):
+    d, k, rowid = workloads.sort_table(n, seed_idx=30 + n % 11)
+    _check_sort(ctx, [d, k], payload=[rowid], rowid=False)
+    _check_sort(ctx, [d, k], rowid=True)
+
+
+def test_sort_config_shape_and_zipf(ctx):
+    for z in (False, True):
+        d, k, rowid = workloads.sort_table(300_000, zipf=z, seed_idx=31)
+        _check_sort(ctx, [d, k], payload=[rowid], rowid=False)
+
+
+def test_sort_desc_nulls_doubles(ctx):
+    g = np.random.default_rng(33)
+    n = 60_000
+    a = g.integers(-3, 3, n, dtype=np.int32)
+    an = g.random(n) < 0.1
+    x = g.choice(np.array([-np.inf, -1.5, -0.0, 0.0, 2.5, np.inf, 1e-300]), n)
+    xn = g.random(n) < 0.1
+    for orders in ([abi.ASC, abi.DESC], [abi.DESC, abi.ASC]):
+        for nulls in ([abi.NULLS_DEFAULT] * 2, [abi.NULLS_LAST, abi.NULLS_FIRST]):
+            _check_sort(ctx, [(a, an), (x, xn)], orders, nulls)
+    i64 = np.iinfo(np.int64)
+    big = g.choice(np.array([i64.min, i64.max, 0, -1, 1], dtype=np.int64), n)
+    _check_sort(ctx, [big], [abi.DESC])
+
+
+def test_sort_all_equal_and_wide_key_rejected(ctx):
+    from ghive_b200._lib import GhbError
+    n = 10_000
+    same = np.full(n, 42, dtype=np.int64)
+    _check_sort(ctx, [same], payload=[np.arange(n, dtype=np.int32)], rowid=False)
+    g = np.random.default_rng(34)
+    wide = [g.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64),
+            g.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64)]
+    with pytest.raises(GhbError) as e:
+        ctx.sort([dev(w) for w in wide])
+    assert e.value.code == abi.ERR_UNSUPPORTED
+
+
+# ------------------------------------------------------- host entry points
+def test_host_entry_points_match_device(ctx):
+    cols = workloads.fact_table(100_000, seed_idx=40)
+    gk, ga, g = ctx.filter_groupby_host(workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT,
+                                        capacity=1000, max_groups=1000)
+    ok, oa = oracle.filter_groupby(workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT)
+    assert g == 1000
+    got = _norm_rows(gk, ga)
+    exp = _norm_rows(ok, oa)
+    for a, b in zip(got, exp):
+        assert a[:3] == b[:3] and a[5:] == b[5:]
+        assert abs(a[3] - b[3]) <= REL_TOL * abs(b[3])
+    outs, k = ctx.filter_host(workloads.fact_predicate(), cols)
+    sel = oracle.filter_rows(workloads.fact_predicate(), cols)
+    assert k == len(sel) and np.array_equal(outs[3][0], cols[3][sel])
+    (bkey, bpay), (fk, ppay) = workloads.join_tables(10_000, 200_000, seed_idx=41)
+    r = ctx.hash_join_host(bkey, fk, build_payload=bpay, probe_payload=[ppay])
+    pr, br = oracle.hash_join(bkey, fk)
+    assert r["rows"] == len(pr)
+    assert np.array_equal(r["probe_rowid"], pr) and np.array_equal(r["build_rowid"], br)
+    assert np.array_equal(r["build"][0][0], bpay[0][br])
+    d, k2, rowid = workloads.sort_table(100_000, seed_idx=42)
+    okk, opp, _ = ctx.sort_host([d, k2], payload=[rowid])
+    perm = oracle.sort_perm([d, k2])
+    assert np.array_equal(opp[0][0], rowid[perm]) and np.array_equal(okk[1][0], k2[perm])
