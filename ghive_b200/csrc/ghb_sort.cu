@@ -1,4 +1,4 @@
-// ghb_sort.cu — stable ORDER BY sort (S1): LSD radix sort on a packed key.
+// ghb_sort.cu — stable ORDER BY sort (S1): LSD radix sort on packed keys.
 //
 // Replaces the Sink sort of the reference (gpu_impl/src/Operator/
 // SinkOperator.cu:153-286: H2D of the key columns, thrust::sort of row
@@ -9,22 +9,25 @@
 // NULLS FIRST/LAST; ties keep input order (LSD radix sort is stable).
 //
 // Pipeline (one call):
-//   1. analyse  one read of the key columns: per key the min/max of its
-//               order image and whether it holds NULLs;
-//   2. plan     (host) each key becomes a bit field [null bit][value - min]
-//               of just the width its range needs; the fields are packed
-//               most-significant-key-first into one 64-bit word;
-//   3. histogram one read: 8-bit digit histograms of every pass at once;
-//               passes whose digit is constant are skipped;
-//   4. passes   onesweep-style: each CTA claims a tile, ranks its keys by
-//               digit with warp ballots (stable), gets each digit's global
-//               offset by decoupled look-back over earlier tiles, reorders
-//               the tile in shared memory and writes runs per digit.  The
-//               first pass reads the user's columns and packs on the fly; the
-//               last pass unpacks straight into the user's output columns.
-// The carried value is the payload itself when there is one payload column
-// and no permutation is asked for, else the row index (payloads are then
-// gathered in the last pass).
+//   1. analyse   one read of the key columns: per key the min/max of its
+//                order image and whether it holds NULLs;
+//   2. plan      (host) each key becomes sub-fields [null flag][value - min]
+//                of just the width its range needs, packed least-significant
+//                key first into 64-bit segments;
+//   3. histogram one read per segment: 8-bit digit histograms of all of the
+//                segment's passes at once; passes whose digit is constant are
+//                skipped;
+//   4. passes    onesweep-style: each CTA claims a tile, ranks its keys by
+//                digit with warp ballots (stable), gets each digit's global
+//                offset by decoupled look-back over earlier tiles, reorders
+//                the tile in shared memory and writes one run per digit.
+// A one-segment key (the common case, e.g. (int32 d, int64 k) with the ranges
+// of the sort workload) is packed by the first pass straight from the user's
+// columns and unpacked by the last pass straight into the output columns; the
+// value carried with it is the single payload column, or the row index.  A
+// key wider than 64 bits is sorted segment by segment (least significant
+// first), each later segment packed from the row order the previous one left,
+// and the output is gathered by the final row order.
 #include <algorithm>
 #include <vector>
 
@@ -37,49 +40,89 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   // 4096
 constexpr int kDigitBits = 8;
 constexpr int kBins = 1 << kDigitBits;
-constexpr int kMaxPasses = 8;
+constexpr int kMaxPasses = 8;                          // per 64-bit segment
 constexpr int kMaxSortKeys = 8;
 constexpr int kMaxSortPay = 8;
-constexpr uint32_t kSFlagA = 1u << 30, kSFlagP = 2u << 30, kSCount = (1u << 30) - 1;
+constexpr int kMaxSub = 2 * kMaxSortKeys;
+constexpr int kMaxSeg = kMaxSub;
 
 struct KeyField {
   ghb_column col;
   int32_t desc;
   int32_t nulls_first;
-  int32_t has_null_bit;  // field carries a null flag above its value bits
+  int32_t has_null;      // the column holds NULLs: the key has a flag sub-field
   int32_t vbits;         // value bits
-  int32_t shift;         // position of the field's lowest bit in the packed key
   uint64_t umin;         // min of the (possibly inverted) order image
 };
 
-struct SortLayout {
+struct SubField {
+  int8_t key;
+  int8_t is_flag;        // 1: the NULL flag, 0: the value bits
+  int8_t bits;
+  int8_t shift;          // within the segment word
+};
+
+struct Segment {
+  int32_t n;
+  int32_t bits;
+  SubField f[kMaxSub];
+};
+
+struct KeySet {
   int32_t nkeys;
-  KeyField f[kMaxSortKeys];
+  KeyField k[kMaxSortKeys];
 };
 
 __device__ __forceinline__ uint64_t key_image(const ghb_column& c, int64_t raw) {
   return c.type == GHB_DOUBLE ? flip_f64_bits((uint64_t)raw) : flip_i64(raw);
 }
 
+// Contribution of one sub-field for row r (value already shifted into place).
+__device__ __forceinline__ uint64_t sub_bits(const KeySet& K, const SubField& sf, int64_t r) {
+  const KeyField& kf = K.k[sf.key];
+  int64_t raw = ld_raw(kf.col, r);
+  bool null = kf.has_null && raw_is_null(kf.col, raw, r);
+  uint64_t v;
+  if (sf.is_flag) {
+    v = (null == (bool)kf.nulls_first) ? 0 : 1;   // NULLS FIRST: null 0 / value 1
+  } else {
+    uint64_t u = key_image(kf.col, raw);
+    if (kf.desc) u = ~u;
+    v = null ? 0 : u - kf.umin;
+  }
+  return v << sf.shift;
+}
+
 // ---------------------------------------------------------------- analyse
 struct MinMaxParams {
-  SortLayout L;
+  KeySet K;
   int64_t n;
   unsigned long long* out;  // per key: [0] min image, [1] max image, [2] any NULL
 };
 
 __global__ void __launch_bounds__(256) sort_minmax_kernel(MinMaxParams p) {
-  for (int j = 0; j < p.L.nkeys; j++) {
-    const KeyField& f = p.L.f[j];
+  constexpr int U = 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int j = 0; j < p.K.nkeys; j++) {
+    const KeyField& f = p.K.k[j];
     unsigned long long mn = ~0ull, mx = 0, anynull = 0;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < p.n;
-         r += (int64_t)gridDim.x * blockDim.x) {
-      int64_t raw = ld_raw(f.col, r);
-      if (raw_is_null(f.col, raw, r)) { anynull = 1; continue; }
-      uint64_t u = key_image(f.col, raw);
-      if (f.desc) u = ~u;
-      mn = min(mn, (unsigned long long)u);
-      mx = max(mx, (unsigned long long)u);
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < p.n; base += U * stride) {
+      int64_t raw[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        int64_t r = base + u * stride;
+        raw[u] = r < p.n ? ld_raw(f.col, r) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        int64_t r = base + u * stride;
+        if (r >= p.n) continue;
+        if (f.col.null_mode != GHB_NULLS_NONE && raw_is_null(f.col, raw[u], r)) { anynull = 1; continue; }
+        uint64_t img = key_image(f.col, raw[u]);
+        if (f.desc) img = ~img;
+        mn = min(mn, (unsigned long long)img);
+        mx = max(mx, (unsigned long long)img);
+      }
     }
     for (int o = 16; o > 0; o >>= 1) {
       mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
@@ -94,42 +137,37 @@ __global__ void __launch_bounds__(256) sort_minmax_kernel(MinMaxParams p) {
   }
 }
 
-// Packed key of row r.
-__device__ __forceinline__ uint64_t pack_row(const SortLayout& L, int64_t r) {
-  uint64_t k = 0;
-  for (int j = 0; j < L.nkeys; j++) {
-    const KeyField& f = L.f[j];
-    int64_t raw = ld_raw(f.col, r);
-    uint64_t field;
-    if (f.col.null_mode != GHB_NULLS_NONE && raw_is_null(f.col, raw, r)) {
-      field = f.nulls_first ? 0 : (1ull << f.vbits);   // value bits 0
-    } else {
-      uint64_t u = key_image(f.col, raw);
-      if (f.desc) u = ~u;
-      field = u - f.umin;
-      if (f.has_null_bit && f.nulls_first) field |= 1ull << f.vbits;
-    }
-    k |= field << f.shift;
-  }
-  return k;
-}
-
 // ---------------------------------------------------------------- histogram
 struct HistParams {
-  SortLayout L;
+  KeySet K;
+  Segment seg;
   int64_t n;
   int32_t npasses;
   uint32_t* hist;  // [npasses][kBins]
 };
 
 __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
+  constexpr int U = 4;
   __shared__ uint32_t sh[kMaxPasses][kBins];
   for (int i = threadIdx.x; i < kMaxPasses * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < p.n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t k = pack_row(p.L, r);
-    for (int q = 0; q < p.npasses; q++) atomicAdd(&sh[q][(k >> (q * kDigitBits)) & (kBins - 1)], 1u);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < p.n; base += U * stride) {
+    uint64_t k[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) k[u] = 0;
+    for (int i = 0; i < p.seg.n; i++) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        int64_t r = base + u * stride;
+        if (r < p.n) k[u] |= sub_bits(p.K, p.seg.f[i], r);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (base + u * stride >= p.n) continue;
+      for (int q = 0; q < p.npasses; q++) atomicAdd(&sh[q][(k[u] >> (q * kDigitBits)) & (kBins - 1)], 1u);
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < p.npasses * kBins; i += blockDim.x) {
@@ -139,90 +177,110 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
 }
 
 // ---------------------------------------------------------------- passes
+enum SrcMode { kSrcPacked = 0, kSrcCols = 1, kSrcPerm = 2 };
+enum DstMode { kDstPacked = 0, kDstDecode = 1, kDstGather = 2 };
+
 struct PassParams {
-  SortLayout L;
+  KeySet K;
+  Segment seg;
   int64_t n;
   int64_t ntiles;
   int32_t shift;
   int32_t carry_rowid;       // value = row index (else the single payload's raw bits)
-  // packed buffers
   const uint64_t* keys_in;
-  const uint64_t* vals_in;
+  const void* vals_in;
   uint64_t* keys_out;
-  uint64_t* vals_out;
-  // first pass source
+  void* vals_out;
   ghb_column pay_src;        // single carried payload (when !carry_rowid)
-  // last pass destination
   ghb_out_column out_keys[kMaxSortKeys];
   int32_t npay;
   ghb_column pay[kMaxSortPay];
   ghb_out_column out_pay[kMaxSortPay];
   int32_t* out_rowid;
   uint32_t digit_base[kBins];  // exclusive global offset of each digit
-  uint32_t* status;           // [ntiles][kBins]
+  uint64_t* status;            // [ntiles][kBins] epoch-tagged look-back words
+  uint32_t epoch;
   unsigned long long* counters;
   int32_t* dev_status;
 };
 
-__device__ __forceinline__ void unpack_write(const PassParams& p, uint64_t k, uint64_t v, int64_t pos) {
-  for (int j = 0; j < p.L.nkeys; j++) {
-    const KeyField& f = p.L.f[j];
-    uint64_t field = (k >> f.shift);
-    uint64_t vmask = f.vbits >= 64 ? ~0ull : ((1ull << f.vbits) - 1);
+__device__ __forceinline__ void write_raw(const ghb_out_column& o, int64_t pos, int type, int64_t raw,
+                                          bool null) {
+  if (null) {
+    if (o.is_null) o.is_null[pos] = 1;
+    if (type == GHB_INT) ((int32_t*)o.data)[pos] = INT32_MAX;
+    else if (type == GHB_LONG) ((int64_t*)o.data)[pos] = INT64_MAX;
+    else ((long long*)o.data)[pos] = 0x7ff8000000000000ll;
+    return;
+  }
+  if (type == GHB_INT) ((int32_t*)o.data)[pos] = (int32_t)raw;
+  else ((long long*)o.data)[pos] = raw;
+  if (o.is_null) o.is_null[pos] = 0;
+}
+
+// Copies keys and payloads of input row `row` to output position `pos`.
+__device__ __forceinline__ void gather_write(const PassParams& p, int64_t row, int64_t pos) {
+  for (int j = 0; j < p.K.nkeys; j++) {
+    const ghb_column& c = p.K.k[j].col;
+    int64_t raw = ld_raw(c, row);
+    write_raw(p.out_keys[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row));
+  }
+  if (p.out_rowid) p.out_rowid[pos] = (int32_t)row;
+  for (int j = 0; j < p.npay; j++) {
+    const ghb_column& c = p.pay[j];
+    int64_t raw = ld_raw(c, row);
+    write_raw(p.out_pay[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row));
+  }
+}
+
+// Unpacks a one-segment key (and the carried value) to output position `pos`.
+__device__ __forceinline__ void decode_write(const PassParams& p, uint64_t k, uint64_t v, int64_t pos) {
+  for (int j = 0; j < p.K.nkeys; j++) {
+    const KeyField& kf = p.K.k[j];
+    uint64_t field = 0;
     bool null = false;
-    if (f.has_null_bit) {
-      bool flag = (field >> f.vbits) & 1ull;
-      null = f.nulls_first ? !flag : flag;
+    for (int i = 0; i < p.seg.n; i++) {
+      const SubField& sf = p.seg.f[i];
+      if (sf.key != j) continue;
+      uint64_t bits = (k >> sf.shift) & (sf.bits >= 64 ? ~0ull : ((1ull << sf.bits) - 1));
+      if (sf.is_flag) null = (bits == 0) == (bool)kf.nulls_first;
+      else field = bits;
     }
-    const ghb_out_column& o = p.out_keys[j];
-    if (null) {
-      if (o.is_null) o.is_null[pos] = 1;
-      if (o.type == GHB_INT) ((int32_t*)o.data)[pos] = INT32_MAX;
-      else if (o.type == GHB_LONG) ((int64_t*)o.data)[pos] = INT64_MAX;
-      else ((long long*)o.data)[pos] = 0x7ff8000000000000ll;
-      continue;
-    }
-    uint64_t u = (field & vmask) + f.umin;
-    if (f.desc) u = ~u;
-    int64_t raw = f.col.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(u) : (int64_t)(u ^ 0x8000000000000000ull);
-    if (o.type == GHB_INT) ((int32_t*)o.data)[pos] = (int32_t)raw;
-    else ((long long*)o.data)[pos] = raw;
-    if (o.is_null) o.is_null[pos] = 0;
+    uint64_t u = field + kf.umin;
+    if (kf.desc) u = ~u;
+    int64_t raw = kf.col.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(u) : (int64_t)(u ^ 0x8000000000000000ull);
+    write_raw(p.out_keys[j], pos, kf.col.type, raw, null);
   }
   if (p.carry_rowid) {
     int64_t row = (int64_t)v;
     if (p.out_rowid) p.out_rowid[pos] = (int32_t)row;
     for (int j = 0; j < p.npay; j++) {
       const ghb_column& c = p.pay[j];
-      const ghb_out_column& o = p.out_pay[j];
       int64_t raw = ld_raw(c, row);
-      if (c.type == GHB_INT) ((int32_t*)o.data)[pos] = (int32_t)raw;
-      else ((long long*)o.data)[pos] = raw;
-      if (o.is_null) o.is_null[pos] = (c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row)) ? 1 : 0;
+      write_raw(p.out_pay[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row));
     }
   } else if (p.npay == 1) {
-    const ghb_out_column& o = p.out_pay[0];
-    if (p.pay[0].type == GHB_INT) ((int32_t*)o.data)[pos] = (int32_t)v;
-    else ((unsigned long long*)o.data)[pos] = v;
-    if (o.is_null) {
-      const ghb_column& c = p.pay[0];
-      o.is_null[pos] = (c.null_mode == GHB_NULLS_SENTINEL && raw_is_null(c, (int64_t)v, 0)) ? 1 : 0;
-    }
+    const ghb_column& c = p.pay[0];
+    bool null = c.null_mode == GHB_NULLS_SENTINEL && raw_is_null(c, (int64_t)v, 0);
+    write_raw(p.out_pay[0], pos, c.type, (int64_t)v, null);
   }
 }
 
-template <bool FIRST, bool LAST>
+template <typename V, int SRC, int DST>
 __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
   __shared__ uint32_t s_whist[kSortThreads / 32][kBins];  // per-warp counts, then exclusive over warps
   __shared__ uint32_t s_bexcl[kBins];                      // block-local exclusive offset per digit
   __shared__ uint64_t s_gbase[kBins];                      // global destination of each digit's run
+  __shared__ uint32_t s_wsum[kSortThreads / 32];
+  __shared__ int64_t s_tile;
   extern __shared__ uint64_t s_dyn[];                      // reordered tile: keys, then values
   uint64_t* s_keys = s_dyn;
-  uint64_t* s_vals = s_dyn + kSortTile;
-  __shared__ int64_t s_tile;
+  V* s_vals = (V*)(s_dyn + kSortTile);
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
+  const V* vals_in = (const V*)p.vals_in;
+  V* vals_out = (V*)p.vals_out;
 
   while (true) {
     if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&p.counters[0], 1ull);
@@ -232,21 +290,47 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
     if (tile >= p.ntiles) break;
     const int64_t wbase = tile * kSortTile + (int64_t)warp * (32 * kSortItems);
 
-    uint64_t key[kSortItems], val[kSortItems];
-    uint32_t rank[kSortItems];
+    uint64_t key[kSortItems];
+    V val[kSortItems];
+    if (SRC == kSrcPacked) {
 #pragma unroll
-    for (int k = 0; k < kSortItems; k++) {
-      int64_t row = wbase + k * 32 + lane;
-      bool live = row < p.n;
-      if (FIRST) {
-        key[k] = live ? pack_row(p.L, row) : ~0ull;
-        val[k] = p.carry_rowid ? (uint64_t)row : (live ? (uint64_t)ld_raw(p.pay_src, row) : 0);
-      } else {
-        key[k] = live ? p.keys_in[row] : ~0ull;
-        val[k] = live ? p.vals_in[row] : 0;
+      for (int k = 0; k < kSortItems; k++) {
+        int64_t row = wbase + k * 32 + lane;
+        key[k] = row < p.n ? __ldcs((const unsigned long long*)p.keys_in + row) : ~0ull;
+      }
+#pragma unroll
+      for (int k = 0; k < kSortItems; k++) {
+        int64_t row = wbase + k * 32 + lane;
+        val[k] = row < p.n ? vals_in[row] : (V)0;
+      }
+    } else {
+      int64_t src[kSortItems];
+#pragma unroll
+      for (int k = 0; k < kSortItems; k++) {
+        int64_t row = wbase + k * 32 + lane;
+        key[k] = 0;
+        if (SRC == kSrcPerm) src[k] = row < p.n ? (int64_t)vals_in[row] : 0;
+        else src[k] = row;
+      }
+      // one sub-field at a time over all items: the loads are independent
+      for (int i = 0; i < p.seg.n; i++) {
+        const SubField sf = p.seg.f[i];
+#pragma unroll
+        for (int k = 0; k < kSortItems; k++) {
+          int64_t row = wbase + k * 32 + lane;
+          if (row < p.n) key[k] |= sub_bits(p.K, sf, src[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kSortItems; k++) {
+        int64_t row = wbase + k * 32 + lane;
+        if (row >= p.n) key[k] = ~0ull;
+        if (p.carry_rowid) val[k] = (V)src[k];
+        else val[k] = row < p.n ? (V)ld_raw(p.pay_src, row) : (V)0;
       }
     }
     // stable rank of each key among the warp's keys with the same digit
+    uint32_t rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; k++) {
       int64_t row = wbase + k * 32 + lane;
@@ -266,34 +350,32 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
     }
     __syncthreads();
     // per digit (one thread each): exclusive over warps, block total
+    const int d = threadIdx.x;  // kSortThreads == kBins
     uint32_t total = 0;
-    {
-      const int d = threadIdx.x;  // kSortThreads == kBins
 #pragma unroll
-      for (int w = 0; w < kSortThreads / 32; w++) {
-        uint32_t c = s_whist[w][d];
-        s_whist[w][d] = total;
-        total += c;
-      }
+    for (int w = 0; w < kSortThreads / 32; w++) {
+      uint32_t c = s_whist[w][d];
+      s_whist[w][d] = total;
+      total += c;
     }
     // publish this tile's count of digit d, then look back for its prefix
     {
-      const int d = threadIdx.x;
-      uint32_t* st = p.status + tile * kBins;
+      uint64_t* st = p.status + tile * kBins;
       uint64_t excl = 0;
       if (tile == 0) {
-        atomicExch(&st[d], kSFlagP | total);
+        lb_store(&st[d], lb_pack(p.epoch, kFlagPrefix, total));
       } else {
-        atomicExch(&st[d], kSFlagA | total);
+        lb_store(&st[d], lb_pack(p.epoch, kFlagAgg, total));
         int64_t t = tile - 1;
         int spins = 0;
         while (t >= 0) {
-          uint32_t v = *(volatile uint32_t*)&p.status[t * kBins + d];
-          if (v & kSFlagP) { excl += v & kSCount; break; }
-          if (v & kSFlagA) { excl += v & kSCount; t--; continue; }
+          uint64_t v = lb_load(&p.status[t * kBins + d]);
+          bool ok = ((v >> kEpochShift) & kEpochMask) == (p.epoch & kEpochMask);
+          if (ok && (v & kFlagPrefix)) { excl += v & kCountMask; break; }
+          if (ok && (v & kFlagAgg)) { excl += v & kCountMask; t--; continue; }
           if (++spins > kSpinLimit) { raise_status(p.dev_status, kDevTimeout); break; }
         }
-        atomicExch(&st[d], kSFlagP | (uint32_t)((excl + total) & kSCount));
+        lb_store(&st[d], lb_pack(p.epoch, kFlagPrefix, excl + total));
       }
       s_gbase[d] = (uint64_t)p.digit_base[d] + excl;
     }
@@ -304,7 +386,6 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
         uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
       }
-      __shared__ uint32_t s_wsum[kSortThreads / 32];
       if (lane == 31) s_wsum[warp] = incl;
       __syncthreads();
       if (warp == 0) {
@@ -317,7 +398,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
         if (lane < kSortThreads / 32) s_wsum[lane] = x - v;
       }
       __syncthreads();
-      s_bexcl[threadIdx.x] = s_wsum[warp] + incl - total;
+      s_bexcl[d] = s_wsum[warp] + incl - total;
     }
     __syncthreads();
     // scatter into shared memory in digit order (stable)
@@ -325,8 +406,8 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
     for (int k = 0; k < kSortItems; k++) {
       int64_t row = wbase + k * 32 + lane;
       if (row >= p.n) continue;
-      uint32_t d = (uint32_t)(key[k] >> p.shift) & (kBins - 1);
-      uint32_t at = s_bexcl[d] + s_whist[warp][d] + rank[k];
+      uint32_t dk = (uint32_t)(key[k] >> p.shift) & (kBins - 1);
+      uint32_t at = s_bexcl[dk] + s_whist[warp][dk] + rank[k];
       s_keys[at] = key[k];
       s_vals[at] = val[k];
     }
@@ -335,13 +416,15 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
     const int64_t tile_n = min((int64_t)kSortTile, p.n - tile * kSortTile);
     for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
       uint64_t k = s_keys[i];
-      uint32_t d = (uint32_t)(k >> p.shift) & (kBins - 1);
-      int64_t pos = (int64_t)(s_gbase[d] + (i - s_bexcl[d]));
-      if (LAST) {
-        unpack_write(p, k, s_vals[i], pos);
+      uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
+      int64_t pos = (int64_t)(s_gbase[dk] + (i - s_bexcl[dk]));
+      if (DST == kDstDecode) {
+        decode_write(p, k, (uint64_t)s_vals[i], pos);
+      } else if (DST == kDstGather) {
+        gather_write(p, (int64_t)s_vals[i], pos);
       } else {
-        p.keys_out[pos] = k;
-        p.vals_out[pos] = s_vals[i];
+        __stcs((unsigned long long*)p.keys_out + pos, (unsigned long long)k);
+        vals_out[pos] = s_vals[i];
       }
     }
     __syncthreads();
@@ -357,27 +440,121 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
   }
 }
 
-// Identity pass for an input whose packed keys are all equal (or n <= 1):
-// copies keys and payloads in input order.
-__global__ void sort_copy_kernel(PassParams p) {
+// Output in input order (keys all equal, or n tiny): gathers row r to r, or
+// row perm[r] to r when a permutation is given.
+template <typename V>
+__global__ void sort_identity_kernel(PassParams p, const V* perm) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < p.n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t k = pack_row(p.L, r);
-    uint64_t v = p.carry_rowid ? (uint64_t)r : (uint64_t)ld_raw(p.pay_src, r);
-    unpack_write(p, k, v, r);
-  }
+       r += (int64_t)gridDim.x * blockDim.x)
+    gather_write(p, perm ? (int64_t)perm[r] : r, r);
 }
+
+static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Scratch needed by sort_impl for n rows.
 size_t sort_scratch_bytes(int64_t n) {
   int64_t ntiles = (n + kSortTile - 1) / kSortTile;
   size_t b = 0;
-  b += 2 * (((size_t)n * 8 + 255) & ~(size_t)255);       // keys ping-pong
-  b += 2 * (((size_t)n * 8 + 255) & ~(size_t)255);       // values ping-pong
-  b += (size_t)kMaxPasses * ntiles * kBins * 4 + 256;    // look-back status
-  b += (size_t)kMaxPasses * kBins * 4 + 256;             // histograms
-  b += 3 * 8 * kMaxSortKeys + 256;                       // min/max
+  b += 2 * align256((size_t)n * 8);                        // keys ping-pong
+  b += 2 * align256((size_t)n * 8);                        // values ping-pong
+  b += align256((size_t)ntiles * kBins * 8);               // look-back status
+  b += align256((size_t)kMaxSeg * kMaxPasses * kBins * 4); // histograms
+  b += align256(3 * 8 * kMaxSortKeys);                     // min/max
   return b + 4096;
+}
+
+template <typename V>
+static void launch_pass(int src, int dst, int grid, size_t dyn, cudaStream_t s, const PassParams& pp) {
+#define GHB_PASS(S, D) sort_pass_kernel<V, S, D><<<grid, kSortThreads, dyn, s>>>(pp)
+  if (src == kSrcPacked && dst == kDstPacked) GHB_PASS(kSrcPacked, kDstPacked);
+  else if (src == kSrcPacked && dst == kDstDecode) GHB_PASS(kSrcPacked, kDstDecode);
+  else if (src == kSrcPacked && dst == kDstGather) GHB_PASS(kSrcPacked, kDstGather);
+  else if (src == kSrcCols && dst == kDstPacked) GHB_PASS(kSrcCols, kDstPacked);
+  else if (src == kSrcCols && dst == kDstDecode) GHB_PASS(kSrcCols, kDstDecode);
+  else if (src == kSrcCols && dst == kDstGather) GHB_PASS(kSrcCols, kDstGather);
+  else if (src == kSrcPerm && dst == kDstPacked) GHB_PASS(kSrcPerm, kDstPacked);
+  else if (src == kSrcPerm && dst == kDstGather) GHB_PASS(kSrcPerm, kDstGather);
+#undef GHB_PASS
+}
+
+template <typename V>
+static int32_t set_smem(ghb_ctx* ctx, size_t dyn) {
+#define GHB_ATTR(S, D) \
+  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<V, S, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn))
+  GHB_ATTR(kSrcPacked, kDstPacked);
+  GHB_ATTR(kSrcPacked, kDstDecode);
+  GHB_ATTR(kSrcPacked, kDstGather);
+  GHB_ATTR(kSrcCols, kDstPacked);
+  GHB_ATTR(kSrcCols, kDstDecode);
+  GHB_ATTR(kSrcCols, kDstGather);
+  GHB_ATTR(kSrcPerm, kDstPacked);
+  GHB_ATTR(kSrcPerm, kDstGather);
+#undef GHB_ATTR
+  return GHB_OK;
+}
+
+template <typename V>
+static int32_t run_passes(ghb_ctx* ctx, PassParams& pp, const std::vector<Segment>& segs,
+                          const std::vector<std::vector<int>>& run, const std::vector<uint32_t>& hist,
+                          cudaStream_t stream) {
+  int32_t st;
+  const int64_t n = pp.n;
+  int total = 0;
+  for (auto& r : run) total += (int)r.size();
+  uint64_t* kb[2] = {nullptr, nullptr};
+  V* vb[2] = {nullptr, nullptr};
+  for (int i = 0; i < 2; i++) {
+    if ((st = scratch_alloc(ctx, (size_t)n * 8, (void**)&kb[i], stream))) return st;
+    if ((st = scratch_alloc(ctx, (size_t)n * sizeof(V), (void**)&vb[i], stream))) return st;
+  }
+  const bool multi = segs.size() > 1;
+  if (total == 0) {
+    int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8);
+    sort_identity_kernel<V><<<grid, 256, 0, stream>>>(pp, (const V*)nullptr);
+    GHB_LAUNCH_CHECK(ctx);
+    return GHB_OK;
+  }
+  uint64_t* status = nullptr;
+  size_t status_bytes = (size_t)pp.ntiles * kBins * 8;
+  if ((st = scratch_alloc(ctx, status_bytes, (void**)&status, stream))) return st;
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(status, 0, status_bytes, stream));
+  pp.status = status;
+  const size_t dyn = (size_t)kSortTile * (8 + sizeof(V));
+  if ((st = set_smem<V>(ctx, dyn))) return st;
+  int per_sm = 0;
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &per_sm, sort_pass_kernel<V, kSrcPacked, kDstPacked>, kSortThreads, dyn));
+  int pgrid = (int)std::min<int64_t>(pp.ntiles, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  int done = 0;
+  bool have_perm = false;  // a previous pass left the row order in vb[cur]
+  int cur = 0;
+  for (size_t s = 0; s < segs.size(); s++) {
+    pp.seg = segs[s];
+    for (size_t i = 0; i < run[s].size(); i++) {
+      int q = run[s][i];
+      bool last = ++done == total;
+      int src = i == 0 ? (have_perm ? kSrcPerm : kSrcCols) : kSrcPacked;
+      int dst = last ? (multi ? kDstGather : kDstDecode) : kDstPacked;
+      pp.shift = q * kDigitBits;
+      uint32_t acc = 0;
+      const uint32_t* h = &hist[((size_t)s * kMaxPasses + q) * kBins];
+      for (int b = 0; b < kBins; b++) {
+        pp.digit_base[b] = acc;
+        acc += h[b];
+      }
+      pp.keys_in = kb[cur];
+      pp.vals_in = vb[cur];
+      pp.keys_out = kb[cur ^ 1];
+      pp.vals_out = vb[cur ^ 1];
+      // the status region was cleared at the start of this call: tag pass k with k
+      pp.epoch = (uint32_t)done;
+      launch_pass<V>(src, dst, pgrid, dyn, stream, pp);
+      GHB_LAUNCH_CHECK(ctx);
+      cur ^= 1;
+      have_perm = true;
+    }
+  }
+  return GHB_OK;
 }
 
 int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
@@ -398,7 +575,7 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     if (pn != n) return set_error(ctx, GHB_ERR_INVALID, "payload rows %lld != key rows %lld",
                                   (long long)pn, (long long)n);
   }
-  if (n >= (int64_t)kSCount) return set_error(ctx, GHB_ERR_UNSUPPORTED, "sort of more than 2^30-1 rows");
+  if (n >= (int64_t)INT32_MAX) return set_error(ctx, GHB_ERR_UNSUPPORTED, "sort of 2^31 rows or more");
   if (!out_keys) return set_error(ctx, GHB_ERR_INVALID, "out_keys is NULL");
   for (int j = 0; j < nkeys; j++)
     if (out_keys[j].type != keys[j].type || (!out_keys[j].data && n > 0))
@@ -410,25 +587,24 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
 
   PassParams pp;
   std::memset(&pp, 0, sizeof(pp));
-  SortLayout& L = pp.L;
-  L.nkeys = nkeys;
+  KeySet& K = pp.K;
+  K.nkeys = nkeys;
   for (int j = 0; j < nkeys; j++) {
-    L.f[j].col = keys[j];
-    L.f[j].desc = orders && orders[j] == GHB_DESC;
+    K.k[j].col = keys[j];
+    K.k[j].desc = orders && orders[j] == GHB_DESC;
     int no = null_orders ? null_orders[j] : GHB_NULLS_DEFAULT;
-    L.f[j].nulls_first = no == GHB_NULLS_FIRST || (no == GHB_NULLS_DEFAULT && !L.f[j].desc);
+    K.k[j].nulls_first = no == GHB_NULLS_FIRST || (no == GHB_NULLS_DEFAULT && !K.k[j].desc);
   }
   unsigned long long* d_mm = nullptr;
   uint32_t* d_hist = nullptr;
   if ((st = scratch_alloc(ctx, 3 * 8 * kMaxSortKeys, (void**)&d_mm, stream))) return st;
-  if ((st = scratch_alloc(ctx, kMaxPasses * kBins * 4, (void**)&d_hist, stream))) return st;
+  if ((st = scratch_alloc(ctx, (size_t)kMaxSeg * kMaxPasses * kBins * 4, (void**)&d_hist, stream))) return st;
   std::vector<unsigned long long> mm_init(3 * kMaxSortKeys, 0);
   for (int j = 0; j < kMaxSortKeys; j++) mm_init[3 * j] = ~0ull;
   GHB_CUDA_TRY(ctx, cudaMemcpyAsync(d_mm, mm_init.data(), mm_init.size() * 8, cudaMemcpyHostToDevice, stream));
-  GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_hist, 0, kMaxPasses * kBins * 4, stream));
   int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8);
   MinMaxParams mp;
-  mp.L = L;
+  mp.K = K;
   mp.n = n;
   mp.out = d_mm;
   sort_minmax_kernel<<<grid, 256, 0, stream>>>(mp);
@@ -437,27 +613,69 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   GHB_CUDA_TRY(ctx, cudaMemcpyAsync(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost, stream));
   GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
 
-  // plan the packed layout: key 0 most significant
-  int bits = 0;
+  // plan: least significant key first, value bits then its NULL flag above
+  std::vector<Segment> segs(1);
+  std::memset(&segs[0], 0, sizeof(Segment));
+  auto add_sub = [&](int key, int is_flag, int bits) {
+    if (bits == 0) return;
+    if (segs.back().bits + bits > 64) {
+      segs.emplace_back();
+      std::memset(&segs.back(), 0, sizeof(Segment));
+    }
+    Segment& sg = segs.back();
+    SubField& sf = sg.f[sg.n++];
+    sf.key = (int8_t)key;
+    sf.is_flag = (int8_t)is_flag;
+    sf.bits = (int8_t)bits;
+    sf.shift = (int8_t)sg.bits;
+    sg.bits += bits;
+  };
   for (int j = nkeys - 1; j >= 0; j--) {
-    KeyField& f = L.f[j];
+    KeyField& f = K.k[j];
     bool anyval = mm[3 * j] <= mm[3 * j + 1];
     f.umin = anyval ? mm[3 * j] : 0;
     uint64_t range = anyval ? mm[3 * j + 1] - mm[3 * j] : 0;
     f.vbits = range == 0 ? 0 : 64 - __builtin_clzll(range);
-    f.has_null_bit = mm[3 * j + 2] ? 1 : 0;
-    f.shift = bits;
-    bits += f.vbits + f.has_null_bit;
+    f.has_null = mm[3 * j + 2] ? 1 : 0;
+    add_sub(j, 0, f.vbits);
+    add_sub(j, 1, f.has_null);
   }
-  if (bits > 64)
-    return set_error(ctx, GHB_ERR_UNSUPPORTED, "sort keys need %d bits after range packing (max 64)", bits);
-  const int npasses = (bits + kDigitBits - 1) / kDigitBits;
+  if (segs.size() > (size_t)kMaxSeg) return set_error(ctx, GHB_ERR_UNSUPPORTED, "too many key segments");
+  const bool multi = segs.size() > 1;
 
-  // a BYTEMAP payload's NULL flags do not travel with its value: carry the row
-  bool carry_rowid = out_rowid != nullptr || npayload > 1 ||
-                     (npayload == 1 && payload[0].null_mode == GHB_NULLS_BYTEMAP);
+  // histograms of every segment, one read each, then one sync
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_hist, 0, segs.size() * kMaxPasses * kBins * 4, stream));
+  for (size_t s = 0; s < segs.size(); s++) {
+    int np = (segs[s].bits + kDigitBits - 1) / kDigitBits;
+    if (np == 0) continue;
+    HistParams hp;
+    hp.K = K;
+    hp.seg = segs[s];
+    hp.n = n;
+    hp.npasses = np;
+    hp.hist = d_hist + s * kMaxPasses * kBins;
+    sort_hist_kernel<<<std::min(grid, ctx->num_sms * 4), 256, 0, stream>>>(hp);
+    GHB_LAUNCH_CHECK(ctx);
+  }
+  std::vector<uint32_t> hist((size_t)segs.size() * kMaxPasses * kBins, 0);
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(hist.data(), d_hist, hist.size() * 4, cudaMemcpyDeviceToHost, stream));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+  std::vector<std::vector<int>> run(segs.size());
+  for (size_t s = 0; s < segs.size(); s++) {
+    int np = (segs[s].bits + kDigitBits - 1) / kDigitBits;
+    for (int q = 0; q < np; q++) {
+      bool trivial = false;
+      for (int b = 0; b < kBins; b++)
+        if (hist[((size_t)s * kMaxPasses + q) * kBins + b] == (uint32_t)n) trivial = true;
+      if (!trivial) run[s].push_back(q);
+    }
+  }
+
+  // the value: the single payload itself, else the row index
+  bool carry_rowid = multi || out_rowid != nullptr || npayload != 1 ||
+                     payload[0].null_mode == GHB_NULLS_BYTEMAP;
   pp.carry_rowid = carry_rowid ? 1 : 0;
-  if (!carry_rowid && npayload == 1) pp.pay_src = payload[0];
+  if (!carry_rowid) pp.pay_src = payload[0];
   for (int j = 0; j < nkeys; j++) pp.out_keys[j] = out_keys[j];
   pp.npay = npayload;
   for (int j = 0; j < npayload; j++) {
@@ -469,74 +687,9 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   pp.ntiles = (n + kSortTile - 1) / kSortTile;
   pp.counters = ctx->d_counters + 2;
   pp.dev_status = ctx->d_status;
-
-  std::vector<int> run_passes;
-  std::vector<uint32_t> hist((size_t)kMaxPasses * kBins, 0);
-  if (npasses > 0) {
-    HistParams hp;
-    hp.L = L;
-    hp.n = n;
-    hp.npasses = npasses;
-    hp.hist = d_hist;
-    sort_hist_kernel<<<std::min(grid, ctx->num_sms * 4), 256, 0, stream>>>(hp);
-    GHB_LAUNCH_CHECK(ctx);
-    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(hist.data(), d_hist, (size_t)npasses * kBins * 4,
-                                      cudaMemcpyDeviceToHost, stream));
-    GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
-    for (int q = 0; q < npasses; q++) {
-      bool trivial = false;
-      for (int b = 0; b < kBins; b++)
-        if (hist[(size_t)q * kBins + b] == (uint32_t)n) trivial = true;
-      if (!trivial) run_passes.push_back(q);
-    }
-  }
-  if (run_passes.empty()) {
-    sort_copy_kernel<<<grid, 256, 0, stream>>>(pp);
-    GHB_LAUNCH_CHECK(ctx);
-    return GHB_OK;
-  }
-  uint64_t *kb[2] = {nullptr, nullptr}, *vb[2] = {nullptr, nullptr};
-  uint32_t* status = nullptr;
-  size_t nb = (size_t)n * 8;
-  if (run_passes.size() > 1) {
-    for (int i = 0; i < 2; i++) {
-      if ((st = scratch_alloc(ctx, nb, (void**)&kb[i], stream))) return st;
-      if ((st = scratch_alloc(ctx, nb, (void**)&vb[i], stream))) return st;
-    }
-  }
-  size_t status_bytes = (size_t)run_passes.size() * pp.ntiles * kBins * 4;
-  if ((st = scratch_alloc(ctx, status_bytes, (void**)&status, stream))) return st;
-  GHB_CUDA_TRY(ctx, cudaMemsetAsync(status, 0, status_bytes, stream));
-  const size_t dyn = 2 * (size_t)kSortTile * sizeof(uint64_t);
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  int per_sm = 0;
-  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sort_pass_kernel<false, false>,
-                                                                 kSortThreads, dyn));
-  int pgrid = (int)std::min<int64_t>(pp.ntiles, (int64_t)ctx->num_sms * std::max(1, per_sm));
-  for (size_t i = 0; i < run_passes.size(); i++) {
-    int q = run_passes[i];
-    bool first = i == 0, last = i + 1 == run_passes.size();
-    pp.shift = q * kDigitBits;
-    uint32_t acc = 0;
-    for (int b = 0; b < kBins; b++) {
-      pp.digit_base[b] = acc;
-      acc += hist[(size_t)q * kBins + b];
-    }
-    pp.keys_in = kb[(i + 1) & 1];
-    pp.vals_in = vb[(i + 1) & 1];
-    pp.keys_out = kb[i & 1];
-    pp.vals_out = vb[i & 1];
-    pp.status = status + i * (size_t)pp.ntiles * kBins;
-    if (first && last) sort_pass_kernel<true, true><<<pgrid, kSortThreads, dyn, stream>>>(pp);
-    else if (first) sort_pass_kernel<true, false><<<pgrid, kSortThreads, dyn, stream>>>(pp);
-    else if (last) sort_pass_kernel<false, true><<<pgrid, kSortThreads, dyn, stream>>>(pp);
-    else sort_pass_kernel<false, false><<<pgrid, kSortThreads, dyn, stream>>>(pp);
-    GHB_LAUNCH_CHECK(ctx);
-  }
-  return GHB_OK;
+  bool wide = !carry_rowid && type_width(payload[0].type) == 8;
+  if (wide) return run_passes<uint64_t>(ctx, pp, segs, run, hist, stream);
+  return run_passes<uint32_t>(ctx, pp, segs, run, hist, stream);
 }
 
 }  // namespace ghb

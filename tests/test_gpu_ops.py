@@ -449,17 +449,21 @@ def test_sort_desc_nulls_doubles(ctx):
     _check_sort(ctx, [big], [abi.DESC])
 
 
-def test_sort_all_equal_and_wide_key_rejected(ctx):
-    from ghive_b200._lib import GhbError
+def test_sort_all_equal_and_keys_wider_than_64_bits(ctx):
     n = 10_000
     same = np.full(n, 42, dtype=np.int64)
     _check_sort(ctx, [same], payload=[np.arange(n, dtype=np.int32)], rowid=False)
+    _check_sort(ctx, [same], rowid=True)
     g = np.random.default_rng(34)
-    wide = [g.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64),
-            g.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64)]
-    with pytest.raises(GhbError) as e:
-        ctx.sort([dev(w) for w in wide])
-    assert e.value.code == abi.ERR_UNSUPPORTED
+    i64 = np.iinfo(np.int64)
+    wide = [g.integers(-3, 3, n, dtype=np.int64),
+            g.integers(i64.min, i64.max, n, dtype=np.int64),
+            g.integers(i64.min, i64.max, n, dtype=np.int64)]
+    isnull = g.random(n) < 0.05
+    # three segments: a full-range key with NULLs needs 65 bits on its own
+    _check_sort(ctx, [wide[0], (wide[1], isnull), wide[2]], [abi.ASC, abi.DESC, abi.ASC],
+                payload=[np.arange(n, dtype=np.int32), g.random(n)])
+    _check_sort(ctx, wide[1:], rowid=False, payload=[g.integers(0, 9, n, dtype=np.int64)])
 
 
 # ------------------------------------------------------- host entry points
