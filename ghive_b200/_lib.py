@@ -29,6 +29,7 @@ _PROTOS = {
     "ghb_join_table_info": (I32, [P, P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
     "ghb_join_probe": (I32, [P, P, P, I32, P, I32, P, P, I32, P, P, P, I64, P, P]),
     "ghb_sort": (I32, [P, P, P, P, I32, P, I32, P, P, P, P, P]),
+    "ghb_filter_groupby_noalloc": (I32, [P, P, I32, P, I32, P, I32, P, I64, P, P, P]),
     "ghb_filter_host": (I32, [P, P, P, I32, P, I32, P, I64, C.POINTER(I64)]),
     "ghb_filter_groupby_host": (I32, [P, P, P, I32, P, I32, P, I32, P, I64, C.POINTER(I64), P]),
     "ghb_hash_join_host": (I32, [P, P, P, I32, P, I32, P, P, I32, P, P, P, I64,

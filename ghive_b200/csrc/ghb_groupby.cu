@@ -536,6 +536,8 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
     if (table_bytes > fixed_table_bytes)
       return set_error(ctx, GHB_ERR_CAPACITY, "group-by table needs %zu bytes, %zu available",
                        table_bytes, fixed_table_bytes);
+    // a caller-provided table may hold anything: clear the part this call uses
+    GHB_CUDA_TRY(ctx, cudaMemsetAsync(fixed_table, 0, table_bytes, stream));
     p.gkeys = (uint64_t*)fixed_table;
   } else {
     if (table_bytes > ctx->gb_bytes || ctx->gb_dirty || !ctx->gb_table) {

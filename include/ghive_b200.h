@@ -281,6 +281,35 @@ int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
                  ghb_out_column* out_keys, ghb_out_column* out_payload,
                  int32_t* out_rowid, const ghb_sort_cfg* cfg, void* stream);
 
+/* ---- fused filter + group-by without allocation -------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * a task whose device memory is all reserved by another allocator, or code
+ * that must not risk the device-wide synchronisation an allocation may
+ * imply.  Same operator and arguments as ghb_filter_groupby (device columns,
+ * device outputs, device group count), but no context: the hash table and the
+ * device status word live in a file-scope __device__ array of
+ * GHB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; nothing is allocated or freed.  The table needs
+ * (2 + next_pow2(max(2 * max_groups, 64))) * 8 * (1 + accumulator words)
+ * bytes (one accumulator word per COUNT/SUM/MIN/MAX state, two per double
+ * SUM/AVG, plus COUNT(*)); a call that would need more than the array holds
+ * returns GHB_ERR_CAPACITY before launching.  About 30,000 groups fit with
+ * the fact-table aggregates.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Each call clears the part of the
+ * array it uses, runs on `stream`, waits for it and returns the device
+ * status (GHB_ERR_CAPACITY for a short output).  Calls share the one array:
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * corrupt each other's tables. */
+#define GHB_NOALLOC_SCRATCH_BYTES (8u << 20)
+int32_t ghb_filter_groupby_noalloc(const ghb_predicate* pred,
+                                   const ghb_column* cols, int32_t ncols,
+                                   const int32_t* key_cols, int32_t nkeys,
+                                   const ghb_agg_desc* aggs, int32_t naggs,
+                                   ghb_out_column* out, int64_t out_capacity,
+                                   int64_t* d_out_groups,
+                                   const ghb_groupby_cfg* cfg, void* stream);
+
 /* ---- host-buffer entry points (end-to-end) -------------------------------
  * Same operators with every column in HOST memory (pageable or pinned).
  * These copy the inputs in, run the operator, copy the result out and
