@@ -199,11 +199,11 @@ def run_ours(args, world, rank, local):
 
     def join_step(ev=None):
         nonlocal outs
-        t = ctx.join_build(d_bkey)
+        t = ctx.join_build(d_bkey, build_payload=d_bpay)
         if ev:
             ev[0].record(stream)
-        outs = ctx.join_probe(t, d_fk, abi.INNER_JOIN, build_payload=d_bpay, capacity=cap,
-                              rowids=False, sync=False, outs=outs)
+        outs = ctx.join_probe(t, d_fk, abi.INNER_JOIN, capacity=cap, rowids=False, sync=False,
+                              outs=outs)
         if ev:
             ev[1].record(stream)
         t.free()

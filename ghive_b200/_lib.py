@@ -24,10 +24,10 @@ _PROTOS = {
     "ghb_kernel_launches": (I64, [P]),
     "ghb_filter": (I32, [P, P, P, I32, P, I32, P, I64, P, P]),
     "ghb_filter_groupby": (I32, [P, P, P, I32, P, I32, P, I32, P, I64, P, P, P]),
-    "ghb_join_build": (I32, [P, P, P, C.POINTER(C.c_void_p), P]),
+    "ghb_join_build": (I32, [P, P, P, I32, P, C.POINTER(C.c_void_p), P]),
     "ghb_join_table_free": (I32, [P, P]),
     "ghb_join_table_info": (I32, [P, P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
-    "ghb_join_probe": (I32, [P, P, P, I32, P, I32, P, P, I32, P, P, P, I64, P, P]),
+    "ghb_join_probe": (I32, [P, P, P, I32, P, P, I32, P, P, P, I64, P, P]),
     "ghb_sort": (I32, [P, P, P, P, I32, P, I32, P, P, P, P, P]),
     "ghb_filter_groupby_noalloc": (I32, [P, P, I32, P, I32, P, I32, P, I64, P, P, P]),
     "ghb_filter_host": (I32, [P, P, P, I32, P, I32, P, I64, C.POINTER(I64)]),

@@ -50,19 +50,23 @@ struct ghb_ctx {
 };
 
 struct ghb_join_table {
-  uint64_t* keys = nullptr;   // stored key (flip_i64), 0 = empty
-  int32_t* head = nullptr;    // first build row of the key
-  int32_t* count = nullptr;   // build rows sharing the key
-  int32_t* next = nullptr;    // chain of build rows (duplicates)
-  int64_t slots = 0;          // power of two
+  unsigned long long* kimg = nullptr;  // per slot: key image (0 = empty)
+  int2* meta = nullptr;                // per slot: {first row + 1, rows with the key}
+  ulonglong2* payw = nullptr;          // per slot: first row's inline payload words
+  int32_t* chain = nullptr;   // per slot: chain head (row + 1) of the key's 2nd.. rows
+  int32_t* next = nullptr;    // per build row: next row + 1 in its key's chain
+  int64_t slots = 0;          // hashed slots (power of two); slot `slots` is the side slot
   int64_t build_rows = 0;
   int32_t key_type = GHB_LONG;
-  unsigned long long* d_stats = nullptr;  // [0] rows stored, [1] max dup, [2] side-slot rows
-  int32_t side_head = -1;     // unused (INT64_MIN key lives in the side slot)
-  void* alloc = nullptr;
+  int32_t nbp = 0;            // build payload columns the table serves
+  int32_t n_inline = 0;       // of which copied into the slots
+  ghb_column pay[8];          // the build payload columns (caller-owned)
+  unsigned long long* d_stats = nullptr;  // [0] rows stored, [1] max duplicates
+  void* alloc = nullptr;      // slots, then chain, next and stats
   size_t alloc_bytes = 0;
   cudaStream_t stream = 0;    // build stream; the table is released in its order
   bool l2_window = false;
+  int32_t probe_threads = 256; // probe CTA size (ghb_join_cfg.block_threads)
 };
 
 namespace ghb {

@@ -60,8 +60,7 @@ __global__ void __launch_bounds__(kFiltThreads) filter_kernel(FilterParams p) {
   const unsigned lt_mask = (1u << lane) - 1u;
 
   while (true) {
-    if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&p.counters[0], 1ull);
-    __syncthreads();
+    claim_tile(&p.counters[0], &s_tile);
     const int64_t tile = s_tile;
     if (tile >= p.ntiles) break;
     const int64_t base = tile * kFiltTile;
@@ -114,16 +113,7 @@ __global__ void __launch_bounds__(kFiltThreads) filter_kernel(FilterParams p) {
     }
     __syncthreads();
   }
-  // the last CTA to finish resets the tile counter for the next launch
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned long long done = atomicAdd(&p.counters[1], 1ull);
-    if (done == gridDim.x - 1) {
-      p.counters[0] = 0;
-      p.counters[1] = 0;
-      __threadfence();
-    }
-  }
+  claim_finish(p.counters);
 }
 
 int32_t filter_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,

@@ -20,15 +20,16 @@ int32_t filter_impl(ghb_ctx*, const ghb_predicate*, const ghb_column*, int32_t, 
 int32_t filter_groupby_impl(ghb_ctx*, const ghb_predicate*, const ghb_column*, int32_t,
                             const int32_t*, int32_t, const ghb_agg_desc*, int32_t, ghb_out_column*,
                             int64_t, int64_t*, const ghb_groupby_cfg*, cudaStream_t, void*, size_t);
-int32_t join_build_impl(ghb_ctx*, const ghb_column*, const ghb_join_cfg*, ghb_join_table**,
-                        cudaStream_t);
+int32_t join_build_impl(ghb_ctx*, const ghb_column*, const ghb_column*, int32_t,
+                        const ghb_join_cfg*, ghb_join_table**, cudaStream_t);
 int32_t join_probe_impl(ghb_ctx*, const ghb_join_table*, const ghb_column*, int32_t,
-                        const ghb_column*, int32_t, ghb_out_column*, const ghb_column*, int32_t,
-                        ghb_out_column*, int32_t*, int32_t*, int64_t, int64_t*, cudaStream_t);
+                        ghb_out_column*, const ghb_column*, int32_t, ghb_out_column*, int32_t*,
+                        int32_t*, int64_t, int64_t*, cudaStream_t);
 int32_t sort_impl(ghb_ctx*, const ghb_column*, const int32_t*, const int32_t*, int32_t,
                   const ghb_column*, int32_t, ghb_out_column*, ghb_out_column*, int32_t*,
                   const ghb_sort_cfg*, cudaStream_t);
 size_t sort_scratch_bytes(int64_t n);
+size_t join_probe_scratch_bytes(int64_t n);
 
 namespace {
 
@@ -199,6 +200,7 @@ int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_
   for (int j = 0; j < npp; j++) need += in_bytes(probe_payload[j]) + out_bytes(out_probe[j], out_capacity) + 1024;
   if (out_probe_rowid) need += align256((size_t)out_capacity * 4) + 256;
   if (out_build_rowid) need += align256((size_t)out_capacity * 4) + 256;
+  need += join_probe_scratch_bytes(probe_key->n);
   int32_t st = scratch_reserve(ctx, need, s);
   if (st) return st;
   std::vector<ghb_column> dbk, dpk, dbp, dpp;
@@ -215,10 +217,10 @@ int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_
   if (out_probe_rowid && (st = scratch_alloc(ctx, (size_t)out_capacity * 4 + 16, (void**)&d_prow, s))) return st;
   if (out_build_rowid && (st = scratch_alloc(ctx, (size_t)out_capacity * 4 + 16, (void**)&d_brow, s))) return st;
   ghb_join_table* t = nullptr;
-  st = join_build_impl(ctx, dbk.data(), cfg, &t, s);
+  st = join_build_impl(ctx, dbk.data(), dbp.data(), nbp, cfg, &t, s);
   if (st) return st;
-  st = join_probe_impl(ctx, t, dpk.data(), join_type, dbp.data(), nbp, dob.data(), dpp.data(), npp,
-                       dop.data(), d_prow, d_brow, out_capacity, d_rows, s);
+  st = join_probe_impl(ctx, t, dpk.data(), join_type, dob.data(), dpp.data(), npp, dop.data(),
+                       d_prow, d_brow, out_capacity, d_rows, s);
   int64_t rows = 0;
   if (!st) st = read_count(ctx, d_rows, &rows, s);
   *out_rows = rows;

@@ -54,6 +54,13 @@ __device__ __forceinline__ int64_t ld_raw(const ghb_column& c, int64_t i) {
   return ld_i64(c, i);
 }
 
+// Same, for data read exactly once: an evict-first load (ld.global.cs) keeps
+// a streamed column from pushing reused data (hash tables) out of L2.
+__device__ __forceinline__ int64_t ld_raw_cs(const ghb_column& c, int64_t i) {
+  if (c.type == GHB_INT) return (int64_t)__ldcs((const int*)c.data + i);
+  return (int64_t)__ldcs((const long long*)c.data + i);
+}
+
 __device__ __forceinline__ double raw_to_f64(int type, int64_t raw) {
   return type == GHB_DOUBLE ? __longlong_as_double(raw) : (double)raw;
 }
@@ -179,24 +186,20 @@ __device__ __forceinline__ uint64_t lb_load(const uint64_t* p) {
 
 // Exclusive prefix of tile `tile` given its own `count`.  Called by one warp
 // (all 32 lanes).  Publishes the tile's aggregate, walks back over earlier
-// tiles 32 at a time, then publishes the inclusive prefix.  Every wait is
-// bounded: after kSpinLimit polls it raises GHB_ERR_TIMEOUT and returns 0
-// (the results of that launch are then invalid and the host is told).
+// tiles 32 at a time, then publishes the inclusive prefix.  The words carry
+// only counts (no tile reads another tile's output), so relaxed stores and
+// loads suffice and no fence is needed.  Every wait is bounded: after
+// kSpinLimit polls it raises GHB_ERR_TIMEOUT and returns 0 (the results of
+// that launch are then invalid and the host is told).
 __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status_arr, uint32_t epoch,
                                                        int64_t tile, uint64_t count,
                                                        int32_t* dev_status) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
-    if (lane == 0) {
-      __threadfence();
-      lb_store(&status_arr[0], lb_pack(epoch, kFlagPrefix, count));
-    }
+    if (lane == 0) lb_store(&status_arr[0], lb_pack(epoch, kFlagPrefix, count));
     return 0;
   }
-  if (lane == 0) {
-    __threadfence();
-    lb_store(&status_arr[tile], lb_pack(epoch, kFlagAgg, count));
-  }
+  if (lane == 0) lb_store(&status_arr[tile], lb_pack(epoch, kFlagAgg, count));
   uint64_t exclusive = 0;
   int64_t base = tile - 1;  // highest tile index the warp examines this round
   int spins = 0;
@@ -237,11 +240,32 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status_arr, uin
     if (pref) break;
     base -= 32;
   }
-  if (lane == 0) {
-    __threadfence();
-    lb_store(&status_arr[tile], lb_pack(epoch, kFlagPrefix, exclusive + count));
-  }
+  if (lane == 0) lb_store(&status_arr[tile], lb_pack(epoch, kFlagPrefix, exclusive + count));
   return exclusive;
+}
+
+// Tiles are claimed in launch order from a global counter, so a tile's
+// predecessors are always owned by running CTAs and the look-back cannot
+// wait on a CTA that never started.  A tile is claimed only when its CTA is
+// ready to work on it: a claim held back behind another tile would make
+// every later tile's look-back wait for it.
+__device__ __forceinline__ void claim_tile(unsigned long long* counter, int64_t* s_cur) {
+  if (threadIdx.x == 0) *s_cur = (int64_t)atomicAdd(counter, 1ull);
+  __syncthreads();
+}
+
+// Called once by every CTA at exit: the last one resets the claim counter
+// and the finish counter for the next launch.
+__device__ __forceinline__ void claim_finish(unsigned long long* counters) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long done = atomicAdd(&counters[1], 1ull);
+    if (done == gridDim.x - 1) {
+      counters[0] = 0;
+      counters[1] = 0;
+      __threadfence();
+    }
+  }
 }
 
 }  // namespace ghb

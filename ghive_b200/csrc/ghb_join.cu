@@ -4,46 +4,75 @@
 // GPU and merged them single-threaded on the CPU
 // (gpu_impl/src/Operator/SortMergeJoinPredicate.cu:8-461), then gathered the
 // retained columns on the host (gpu_impl/src/Operator/BaseJoinPredicate.cu:
-// 4-97).  Hive's CPU map-join probes a power-of-two open-addressing table of
-// (valueRef, key) slot pairs (VectorMapJoinFastLongHashTable.java:99-254);
-// the device table keeps that shape with 16-byte slots:
+// 4-97).  Hive's CPU map-join probes a power-of-two open-addressing table
+// whose value store holds each build row's retained columns
+// (VectorMapJoinFastLongHashTable.java:99-254, VectorMapJoinFastLongHashMap.
+// java:71-84).  The device table keeps keys and values together, laid out in
+// 128-byte buckets, one L2 line each, of four slots:
 //
-//   slot = { uint64 key image (flip_i64, 0 = empty), int32 head+1, int32 count }
+//   sector 0   uint64 key image[4]      (flip_i64 of the key, 0 = empty)
+//   sector 1   int32  first row + 1 [4], int32 rows with this key [4]
+//   sectors 2-3 uint64 payload[4][2]    (first build row's payload words)
 //
-// Duplicate build keys chain through next[] (head/next hold row+1, 0 ends the
-// chain), pushed with atomicExch so concurrent inserts of one key stay
-// consistent.  The key INT64_MIN, whose image is the empty marker, lives in
-// a side slot at index `slots`.
+// Slots fill in order inside a bucket and spill to the next bucket (linear
+// probing by buckets), so one 32-byte load of sector 0 settles almost every
+// probe: probe chains stay short, the warp does not wait for a long tail.  A
+// key that occurs more than once in the build chains its later rows through
+// chain[slot] / next[row] (row + 1, 0 ends the chain; pushed with atomicExch)
+// and their payloads are read from the build columns.  The key INT64_MIN,
+// whose image is the empty marker, lives in slot 0 of an extra side bucket.
+// The default load factor is Hive's hive.hashtable.loadfactor (0.75): the
+// 1.5M-key table is 512K buckets = 64 MB, resident in the 126 MB L2 while the
+// probe streams keys and results with evict-first loads and stores.
 //
-// The probe is one pass: each CTA claims tiles of probe rows in launch order,
-// finds each key's slot with linear probing, counts its output rows (build
-// matches for INNER, 0/1 for LEFT SEMI, max(matches,1) for LEFT OUTER), scans
-// the counts across the CTA, takes the tile's output offset by decoupled
-// look-back, and writes (probe row, build row, gathered payloads) in
-// probe-row order.
+// The probe counts, then writes (two passes over fixed chunks of probe rows,
+// no ordering dependency between CTAs):
+//   J2a  count: each CTA takes a chunk, loads its keys, issues the key-sector
+//        loads of all its rows together, stores each row's slot (-1 = no
+//        match) and the chunk's output-row count;
+//   J2b  scan: one CTA turns the chunk counts into output offsets;
+//   J2c  write: each CTA re-reads its chunk's slots, loads each matching
+//        slot's payload sector, scans the rows' output counts inside the
+//        chunk and writes (probe row, build row, payloads) at its offset, in
+//        probe-row order.
 #include <algorithm>
 
 #include "ghb_ctx.hpp"
 
 namespace ghb {
 
-struct __align__(16) JSlot {
-  unsigned long long key;
-  int32_t head_p1;
-  int32_t count;
-};
+// Slot s = bucket * 4 + index.  The slots' fields live in three arrays, so
+// each probe pass reads one dense array: the count pass only keys (4 per
+// bucket = one 32-byte sector; 16 MB for 1.5M keys), the write pass the
+// payload words and, when it needs them, the (first row, count) pairs.
+//   key[s]   uint64 key image (flip_i64 of the key, 0 = empty)
+//   meta[s]  int2 {first build row + 1, build rows with this key}
+//   pay[s]   ulonglong2, the first build row's inline payload words
 
 constexpr int kJThreads = 256;
-constexpr int kJItems = 8;
-constexpr int kJTile = kJThreads * kJItems;
+constexpr int kJItems = 4;
+constexpr int kChunk = kJThreads * kJItems;   // probe rows per chunk
 constexpr int kMaxPay = 8;
+constexpr int kInline = 2;
+
+// Bucket of a key image: Fibonacci (multiplicative) hashing, the top bits of
+// u * 2^64/phi.  One 64-bit multiply; consecutive keys land far apart.
+__device__ __forceinline__ int64_t bucket_of(unsigned long long u, int shift) {
+  return (int64_t)((u * 0x9E3779B97F4A7C15ull) >> shift);
+}
 
 struct BuildParams {
   ghb_column key;
-  JSlot* slots;
-  int32_t* next_p1;
-  int64_t mask;
-  int64_t side;          // index of the side slot (= number of hashed slots)
+  int32_t n_inline;
+  ghb_column pay[kInline];
+  unsigned long long* kimg;   // key[s] of the layout above
+  int2* meta;
+  ulonglong2* payw;
+  int32_t* chain_p1;     // [slots]
+  int32_t* next_p1;      // [build rows]
+  int64_t bmask;         // hashed buckets - 1
+  int32_t hshift;        // 64 - log2(hashed buckets)
+  int64_t side;          // index of the side bucket
   unsigned long long* stats;  // [0] rows stored, [1] max duplicates
   int32_t* status;
 };
@@ -55,31 +84,38 @@ __global__ void __launch_bounds__(256) join_build_kernel(BuildParams p) {
     int64_t raw = ld_raw(p.key, r);
     if (raw_is_null(p.key, raw, r)) continue;   // NULL keys never join
     unsigned long long u = flip_i64(raw);
-    int64_t s;
+    int64_t bk, j = -1;
     if (u == 0) {
-      s = p.side;
+      bk = p.side;
+      j = 0;
     } else {
-      s = (int64_t)(mix64(u) & (uint64_t)p.mask);
-      int64_t probes = 0;
-      while (true) {
-        unsigned long long cur = p.slots[s].key;
-        if (cur == u) break;
-        if (cur == 0) {
-          unsigned long long prev = atomicCAS(&p.slots[s].key, 0ull, u);
-          if (prev == 0 || prev == u) break;
+      bk = bucket_of(u, p.hshift);
+      for (int64_t probes = 0; probes <= p.bmask && j < 0; probes++) {
+        for (int q = 0; q < 4; q++) {
+          unsigned long long cur = p.kimg[bk * 4 + q];
+          if (cur == 0) {
+            unsigned long long prev = atomicCAS(&p.kimg[bk * 4 + q], 0ull, u);
+            if (prev == 0 || prev == u) { j = q; break; }
+            cur = prev;
+          }
+          if (cur == u) { j = q; break; }
         }
-        s = (s + 1) & p.mask;
-        if (++probes > p.mask) {   // table full: cannot happen with load factor < 1
-          raise_status(p.status, kDevCapacity);
-          s = -1;
-          break;
-        }
+        if (j < 0) bk = (bk + 1) & p.bmask;
       }
-      if (s < 0) continue;
+      if (j < 0) {   // table full: cannot happen with load factor < 1
+        raise_status(p.status, kDevCapacity);
+        continue;
+      }
     }
-    int old = atomicAdd(&p.slots[s].count, 1);
-    int prev = atomicExch(&p.slots[s].head_p1, (int)(r + 1));
-    p.next_p1[r] = prev;
+    const int64_t slot = bk * 4 + j;
+    int old = atomicAdd(&p.meta[slot].y, 1);
+    if (old == 0) {
+      p.meta[slot].x = (int32_t)(r + 1);
+      if (p.n_inline > 0) p.payw[slot].x = (unsigned long long)ld_raw(p.pay[0], r);
+      if (p.n_inline > 1) p.payw[slot].y = (unsigned long long)ld_raw(p.pay[1], r);
+    } else {
+      p.next_p1[r] = atomicExch(&p.chain_p1[slot], (int)(r + 1));
+    }
     stored++;
     maxdup = max(maxdup, (unsigned long long)(old + 1));
   }
@@ -94,103 +130,254 @@ __global__ void __launch_bounds__(256) join_build_kernel(BuildParams p) {
   }
 }
 
+// ------------------------------------------------------------------ probe
 struct ProbeParams {
-  const JSlot* slots;
+  const unsigned long long* kimg;
+  const int2* meta;
+  const ulonglong2* payw;
+  const int32_t* chain_p1;
   const int32_t* next_p1;
-  int64_t mask;
+  const unsigned long long* stats;
+  int64_t bmask;
+  int32_t hshift;
   int64_t side;
   ghb_column pkey;
   int32_t join_type;
-  int32_t nbp, npp;
+  int32_t nbp, npp, n_inline;
+  int32_t lean;            // INNER, no probe payloads, every build payload inline and non-NULL
   ghb_column bpay[kMaxPay];
   ghb_out_column obp[kMaxPay];
   ghb_column ppay[kMaxPay];
   ghb_out_column opp[kMaxPay];
   int32_t* out_prow;
   int32_t* out_brow;
-  int64_t n, ntiles, cap;
+  int64_t n, nchunks, cap;
+  int32_t* slot_of_row;    // [n] slot (bucket * 4 + index) of the row's key, -1 = no match
+  int64_t* chunk_count;    // [nchunks] output rows of each chunk, then its offset
   int64_t* d_out_rows;
-  uint64_t* lb;
-  uint32_t epoch;
-  unsigned long long* counters;
   int32_t* status;
 };
 
-__device__ __forceinline__ void put_value(const ghb_column& c, const ghb_out_column& o, int64_t row,
-                                          int64_t pos) {
-  if (row < 0) {  // outer-join miss: NULL
-    if (o.is_null) o.is_null[pos] = 1;
-    if (o.type == GHB_INT) ((int32_t*)o.data)[pos] = INT32_MAX;
-    else if (o.type == GHB_LONG) ((int64_t*)o.data)[pos] = INT64_MAX;
-    else ((long long*)o.data)[pos] = 0x7ff8000000000000ll;
-    return;
+// Output rows a probe row produces, from its slot's count (0 = no match).
+__device__ __forceinline__ int32_t out_rows_of(int join_type, int32_t count) {
+  if (join_type == GHB_LEFT_SEMI_JOIN) return count > 0 ? 1 : 0;
+  if (join_type == GHB_LEFT_OUTER_JOIN) return count > 0 ? count : 1;
+  return count;
+}
+
+__device__ __forceinline__ void load_keys(const unsigned long long* kimg, int64_t bk,
+                                          unsigned long long k[4]) {
+  const ulonglong2* s = (const ulonglong2*)(kimg + bk * 4);
+  ulonglong2 x = s[0], y = s[1];
+  k[0] = x.x;
+  k[1] = x.y;
+  k[2] = y.x;
+  k[3] = y.y;
+}
+
+// Index (0..3) of `u` among the bucket's keys, -1 when an empty slot ends
+// the search, -2 when the bucket is full of other keys.
+__device__ __forceinline__ int find_in(const unsigned long long k[4], unsigned long long u) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (k[q] == u) return q;
+    if (k[q] == 0) return -1;
   }
-  int64_t raw = ld_raw(c, row);
-  if (c.type == GHB_INT) ((int32_t*)o.data)[pos] = (int32_t)raw;
-  else ((long long*)o.data)[pos] = raw;
-  if (o.is_null) o.is_null[pos] = (c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row)) ? 1 : 0;
+  return -2;
 }
 
-__device__ __forceinline__ void emit_pair(const ProbeParams& p, int64_t pos, int64_t prow, int32_t brow) {
-  if (p.out_prow) p.out_prow[pos] = (int32_t)prow;
-  if (p.out_brow) p.out_brow[pos] = brow;
-  for (int j = 0; j < p.nbp; j++) put_value(p.bpay[j], p.obp[j], brow, pos);
-  for (int j = 0; j < p.npp; j++) put_value(p.ppay[j], p.opp[j], prow, pos);
-}
-
-__global__ void __launch_bounds__(kJThreads) join_probe_kernel(ProbeParams p) {
-  __shared__ int64_t s_tile;
-  __shared__ uint64_t s_warp_tot[kJThreads / 32];
-  __shared__ uint64_t s_warp_excl[kJThreads / 32];
-  __shared__ uint64_t s_tile_excl;
+// TH threads x IT rows per thread = one chunk (kChunk rows) per iteration.
+template <int TH, int IT, bool KEY_INT, bool NULLABLE>
+__global__ void __launch_bounds__(TH) join_count_kernel(ProbeParams p) {
+  constexpr int kJThreads = TH, kJItems = IT;
+  static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
+  __shared__ uint64_t s_warp[kJThreads / 32];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-
-  while (true) {
-    if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(&p.counters[0], 1ull);
+  const bool unique = p.stats[1] <= 1;   // every key once: a match is one output row
+  const int woff = warp * (32 * kJItems) + lane;
+  for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
+    const int64_t cbase = c * kChunk;
+    // rows of this chunk left (a full chunk unless it is the last one)
+    const int left = (int)min((int64_t)kChunk, p.n - cbase);
+    unsigned long long u[kJItems];
+    bool valid[kJItems];
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      const int off = woff + k * 32;
+      long long raw = 0;
+      if (off < left)
+        raw = KEY_INT ? (long long)__ldcs((const int*)p.pkey.data + cbase + off)
+                      : __ldcs((const long long*)p.pkey.data + cbase + off);
+      valid[k] = off < left && !(NULLABLE && raw_is_null(p.pkey, raw, cbase + off));
+      u[k] = flip_i64(raw);
+    }
+    int64_t bk[kJItems];
+    unsigned long long keys[kJItems][4];
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      bk[k] = bucket_of(u[k], p.hshift);
+      if (valid[k] && u[k] != 0) load_keys(p.kimg, bk[k], keys[k]);
+    }
+    uint64_t m_sum = 0;
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      const int off = woff + k * 32;
+      const int64_t row = cbase + off;
+      int32_t slot = -1, count = 0;
+      if (valid[k]) {
+        if (u[k] == 0) {
+          int32_t cnt = p.meta[p.side * 4].y;
+          if (cnt > 0) { slot = (int32_t)(p.side * 4); count = cnt; }
+        } else {
+          int q = find_in(keys[k], u[k]);
+          while (q == -2) {   // bucket full of other keys: continue in the next one
+            bk[k] = (bk[k] + 1) & p.bmask;
+            load_keys(p.kimg, bk[k], keys[k]);
+            q = find_in(keys[k], u[k]);
+          }
+          if (q >= 0) {
+            slot = (int32_t)(bk[k] * 4 + q);
+            count = unique ? 1 : p.meta[slot].y;
+          }
+        }
+      }
+      if (off < left) {
+        p.slot_of_row[row] = slot;
+        m_sum += (uint64_t)out_rows_of(p.join_type, count);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) m_sum += __shfl_down_sync(0xffffffffu, m_sum, o);
+    if (lane == 0) s_warp[warp] = m_sum;
     __syncthreads();
-    const int64_t tile = s_tile;
-    if (tile >= p.ntiles) break;
-    // each warp owns a contiguous segment of 32 * kJItems probe rows
-    const int64_t wbase = tile * kJTile + (int64_t)warp * (32 * kJItems);
+    if (threadIdx.x == 0) {
+      uint64_t t = 0;
+      for (int w = 0; w < kJThreads / 32; w++) t += s_warp[w];
+      p.chunk_count[c] = (int64_t)t;
+    }
+    __syncthreads();
+  }
+}
 
-    int32_t head[kJItems];
-    int32_t mult[kJItems];
-    uint32_t excl[kJItems];
-    uint64_t running = 0;
+// One CTA: chunk counts -> exclusive offsets in place; the total to d_out_rows.
+__global__ void __launch_bounds__(1024) join_scan_kernel(int64_t* counts, int64_t n, int64_t* d_total) {
+  __shared__ int64_t s_part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (n + 1023) / 1024;
+  const int64_t lo = t * per, hi = min(n, lo + per);
+  int64_t sum = 0;
+  for (int64_t i = lo; i < hi; i++) sum += counts[i];
+  s_part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int64_t v = t >= o ? s_part[t - o] : 0;
+    __syncthreads();
+    s_part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = s_part[t] - sum;
+  for (int64_t i = lo; i < hi; i++) {
+    int64_t c = counts[i];
+    counts[i] = run;
+    run += c;
+  }
+  if (t == 1023) *d_total = s_part[1023];
+}
+
+__device__ __forceinline__ void put_word(const ghb_out_column& o, int64_t pos, int type, int64_t raw,
+                                         bool null) {
+  if (null) {
+    if (type == GHB_INT) __stcs((int*)o.data + pos, INT32_MAX);
+    else if (type == GHB_LONG) __stcs((long long*)o.data + pos, (long long)INT64_MAX);
+    else __stcs((long long*)o.data + pos, 0x7ff8000000000000ll);
+  } else if (type == GHB_INT) {
+    __stcs((int*)o.data + pos, (int)raw);
+  } else {
+    __stcs((long long*)o.data + pos, (long long)raw);
+  }
+  if (o.is_null) o.is_null[pos] = null ? 1 : 0;
+}
+
+// One output row: probe row `prow`, build row `brow` (-1 for an outer miss /
+// semi), with the first-row payload words `w0`, `w1` when `inl` is set.
+__device__ __forceinline__ void emit_row(const ProbeParams& p, int64_t pos, int64_t prow, int32_t brow,
+                                         bool inl, unsigned long long w0, unsigned long long w1) {
+  if (p.out_prow) __stcs(p.out_prow + pos, (int)prow);
+  if (p.out_brow) __stcs(p.out_brow + pos, brow);
+  if (p.lean) {
+    // every payload non-NULL and brow >= 0 (INNER); the first row of a key
+    // reads the slot's copy, later rows of a duplicated key the build column
+    for (int j = 0; j < p.nbp; j++) {
+      unsigned long long w = inl ? (j == 0 ? w0 : w1) : (unsigned long long)ld_raw(p.bpay[j], brow);
+      if (p.bpay[j].type == GHB_INT) __stcs((int*)p.obp[j].data + pos, (int)w);
+      else __stcs((unsigned long long*)p.obp[j].data + pos, w);
+      if (p.obp[j].is_null) p.obp[j].is_null[pos] = 0;
+    }
+    return;
+  }
+  for (int j = 0; j < p.nbp; j++) {
+    const ghb_column& c = p.bpay[j];
+    if (brow < 0) {
+      put_word(p.obp[j], pos, c.type, 0, true);
+      continue;
+    }
+    int64_t raw = (inl && j < p.n_inline) ? (int64_t)(j == 0 ? w0 : w1) : ld_raw(c, brow);
+    bool null = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, brow);
+    put_word(p.obp[j], pos, c.type, raw, null);
+  }
+  for (int j = 0; j < p.npp; j++) {
+    const ghb_column& c = p.ppay[j];
+    int64_t raw = ld_raw(c, prow);
+    put_word(p.opp[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, prow));
+  }
+}
+
+template <int TH, int IT>
+__global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
+  constexpr int kJThreads = TH, kJItems = IT;
+  static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
+  __shared__ uint32_t s_warp_tot[kJThreads / 32];
+  __shared__ uint32_t s_warp_excl[kJThreads / 32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const bool unique = p.stats[1] <= 1;
+  // the row's (first row, count) is needed for duplicates and build row ids
+  const bool need_meta = !unique || p.out_brow != nullptr || !p.lean;
+  for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
+    const int64_t wbase = c * kChunk + (int64_t)warp * (32 * kJItems);
+    int32_t s[kJItems];
 #pragma unroll
     for (int k = 0; k < kJItems; k++) {
       int64_t row = wbase + k * 32 + lane;
-      int32_t m = 0, h = 0;
-      if (row < p.n) {
-        int64_t raw = ld_raw(p.pkey, row);
-        bool found = false;
-        if (!raw_is_null(p.pkey, raw, row)) {
-          unsigned long long u = flip_i64(raw);
-          int64_t s = u == 0 ? p.side : (int64_t)(mix64(u) & (uint64_t)p.mask);
-          while (true) {
-            JSlot sl = p.slots[s];
-            if (sl.key == u && sl.count > 0) {
-              found = true;
-              m = sl.count;
-              h = sl.head_p1;
-              break;
-            }
-            if (sl.key == 0 || u == 0) break;   // empty slot: no match
-            s = (s + 1) & p.mask;
-          }
+      s[k] = row < p.n ? __ldcs(p.slot_of_row + row) : -1;
+    }
+    ulonglong2 w[kJItems];
+    int32_t first[kJItems], cnt[kJItems];
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      first[k] = 0;
+      cnt[k] = s[k] >= 0 ? 1 : 0;
+      if (s[k] >= 0) {
+        if (p.nbp > 0) w[k] = p.payw[s[k]];
+        if (need_meta) {
+          const int2 m = p.meta[s[k]];
+          first[k] = m.x;
+          cnt[k] = m.y;
         }
-        if (p.join_type == GHB_LEFT_SEMI_JOIN) m = found ? 1 : 0;
-        else if (p.join_type == GHB_LEFT_OUTER_JOIN && !found) m = 1;
-        if (!found) h = 0;
       }
-      head[k] = h;
+    }
+    int32_t mult[kJItems];
+    uint32_t excl[kJItems];
+    uint32_t running = 0;
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      int64_t row = wbase + k * 32 + lane;
+      int32_t m = row < p.n ? out_rows_of(p.join_type, cnt[k]) : 0;
       mult[k] = m;
-      // inclusive warp scan of m (ballot when every lane emits 0 or 1)
       uint32_t incl;
       if (__all_sync(0xffffffffu, m <= 1)) {
-        unsigned b = __ballot_sync(0xffffffffu, m == 1);
-        incl = __popc(b & ((2u << lane) - 1u));
+        unsigned bal = __ballot_sync(0xffffffffu, m == 1);
+        incl = __popc(bal & ((2u << lane) - 1u));
       } else {
         incl = (uint32_t)m;
         for (int o = 1; o < 32; o <<= 1) {
@@ -198,57 +385,45 @@ __global__ void __launch_bounds__(kJThreads) join_probe_kernel(ProbeParams p) {
           if (lane >= o) incl += t;
         }
       }
-      excl[k] = (uint32_t)running + incl - (uint32_t)m;
+      excl[k] = running + incl - (uint32_t)m;
       running += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) s_warp_tot[warp] = running;
     __syncthreads();
     if (warp == 0) {
-      uint64_t v = lane < kJThreads / 32 ? s_warp_tot[lane] : 0;
-      uint64_t incl = v;
+      uint32_t v = lane < kJThreads / 32 ? s_warp_tot[lane] : 0;
+      uint32_t incl = v;
       for (int o = 1; o < 32; o <<= 1) {
-        uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
       }
       if (lane < kJThreads / 32) s_warp_excl[lane] = incl - v;
-      uint64_t total = __shfl_sync(0xffffffffu, incl, 31);
-      uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, total, p.status);
-      if (lane == 0) {
-        s_tile_excl = ex;
-        if (tile == p.ntiles - 1) *p.d_out_rows = (int64_t)(ex + total);
-      }
     }
     __syncthreads();
-    const uint64_t wexcl = s_tile_excl + s_warp_excl[warp];
+    const int64_t wpos = p.chunk_count[c] + s_warp_excl[warp];
 #pragma unroll
     for (int k = 0; k < kJItems; k++) {
       if (mult[k] == 0) continue;
       int64_t row = wbase + k * 32 + lane;
-      int64_t pos = (int64_t)(wexcl + excl[k]);
+      int64_t pos = wpos + excl[k];
       if (pos + mult[k] > p.cap) {
         raise_status(p.status, kDevCapacity);
         continue;
       }
-      if (head[k] == 0 || p.join_type == GHB_LEFT_SEMI_JOIN) {
-        emit_pair(p, pos, row, -1);
+      if (s[k] < 0 || p.join_type == GHB_LEFT_SEMI_JOIN) {
+        emit_row(p, pos, row, -1, false, 0, 0);
         continue;
       }
-      int32_t b = head[k] - 1;
-      for (int j = 0; j < mult[k]; j++) {
-        emit_pair(p, pos + j, row, b);
-        if (j + 1 < mult[k]) b = p.next_p1[b] - 1;
+      emit_row(p, pos, row, first[k] - 1, true, p.nbp > 0 ? w[k].x : 0, p.nbp > 0 ? w[k].y : 0);
+      if (mult[k] > 1) {
+        int32_t b = p.chain_p1[s[k]] - 1;
+        for (int j = 1; j < mult[k]; j++) {
+          emit_row(p, pos + j, row, b, false, 0, 0);
+          if (j + 1 < mult[k]) b = p.next_p1[b] - 1;
+        }
       }
     }
     __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned long long done = atomicAdd(&p.counters[1], 1ull);
-    if (done == gridDim.x - 1) {
-      p.counters[0] = 0;
-      p.counters[1] = 0;
-      __threadfence();
-    }
   }
 }
 
@@ -258,49 +433,79 @@ static int64_t next_pow2(int64_t v) {
   return p;
 }
 
-int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_join_cfg* cfg,
-                        ghb_join_table** out, cudaStream_t stream) {
+int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* build_payload,
+                        int32_t nbp, const ghb_join_cfg* cfg, ghb_join_table** out,
+                        cudaStream_t stream) {
   if (!out) return set_error(ctx, GHB_ERR_INVALID, "out is NULL");
   *out = nullptr;
   int32_t st = validate_columns(ctx, build_key, 1, nullptr);
   if (st) return st;
   if (build_key->type == GHB_DOUBLE)
     return set_error(ctx, GHB_ERR_UNSUPPORTED, "join keys must be LONG or INT");
-  if (build_key->n >= INT32_MAX)
-    return set_error(ctx, GHB_ERR_UNSUPPORTED, "build side above 2^31-1 rows");
-  float lf = (cfg && cfg->load_factor > 0.f && cfg->load_factor < 0.95f) ? cfg->load_factor : 0.5f;
-  int64_t C = next_pow2(std::max<int64_t>(64, (int64_t)((double)build_key->n / lf) + 1));
+  if (build_key->n >= INT32_MAX / 2)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "build side of 2^30 rows or more");
+  if (nbp < 0 || nbp > kMaxPay || (nbp > 0 && !build_payload))
+    return set_error(ctx, GHB_ERR_INVALID, "n_build_payload=%d outside [0,%d]", nbp, kMaxPay);
+  for (int j = 0; j < nbp; j++) {
+    if ((st = validate_columns(ctx, &build_payload[j], 1, nullptr))) return st;
+    if (build_payload[j].n != build_key->n)
+      return set_error(ctx, GHB_ERR_INVALID, "build payload %d has %lld rows, the key %lld", j,
+                       (long long)build_payload[j].n, (long long)build_key->n);
+  }
+  float lf = (cfg && cfg->load_factor > 0.f && cfg->load_factor < 0.95f) ? cfg->load_factor : 0.75f;
+  int64_t nb = next_pow2(std::max<int64_t>(16, (int64_t)((double)build_key->n / (4.0 * lf)) + 1));
   ghb_join_table* t = new ghb_join_table();
-  t->slots = C;
+  t->slots = nb * 4;
   t->build_rows = build_key->n;
   t->key_type = build_key->type;
-  size_t slot_bytes = (size_t)(C + 1) * sizeof(JSlot);
-  size_t next_bytes = ((size_t)std::max<int64_t>(build_key->n, 1) * 4 + 255) & ~(size_t)255;
-  size_t bytes = slot_bytes + next_bytes + 256;
+  t->nbp = nbp;
+  for (int j = 0; j < nbp; j++) t->pay[j] = build_payload[j];
+  // payloads copied into the slots: the first two non-BYTEMAP columns
+  t->n_inline = 0;
+  while (t->n_inline < std::min(nbp, kInline) && build_payload[t->n_inline].null_mode != GHB_NULLS_BYTEMAP)
+    t->n_inline++;
+  const size_t slots = (size_t)(nb + 1) * 4;   // hashed buckets + the side bucket
+  auto a256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t key_bytes = a256(slots * 8), meta_bytes = a256(slots * 8), pay_bytes = a256(slots * 16);
+  size_t bucket_bytes = key_bytes + meta_bytes + pay_bytes;
+  size_t chain_bytes = a256(slots * 4);
+  size_t next_bytes = a256((size_t)std::max<int64_t>(build_key->n, 1) * 4);
+  size_t bytes = bucket_bytes + chain_bytes + next_bytes + 256;
   // stream-ordered allocation: no device-wide sync, and the pool keeps the
   // memory for the next build on this device
   t->stream = stream;
+  if (cfg && cfg->block_threads > 0) t->probe_threads = cfg->block_threads;
   if (cudaMallocAsync(&t->alloc, bytes, stream) != cudaSuccess) {
     cudaGetLastError();
     delete t;
     return set_error(ctx, GHB_ERR_OOM, "cannot allocate a %zu-byte join table", bytes);
   }
   t->alloc_bytes = bytes;
-  t->keys = (uint64_t*)t->alloc;
-  t->next = (int32_t*)((char*)t->alloc + slot_bytes);
-  t->d_stats = (unsigned long long*)((char*)t->alloc + slot_bytes + next_bytes);
-  if (cudaMemsetAsync(t->alloc, 0, slot_bytes, stream) != cudaSuccess ||
+  t->kimg = (unsigned long long*)t->alloc;
+  t->meta = (int2*)((char*)t->alloc + key_bytes);
+  t->payw = (ulonglong2*)((char*)t->alloc + key_bytes + meta_bytes);
+  t->chain = (int32_t*)((char*)t->alloc + bucket_bytes);
+  t->next = (int32_t*)((char*)t->alloc + bucket_bytes + chain_bytes);
+  t->d_stats = (unsigned long long*)((char*)t->alloc + bucket_bytes + chain_bytes + next_bytes);
+  if (cudaMemsetAsync(t->alloc, 0, bucket_bytes + chain_bytes, stream) != cudaSuccess ||
       cudaMemsetAsync(t->d_stats, 0, 256, stream) != cudaSuccess) {
     cudaFreeAsync(t->alloc, stream);
     delete t;
     return set_error(ctx, GHB_ERR_CUDA, "memset of the join table failed");
   }
   BuildParams p;
+  std::memset(&p, 0, sizeof(p));
   p.key = *build_key;
-  p.slots = (JSlot*)t->alloc;
+  p.n_inline = t->n_inline;
+  for (int j = 0; j < t->n_inline; j++) p.pay[j] = build_payload[j];
+  p.kimg = t->kimg;
+  p.meta = t->meta;
+  p.payw = t->payw;
+  p.chain_p1 = t->chain;
   p.next_p1 = t->next;
-  p.mask = C - 1;
-  p.side = C;
+  p.bmask = nb - 1;
+  p.hshift = 64 - __builtin_ctzll((unsigned long long)nb);
+  p.side = nb;
   p.stats = t->d_stats;
   p.status = ctx->d_status;
   if (build_key->n > 0) {
@@ -322,7 +527,7 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_joi
       cudaStreamAttrValue attr;
       std::memset(&attr, 0, sizeof(attr));
       attr.accessPolicyWindow.base_ptr = t->alloc;
-      attr.accessPolicyWindow.num_bytes = std::min(slot_bytes, (size_t)max_persist);
+      attr.accessPolicyWindow.num_bytes = std::min(bucket_bytes, (size_t)max_persist);
       attr.accessPolicyWindow.hitRatio = 1.0f;
       attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
       attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
@@ -334,10 +539,16 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_joi
   return GHB_OK;
 }
 
+// Scratch one probe of n rows needs (slot per row, count per chunk).
+size_t join_probe_scratch_bytes(int64_t n) {
+  int64_t nchunks = (n + kChunk - 1) / kChunk;
+  return (((size_t)std::max<int64_t>(n, 1) * 4 + 255) & ~(size_t)255) +
+         (((size_t)std::max<int64_t>(nchunks, 1) * 8 + 255) & ~(size_t)255) + 512;
+}
+
 int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column* probe_key,
-                        int32_t join_type, const ghb_column* build_payload, int32_t nbp,
-                        ghb_out_column* out_build, const ghb_column* probe_payload, int32_t npp,
-                        ghb_out_column* out_probe, int32_t* out_probe_rowid,
+                        int32_t join_type, ghb_out_column* out_build, const ghb_column* probe_payload,
+                        int32_t npp, ghb_out_column* out_probe, int32_t* out_probe_rowid,
                         int32_t* out_build_rowid, int64_t out_capacity, int64_t* d_out_rows,
                         cudaStream_t stream) {
   if (!t) return set_error(ctx, GHB_ERR_INVALID, "table is NULL");
@@ -349,25 +560,20 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
     return set_error(ctx, GHB_ERR_UNSUPPORTED, "probe side above 2^31-1 rows per call");
   if (join_type != GHB_INNER_JOIN && join_type != GHB_LEFT_SEMI_JOIN && join_type != GHB_LEFT_OUTER_JOIN)
     return set_error(ctx, GHB_ERR_UNSUPPORTED, "join type %d", join_type);
-  if (nbp < 0 || nbp > kMaxPay || npp < 0 || npp > kMaxPay)
-    return set_error(ctx, GHB_ERR_INVALID, "payload counts %d/%d outside [0,%d]", nbp, npp, kMaxPay);
+  if (npp < 0 || npp > kMaxPay)
+    return set_error(ctx, GHB_ERR_INVALID, "n_probe_payload=%d outside [0,%d]", npp, kMaxPay);
   if (!d_out_rows) return set_error(ctx, GHB_ERR_INVALID, "d_out_rows is NULL");
+  if (t->nbp > 0 && !out_build) return set_error(ctx, GHB_ERR_INVALID, "out_build is NULL");
   ProbeParams p;
   std::memset(&p, 0, sizeof(p));
-  for (int j = 0; j < nbp; j++) {
-    st = validate_columns(ctx, &build_payload[j], 1, nullptr);
-    if (st) return st;
-    if (build_payload[j].n != t->build_rows)
-      return set_error(ctx, GHB_ERR_INVALID, "build payload %d has %lld rows, table has %lld", j,
-                       (long long)build_payload[j].n, (long long)t->build_rows);
-    if (out_build[j].type != build_payload[j].type || !out_build[j].data)
+  for (int j = 0; j < t->nbp; j++) {
+    if (out_build[j].type != t->pay[j].type || !out_build[j].data)
       return set_error(ctx, GHB_ERR_INVALID, "build payload output %d: bad type or data", j);
-    p.bpay[j] = build_payload[j];
+    p.bpay[j] = t->pay[j];
     p.obp[j] = out_build[j];
   }
   for (int j = 0; j < npp; j++) {
-    st = validate_columns(ctx, &probe_payload[j], 1, nullptr);
-    if (st) return st;
+    if ((st = validate_columns(ctx, &probe_payload[j], 1, nullptr))) return st;
     if (probe_payload[j].n != probe_key->n)
       return set_error(ctx, GHB_ERR_INVALID, "probe payload %d row count differs from the key", j);
     if (out_probe[j].type != probe_payload[j].type || !out_probe[j].data)
@@ -375,33 +581,59 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
     p.ppay[j] = probe_payload[j];
     p.opp[j] = out_probe[j];
   }
-  p.slots = (const JSlot*)t->alloc;
+  p.kimg = t->kimg;
+  p.meta = t->meta;
+  p.payw = t->payw;
+  p.chain_p1 = t->chain;
   p.next_p1 = t->next;
-  p.mask = t->slots - 1;
-  p.side = t->slots;
+  p.stats = t->d_stats;
+  p.bmask = t->slots / 4 - 1;
+  p.hshift = 64 - __builtin_ctzll((unsigned long long)(t->slots / 4));
+  p.side = t->slots / 4;
   p.pkey = *probe_key;
   p.join_type = join_type;
-  p.nbp = nbp;
+  p.nbp = t->nbp;
   p.npp = npp;
+  p.n_inline = t->n_inline;
+  p.lean = join_type == GHB_INNER_JOIN && npp == 0 && t->nbp == t->n_inline;
+  for (int j = 0; j < t->n_inline && p.lean; j++) p.lean = t->pay[j].null_mode == GHB_NULLS_NONE;
   p.out_prow = out_probe_rowid;
   p.out_brow = out_build_rowid;
   p.n = probe_key->n;
-  p.ntiles = (p.n + kJTile - 1) / kJTile;
+  p.nchunks = (p.n + kChunk - 1) / kChunk;
   p.cap = out_capacity;
   p.d_out_rows = d_out_rows;
-  p.counters = ctx->d_counters;
   p.status = ctx->d_status;
-  if (p.ntiles == 0) {
+  if (p.nchunks == 0) {
     GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_out_rows, 0, sizeof(int64_t), stream));
     return GHB_OK;
   }
-  st = lookback_prepare(ctx, p.ntiles, &p.epoch, stream);
-  if (st) return st;
-  p.lb = ctx->lb_status;
+  if ((st = scratch_alloc(ctx, (size_t)p.n * 4, (void**)&p.slot_of_row, stream))) return st;
+  if ((st = scratch_alloc(ctx, (size_t)p.nchunks * 8, (void**)&p.chunk_count, stream))) return st;
+  // CTA shape (threads x rows per thread, one 1024-row chunk either way),
+  // chosen by the build's ghb_join_cfg.block_threads
+  const int threads = t->probe_threads == 128 || t->probe_threads == 512 ? t->probe_threads : 256;
+  const bool kint = probe_key->type == GHB_INT, knull = probe_key->null_mode != GHB_NULLS_NONE;
+  void (*count_kernel)(ProbeParams) = nullptr;
+  void (*write_kernel)(ProbeParams) = nullptr;
+#define GHB_COUNT(TH, IT)                                                                   \
+  count_kernel = kint ? (knull ? join_count_kernel<TH, IT, true, true> : join_count_kernel<TH, IT, true, false>) \
+                      : (knull ? join_count_kernel<TH, IT, false, true> : join_count_kernel<TH, IT, false, false>); \
+  write_kernel = join_write_kernel<TH, IT>
+  if (threads == 128) { GHB_COUNT(128, 8); }
+  else if (threads == 512) { GHB_COUNT(512, 2); }
+  else { GHB_COUNT(256, 4); }
+#undef GHB_COUNT
   int per_sm = 0;
-  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, join_probe_kernel, kJThreads, 0));
-  int grid = (int)std::min<int64_t>(p.ntiles, (int64_t)ctx->num_sms * std::max(1, per_sm));
-  join_probe_kernel<<<grid, kJThreads, 0, stream>>>(p);
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, count_kernel, threads, 0));
+  int grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  count_kernel<<<grid, threads, 0, stream>>>(p);
+  GHB_LAUNCH_CHECK(ctx);
+  join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, p.nchunks, d_out_rows);
+  GHB_LAUNCH_CHECK(ctx);
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, write_kernel, threads, 0));
+  grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  write_kernel<<<grid, threads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;
 }
@@ -412,10 +644,12 @@ using namespace ghb;
 
 extern "C" {
 
-int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key, const ghb_join_cfg* cfg,
-                       ghb_join_table** out, void* stream) {
+int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* build_payload,
+                       int32_t n_build_payload, const ghb_join_cfg* cfg, ghb_join_table** out,
+                       void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
-  return join_build_impl(ctx, build_key, cfg, out, (cudaStream_t)stream);
+  return join_build_impl(ctx, build_key, build_payload, n_build_payload, cfg, out,
+                         (cudaStream_t)stream);
 }
 
 int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table) {
@@ -445,16 +679,18 @@ int32_t ghb_join_table_info(ghb_ctx* ctx, const ghb_join_table* table, int64_t* 
 }
 
 int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table, const ghb_column* probe_key,
-                       int32_t join_type, const ghb_column* build_payload, int32_t n_build_payload,
-                       ghb_out_column* out_build, const ghb_column* probe_payload,
+                       int32_t join_type, ghb_out_column* out_build, const ghb_column* probe_payload,
                        int32_t n_probe_payload, ghb_out_column* out_probe, int32_t* out_probe_rowid,
                        int32_t* out_build_rowid, int64_t out_capacity, int64_t* d_out_rows,
                        void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
   scratch_reset(ctx);
-  return join_probe_impl(ctx, table, probe_key, join_type, build_payload, n_build_payload, out_build,
-                         probe_payload, n_probe_payload, out_probe, out_probe_rowid, out_build_rowid,
-                         out_capacity, d_out_rows, (cudaStream_t)stream);
+  int64_t n = probe_key ? probe_key->n : 0;
+  int32_t st = scratch_reserve(ctx, join_probe_scratch_bytes(n), (cudaStream_t)stream);
+  if (st) return st;
+  return join_probe_impl(ctx, table, probe_key, join_type, out_build, probe_payload, n_probe_payload,
+                         out_probe, out_probe_rowid, out_build_rowid, out_capacity, d_out_rows,
+                         (cudaStream_t)stream);
 }
 
 }  // extern "C"

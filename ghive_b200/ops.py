@@ -239,33 +239,37 @@ class Context:
         res = outs.rows(min(g, cap))
         return res[:len(keys)], res[len(keys):], g
 
-    def join_build(self, key, load_factor=0.5, l2_persist=False, stream=None):
-        cs = _Cols([key])
+    def join_build(self, key, build_payload=(), load_factor=0.0, l2_persist=False, stream=None):
+        """Builds the device hash table; it keeps the build payload columns
+        (the first two inline in its slots), which must outlive the table."""
+        cs, bp = _Cols([key]), _Cols(build_payload)
         cfg = abi.JoinCfg()
         cfg.load_factor, cfg.l2_persist = load_factor, 1 if l2_persist else 0
         h = C.c_void_p()
-        self._check(lib().ghb_join_build(self.h, cs.ptr, C.byref(cfg), C.byref(h), _stream(stream)))
-        return JoinTable(self, h, cs[0].n, cs)
+        self._check(lib().ghb_join_build(self.h, cs.ptr, bp.ptr, bp.n, C.byref(cfg), C.byref(h),
+                                         _stream(stream)))
+        t = JoinTable(self, h, cs[0].n, (cs, bp))
+        t.payload_types = [bp[j].type for j in range(bp.n)]
+        return t
 
-    def join_probe(self, table, probe_key, join_type=abi.INNER_JOIN, build_payload=(),
-                   probe_payload=(), capacity=None, rowids=True, stream=None, sync=True,
-                   outs=None):
+    def join_probe(self, table, probe_key, join_type=abi.INNER_JOIN, probe_payload=(),
+                   capacity=None, rowids=True, stream=None, sync=True, outs=None):
         pk = _Cols([probe_key])
-        bp, ppl = _Cols(build_payload), _Cols(probe_payload)
+        ppl = _Cols(probe_payload)
         n = pk[0].n
         if capacity is None:
             _, dup, _ = table.info()
             capacity = max(1, n * max(1, dup))
         if outs is None:
-            ob = _Outs([bp[j].type for j in range(bp.n)], capacity, self.torch_device)
+            ob = _Outs(table.payload_types, capacity, self.torch_device)
             op = _Outs([ppl[j].type for j in range(ppl.n)], capacity, self.torch_device)
             prow = torch.empty(capacity, dtype=torch.int32, device=self.torch_device) if rowids else None
             brow = torch.empty(capacity, dtype=torch.int32, device=self.torch_device) if rowids else None
             d_rows = torch.zeros(1, dtype=torch.int64, device=self.torch_device)
             outs = (ob, op, prow, brow, d_rows)
         ob, op, prow, brow, d_rows = outs
-        self._check(lib().ghb_join_probe(self.h, table.handle, pk.ptr, join_type, bp.ptr, bp.n,
-                                         ob.ptr, ppl.ptr, ppl.n, op.ptr, _ptr(prow), _ptr(brow),
+        self._check(lib().ghb_join_probe(self.h, table.handle, pk.ptr, join_type, ob.ptr,
+                                         ppl.ptr, ppl.n, op.ptr, _ptr(prow), _ptr(brow),
                                          capacity, d_rows.data_ptr(), _stream(stream)))
         if not sync:
             return outs

@@ -236,11 +236,17 @@ int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred,
  * Replaces the sort + CPU merge of SortMergeJoinPredicate::process
  * (SortMergeJoinPredicate.cu:8-461) and the host gather of
  * BaseJoinPredicate::generate_result (BaseJoinPredicate.cu:4-97) with a
- * device hash join on one LONG or INT key.  The table keeps build row ids;
- * it stays resident on the device until ghb_join_table_free, so one build
- * serves many probes (a broadcast map-join small table).  NULL build keys
- * are not inserted; NULL probe keys never match. */
+ * device hash join on one LONG or INT key.  Like Hive's hash map, which
+ * stores each build row's retained values with its key
+ * (VectorMapJoinFastLongHashMap.java:71-84), the table holds the build
+ * payload columns: the first build row of every key is copied into its slot
+ * (up to two 8-byte non-BYTEMAP payloads), the others are read from the
+ * build_payload columns, which must stay valid until the table is freed.
+ * The table stays resident on the device until ghb_join_table_free, so one
+ * build serves many probes (a broadcast map-join small table).  NULL build
+ * keys are not inserted; NULL probe keys never match. */
 int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key,
+                       const ghb_column* build_payload, int32_t n_build_payload,
                        const ghb_join_cfg* cfg, ghb_join_table** out,
                        void* stream);
 int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table);
@@ -255,13 +261,13 @@ int32_t ghb_join_table_info(ghb_ctx* ctx, const ghb_join_table* table,
  * each optional (NULL to skip):
  *   out_probe_rowid[i]  probe row index (int32)
  *   out_build_rowid[i]  build row index (int32; -1 for an outer-join miss)
- *   out_build[j]        build_payload[j] gathered at the build row
- *                       (NULL in is_null / sentinel for an outer miss)
+ *   out_build[j]        the table's build payload j at the build row
+ *                       (NULL in is_null / sentinel for an outer miss);
+ *                       an array of the table's n_build_payload columns
  *   out_probe[j]        probe_payload[j] gathered at the probe row
  * d_out_rows (device int64) receives the number of output rows. */
 int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table,
                        const ghb_column* probe_key, int32_t join_type,
-                       const ghb_column* build_payload, int32_t n_build_payload,
                        ghb_out_column* out_build,
                        const ghb_column* probe_payload, int32_t n_probe_payload,
                        ghb_out_column* out_probe,

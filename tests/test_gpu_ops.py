@@ -319,9 +319,9 @@ def test_groupby_repeat_is_stable(ctx):
 # ------------------------------------------------------------------- join
 def _check_join(ctx, bkey, pkey, jt=abi.INNER_JOIN, bpay=(), ppay=()):
     pr, br = oracle.hash_join(bkey, pkey, jt)
-    t = ctx.join_build(dev(bkey))
-    r = ctx.join_probe(t, dev(pkey), jt, build_payload=[dev(c) for c in bpay],
-                       probe_payload=[dev(c) for c in ppay])
+    dbp = [dev(c) for c in bpay]  # the table keeps these columns: they outlive it
+    t = ctx.join_build(dev(bkey), build_payload=dbp)
+    r = ctx.join_probe(t, dev(pkey), jt, probe_payload=[dev(c) for c in ppay])
     assert r["rows"] == len(pr)
     gp, gb = host(r["probe_rowid"]), host(r["build_rowid"])
     assert np.all(np.diff(gp) >= 0)  # probe-row order
