@@ -3,13 +3,17 @@
 // Replaces GroupByPredicate::gpu_execute (gpu_impl/src/Operator/
 // GroupByPredicate.cu:19-359), which sorted row indices with a comparison
 // sort and then ran one H2D + reduce_by_key + D2H pass per aggregate
-// (:506-720).  Here one pass over the rows evaluates the filter predicate in
-// registers and folds every aggregate of the row into a hash table:
+// (:506-720).  Here one pass over the rows evaluates the filter predicate and
+// folds every aggregate of the row into a hash table:
 //
-//   G1  persistent CTAs; each folds its rows into a shared-memory open-
-//       addressing table (keys + one 64-bit accumulator per aggregate state);
-//       rows whose key does not fit go straight to the global table; at the
-//       end the CTA merges its shared table into the global one.
+//   G1  persistent CTAs; each streams 2048-row tiles of the columns it needs
+//       into shared memory with bulk copies (cp.async.bulk, completing on an
+//       mbarrier, two stages so the next tile loads while this one is
+//       folded), evaluates the predicate from shared memory, and folds each
+//       passing row into a shared-memory open-addressing table (keys + one
+//       64-bit accumulator per aggregate state); rows whose key does not fit
+//       go straight to the global table; at the end the CTA merges its shared
+//       table into the global one.
 //   G2  finalize: walks the global table, emits one output row per group
 //       (COUNT, SUM, AVG = sum/count, MIN, MAX with Hive's NULL rules) and
 //       zeroes every slot it read, so the next call needs no memset.
@@ -39,6 +43,7 @@ enum AccKind : int8_t {
 };
 constexpr int kMaxAcc = 16;
 constexpr int kMaxAggs = 16;
+constexpr int kGbThreads = 1024;
 
 struct AccPlan {
   int32_t n_acc;
@@ -64,9 +69,18 @@ struct GbParams {
   uint64_t* gkeys;       // [C + 2] stored keys (flip_i64 of the raw key), 0 = empty
   uint64_t* gacc;        // [n_acc][C + 2]
   int64_t C;             // power of two
+  int32_t gshift;        // 64 - log2(C)
   int32_t gprobe;        // probe limit in the global table
   int32_t* status;
   int64_t* d_out_groups;
+  // column tiles in shared memory
+  int32_t tile_rows;     // rows per tile (multiple of the block size and of 4)
+  int64_t ntiles;
+  int32_t stage_bytes;   // bytes of one stage (128-byte multiple)
+  int32_t tx_bytes;      // bytes the bulk copies of one full tile deliver
+  int32_t col_off[kMaxCols];   // byte offset of a used column's tile in a stage, -1 unused
+  int32_t null_off[kMaxCols];  // byte offset of a BYTEMAP column's null bytes, -1 none
+  int32_t bulk;          // column bases are 16-byte aligned: full tiles arrive by bulk copy
 };
 
 struct FinParams {
@@ -103,11 +117,16 @@ __device__ __forceinline__ uint64_t order_image(int type, int64_t raw) {
   return type == GHB_DOUBLE ? flip_f64_bits((uint64_t)raw) : flip_i64(raw);
 }
 
+// Slot of a key image in a table of 2^(64 - shift) slots: Fibonacci hashing.
+__device__ __forceinline__ int64_t hslot(uint64_t u, int shift) {
+  return (int64_t)((u * 0x9E3779B97F4A7C15ull) >> shift);
+}
+
 // Open-addressing find-or-insert of a non-zero stored key.  Linear probing;
 // returns the slot or -1 after max_probe probes.
-__device__ __forceinline__ int64_t table_insert(uint64_t* keys, int64_t mask, uint64_t u,
+__device__ __forceinline__ int64_t table_insert(uint64_t* keys, int64_t mask, int shift, uint64_t u,
                                                 int max_probe) {
-  int64_t h = (int64_t)(mix64(u) & (uint64_t)mask);
+  int64_t h = hslot(u, shift);
   for (int p = 0; p < max_probe; p++) {
     uint64_t cur = keys[h];
     if (cur == u) return h;
@@ -120,44 +139,108 @@ __device__ __forceinline__ int64_t table_insert(uint64_t* keys, int64_t mask, ui
   return -1;
 }
 
-// Folds row r into the accumulators at `slot` (stride = slots per accumulator).
-__device__ __forceinline__ void acc_row(const GbParams& p, uint64_t* acc, int64_t stride,
-                                        int64_t slot, int64_t r) {
-  for (int a = 0; a < p.acc.n_acc; a++) {
-    uint64_t* cell = acc + a * stride + slot;
-    int8_t kind = p.acc.kind[a];
-    if (kind == A_CNT_STAR) { atomicAdd((unsigned long long*)cell, 1ull); continue; }
-    if (kind == A_COMP_F) continue;
-    const ghb_column& c = p.cols.c[p.acc.col[a]];
-    int64_t v = ld_raw(c, r);
-    if (raw_is_null(c, v, r)) continue;
-    switch (kind) {
-      case A_CNT_NN: atomicAdd((unsigned long long*)cell, 1ull); break;
-      case A_SUM_I: atomicAdd((unsigned long long*)cell, (unsigned long long)v); break;
-      case A_SUM_F: atomic_add_comp(cell, cell + stride, raw_to_f64(c.type, v)); break;
-      case A_MAX_O: atomicMax((unsigned long long*)cell, (unsigned long long)order_image(c.type, v)); break;
-      case A_MIN_O: atomicMax((unsigned long long*)cell, (unsigned long long)~order_image(c.type, v)); break;
-    }
+// One row of the current tile, read from shared memory.
+struct TileRow {
+  const GbParams* p;
+  const unsigned char* stage;
+  int r;
+  __device__ __forceinline__ int64_t raw(int c) const {
+    const unsigned char* b = stage + p->col_off[c];
+    return p->cols.c[c].type == GHB_INT ? (int64_t)((const int32_t*)b)[r] : ((const long long*)b)[r];
   }
+  __device__ __forceinline__ bool null(int c, int64_t v) const {
+    const ghb_column& col = p->cols.c[c];
+    if (col.null_mode == GHB_NULLS_NONE) return false;
+    if (col.null_mode == GHB_NULLS_BYTEMAP) return stage[p->null_off[c] + r] != 0;
+    if (col.type == GHB_INT) return v == (int64_t)INT32_MAX;
+    if (col.type == GHB_LONG) return v == INT64_MAX;
+    double d = __longlong_as_double(v);
+    return d != d;
+  }
+};
+
+__device__ __forceinline__ bool leaf_tile(const ghb_pred_node& nd, const TileRow& t) {
+  const int type = t.p->cols.c[nd.col].type;
+  int64_t x = t.raw(nd.col);
+  if (t.null(nd.col, x)) return false;
+  if (nd.mode == GHB_FILTER_NOT_NULL) return true;
+  if (nd.col2 >= 0) {
+    const int type2 = t.p->cols.c[nd.col2].type;
+    int64_t y = t.raw(nd.col2);
+    if (t.null(nd.col2, y)) return false;
+    if (type == GHB_DOUBLE || type2 == GHB_DOUBLE)
+      return cmp_mode<double>(nd.mode, raw_to_f64(type, x), raw_to_f64(type2, y), 0.0);
+    return cmp_mode<int64_t>(nd.mode, x, y, 0);
+  }
+  if (type == GHB_DOUBLE || nd.lit_is_double) {
+    double a = nd.lit_is_double ? nd.lit_d[0] : (double)nd.lit_i[0];
+    double b = nd.lit_is_double ? nd.lit_d[1] : (double)nd.lit_i[1];
+    return cmp_mode<double>(nd.mode, raw_to_f64(type, x), a, b);
+  }
+  return cmp_mode<int64_t>(nd.mode, x, nd.lit_i[0], nd.lit_i[1]);
+}
+
+__device__ __forceinline__ bool pred_tile(const PredProg& pp, const TileRow& t) {
+  if (pp.n_nodes == 0) return true;
+  if (pp.n_nodes == 1) return leaf_tile(pp.nodes[0], t);
+  uint32_t bits = 0;
+  for (int k = 0; k < pp.n_nodes; k++) {
+    const ghb_pred_node& nd = pp.nodes[k];
+    bool r;
+    if (nd.mode == GHB_FILTER_AND)
+      r = ((bits >> nd.child[0]) & (bits >> nd.child[1]) & 1u) != 0;
+    else if (nd.mode == GHB_FILTER_OR)
+      r = (((bits >> nd.child[0]) | (bits >> nd.child[1])) & 1u) != 0;
+    else
+      r = leaf_tile(nd, t);
+    bits |= (uint32_t)r << k;
+  }
+  return (bits >> (pp.n_nodes - 1)) & 1u;
 }
 
 // Row contribution of accumulator a as a 64-bit word (0 = no contribution).
-__device__ __forceinline__ uint64_t acc_contrib(const GbParams& p, int a, int64_t r, bool live) {
-  if (!live) return 0;
+__device__ __forceinline__ uint64_t acc_contrib(const GbParams& p, int a, const TileRow& t) {
   int8_t kind = p.acc.kind[a];
   if (kind == A_CNT_STAR) return 1;
   if (kind == A_COMP_F) return 0;
-  const ghb_column& c = p.cols.c[p.acc.col[a]];
-  int64_t v = ld_raw(c, r);
-  if (raw_is_null(c, v, r)) return 0;
+  const int c = p.acc.col[a];
+  int64_t v = t.raw(c);
+  if (t.null(c, v)) return 0;
+  const int type = p.cols.c[c].type;
   switch (kind) {
     case A_CNT_NN: return 1;
     case A_SUM_I: return (uint64_t)v;
-    case A_SUM_F: return (uint64_t)__double_as_longlong(raw_to_f64(c.type, v));
-    case A_MAX_O: return order_image(c.type, v);
-    case A_MIN_O: return ~order_image(c.type, v);
+    case A_SUM_F: return (uint64_t)__double_as_longlong(raw_to_f64(type, v));
+    case A_MAX_O: return order_image(type, v);
+    case A_MIN_O: return ~order_image(type, v);
   }
   return 0;
+}
+
+// Folds one row into the accumulators at `slot` (stride = slots per accumulator).
+__device__ __forceinline__ void acc_row(const GbParams& p, uint64_t* acc, int64_t stride, int64_t slot,
+                                        const TileRow& t) {
+  for (int a = 0; a < p.acc.n_acc; a++) {
+    int8_t kind = p.acc.kind[a];
+    if (kind == A_COMP_F) continue;
+    uint64_t w = acc_contrib(p, a, t);
+    uint64_t* cell = acc + a * stride + slot;
+    switch (kind) {
+      case A_CNT_STAR:
+        atomicAdd((unsigned long long*)cell, 1ull);
+        break;
+      case A_CNT_NN:
+      case A_SUM_I:
+        if (w) atomicAdd((unsigned long long*)cell, (unsigned long long)w);
+        break;
+      case A_SUM_F:
+        atomic_add_comp(cell, cell + stride, __longlong_as_double(w));
+        break;
+      default:  // MIN / MAX images: 0 never wins
+        if (w) atomicMax((unsigned long long*)cell, (unsigned long long)w);
+        break;
+    }
+  }
 }
 
 // Merges one partial accumulator word `w` (and its compensation `wc`) into a cell.
@@ -185,7 +268,7 @@ __device__ __forceinline__ void acc_merge(int8_t kind, uint64_t* cell, int64_t s
 // contributions through a per-warp staging row, then the lowest such lane
 // applies one atomic per accumulator.
 __device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, int64_t stride,
-                                             int64_t slot, int64_t r, bool live,
+                                             int64_t slot, const TileRow& t, bool live,
                                              uint64_t* stage) {
   const int lane = threadIdx.x & 31;
   unsigned peers = __match_any_sync(0xffffffffu, live ? slot : -1);
@@ -193,7 +276,7 @@ __device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, i
   for (int a = 0; a < p.acc.n_acc; a++) {
     int8_t kind = p.acc.kind[a];
     if (kind == A_COMP_F) continue;
-    uint64_t w = acc_contrib(p, a, r, live);
+    uint64_t w = live ? acc_contrib(p, a, t) : 0;
     stage[lane] = w;
     __syncwarp();
     if (live && lane == leader) {
@@ -207,9 +290,9 @@ __device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, i
           case A_SUM_I: tot += x; break;
           case A_SUM_F: {
             double xv = __longlong_as_double(x);
-            double t = __dadd_rn(s, xv);
-            c = __dadd_rn(c, two_sum_err(s, xv, t));
-            s = t;
+            double tt = __dadd_rn(s, xv);
+            c = __dadd_rn(c, two_sum_err(s, xv, tt));
+            s = tt;
             break;
           }
           default: tot = max(tot, x); break;
@@ -225,61 +308,150 @@ __device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, i
   }
 }
 
+// Loads tile `tile` into the stage at `stage` with plain loads by all
+// threads (a partial last tile, or unaligned columns).  Ends with a barrier.
+__device__ __forceinline__ void load_tile_plain(const GbParams& p, unsigned char* stage, int64_t tile) {
+  const int64_t base = tile * p.tile_rows;
+  const int rows = (int)min((int64_t)p.tile_rows, p.n - base);
+  for (int c = 0; c < p.cols.n; c++) {
+    if (p.col_off[c] < 0) continue;
+    const ghb_column& col = p.cols.c[c];
+    if (col.type == GHB_INT) {
+      int32_t* d = (int32_t*)(stage + p.col_off[c]);
+      for (int r = threadIdx.x; r < rows; r += blockDim.x) d[r] = __ldcs((const int*)col.data + base + r);
+    } else {
+      long long* d = (long long*)(stage + p.col_off[c]);
+      for (int r = threadIdx.x; r < rows; r += blockDim.x) d[r] = __ldcs((const long long*)col.data + base + r);
+    }
+    if (p.null_off[c] >= 0)
+      for (int r = threadIdx.x; r < rows; r += blockDim.x) stage[p.null_off[c] + r] = col.is_null[base + r];
+  }
+  __syncthreads();
+}
+
+// Thread 0: issues the bulk copies of full tile `tile` into `stage`.
+__device__ __forceinline__ void load_tile_bulk(const GbParams& p, unsigned char* stage, int64_t tile,
+                                               uint64_t* bar) {
+  const int64_t base = tile * p.tile_rows;
+  mbar_expect_tx(bar, (uint32_t)p.tx_bytes);
+  for (int c = 0; c < p.cols.n; c++) {
+    if (p.col_off[c] < 0) continue;
+    const ghb_column& col = p.cols.c[c];
+    const int w = col.type == GHB_INT ? 4 : 8;
+    bulk_g2s(stage + p.col_off[c], (const unsigned char*)col.data + base * w, (uint32_t)(p.tile_rows * w), bar);
+    if (p.null_off[c] >= 0)
+      bulk_g2s(stage + p.null_off[c], col.is_null + base, (uint32_t)p.tile_rows, bar);
+  }
+}
+
 template <bool KEYED>
-__global__ void __launch_bounds__(1024) gb_fold_kernel(GbParams p) {
-  extern __shared__ uint64_t smem[];
+__global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int S = p.smem_slots;
   const int64_t sstride = S + 2;
-  uint64_t* skeys = smem;
-  uint64_t* sacc = smem + sstride;
-  uint64_t* stage = sacc + (int64_t)p.acc.n_acc * sstride + (threadIdx.x >> 5) * 32;
+  // layout: [stage 0][stage 1][mbarriers][hash keys + accumulators][warp staging]
+  // stage s starts at smem_raw + s * stage_bytes
+  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)p.stage_bytes);
+  uint64_t* skeys = bars + 2;
+  uint64_t* sacc = skeys + sstride;
+  uint64_t* wstage = sacc + (int64_t)p.acc.n_acc * sstride + (threadIdx.x >> 5) * 32;
   const int64_t gstride = p.C + 2;
+  const int smask_shift = S > 0 ? 64 - __ffs(S) + 1 : 0;   // 64 - log2(S)
 
-  for (int64_t i = threadIdx.x; i < sstride * (1 + p.acc.n_acc); i += blockDim.x) smem[i] = 0;
+  for (int64_t i = threadIdx.x; i < sstride * (1 + p.acc.n_acc); i += blockDim.x) skeys[i] = 0;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) *p.d_out_groups = 0;
   __syncthreads();
 
-  // Warp-uniform trip count so the warp-cooperative path can use all lanes.
-  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  const int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t iters = (p.n + nthreads - 1) / nthreads;
-  for (int64_t it = 0; it < iters; it++) {
-    int64_t r = first + it * nthreads;
-    bool live = r < p.n && eval_pred(p.pred, p.cols, r);
-    uint64_t u = 0;
-    int side = -1;  // 0: key INT64_MIN, 1: NULL key / global aggregate
-    if (live) {
-      if (KEYED) {
-        const ghb_column& kc = p.cols.c[p.key_col];
-        int64_t raw = ld_raw(kc, r);
-        if (raw_is_null(kc, raw, r)) side = 1;
-        else {
-          u = flip_i64(raw);
-          if (u == 0) side = 0;
+  // stage s holds tile blockIdx.x + i * gridDim.x for the i with i % 2 == s
+  auto full = [&](int64_t tile) { return (tile + 1) * p.tile_rows <= p.n; };
+  uint32_t pending = 0, phase = 0;   // per stage s: bit s = a bulk copy is in flight / its parity
+  bool failed = false;
+  for (int s = 0; s < 2; s++) {
+    int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
+    if (tile >= p.ntiles) break;
+    if (p.bulk && full(tile)) {
+      if (threadIdx.x == 0) load_tile_bulk(p, smem_raw + s * p.stage_bytes, tile, &bars[s]);
+      pending |= 1u << s;
+    } else {
+      load_tile_plain(p, smem_raw + s * p.stage_bytes, tile);
+    }
+  }
+
+  for (int64_t it = 0;; it++) {
+    const int64_t tile = blockIdx.x + it * gridDim.x;
+    if (tile >= p.ntiles) break;
+    const int s = (int)(it & 1);
+    if ((pending >> s) & 1u) {
+      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
+      // one decision for the whole CTA: every thread leaves or none does
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      phase ^= 1u << s;
+      pending &= ~(1u << s);
+    }
+    const unsigned char* stage = smem_raw + s * p.stage_bytes;
+    const int rows = (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows);
+    // warp-uniform trip count so the warp-cooperative path can use all lanes
+    for (int r0 = 0; r0 < p.tile_rows; r0 += blockDim.x) {
+      const int r = r0 + threadIdx.x;
+      TileRow t{&p, stage, r};
+      bool live = r < rows && pred_tile(p.pred, t);
+      uint64_t u = 0;
+      int side = -1;  // 0: key INT64_MIN, 1: NULL key / global aggregate
+      if (live) {
+        if (KEYED) {
+          int64_t raw = t.raw(p.key_col);
+          if (t.null(p.key_col, raw)) side = 1;
+          else {
+            u = flip_i64(raw);
+            if (u == 0) side = 0;
+          }
+        } else {
+          side = 1;
         }
+      }
+      int64_t sslot = -1;
+      if (live && S > 0) sslot = side >= 0 ? S + side : table_insert(skeys, S - 1, smask_shift, u, 8);
+      if (p.warp_agg) {
+        bool in_smem = live && sslot >= 0;
+        if (__any_sync(0xffffffffu, in_smem))
+          acc_row_warp(p, sacc, sstride, in_smem ? sslot : 0, t, in_smem, wstage);
+      } else if (live && sslot >= 0) {
+        acc_row(p, sacc, sstride, sslot, t);
+      }
+      if (live && sslot < 0) {
+        int64_t g = side >= 0 ? p.C + side : table_insert(p.gkeys, p.C - 1, p.gshift, u, p.gprobe);
+        if (g < 0) raise_status(p.status, kDevCapacity);
+        else acc_row(p, p.gacc, gstride, g, t);
+      }
+    }
+    __syncthreads();  // every thread is done with this stage
+    const int64_t next = tile + 2 * (int64_t)gridDim.x;
+    if (next < p.ntiles) {
+      if (p.bulk && full(next)) {
+        if (threadIdx.x == 0) {
+          fence_proxy_async_smem();
+          load_tile_bulk(p, smem_raw + s * p.stage_bytes, next, &bars[s]);
+        }
+        pending |= 1u << s;
       } else {
-        side = 1;
+        load_tile_plain(p, smem_raw + s * p.stage_bytes, next);
       }
     }
-    int64_t sslot = -1;
-    if (live && S > 0) {
-      sslot = side >= 0 ? S + side : table_insert(skeys, S - 1, u, 8);
-    }
-    if (p.warp_agg) {
-      bool in_smem = live && sslot >= 0;
-      if (__any_sync(0xffffffffu, in_smem))
-        acc_row_warp(p, sacc, sstride, in_smem ? sslot : 0, r, in_smem, stage);
-    } else if (live && sslot >= 0) {
-      acc_row(p, sacc, sstride, sslot, r);
-    }
-    if (live && sslot < 0) {
-      int64_t g = side >= 0 ? p.C + side : table_insert(p.gkeys, p.C - 1, u, p.gprobe);
-      if (g < 0) {
-        raise_status(p.status, kDevCapacity);
-        continue;
-      }
-      acc_row(p, p.gacc, gstride, g, r);
-    }
+  }
+  if (failed) {
+    // a bulk copy never completed: wait (bounded) for the other stage's copy
+    // before the CTA's shared memory goes away
+    for (int s = 0; s < 2; s++)
+      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
+    return;
   }
   __syncthreads();
 
@@ -288,7 +460,7 @@ __global__ void __launch_bounds__(1024) gb_fold_kernel(GbParams p) {
     if (sacc[s] == 0) continue;  // accumulator 0 is COUNT(*): empty slot
     int64_t g;
     if (s < S) {
-      g = table_insert(p.gkeys, p.C - 1, skeys[s], p.gprobe);
+      g = table_insert(p.gkeys, p.C - 1, p.gshift, skeys[s], p.gprobe);
       if (g < 0) {
         raise_status(p.status, kDevCapacity);
         continue;
@@ -471,7 +643,13 @@ static int64_t next_pow2(int64_t v) {
   return p;
 }
 
-// Shared implementation; `table` (nullable) overrides the context's table.
+static int log2_exact(int64_t v) {
+  int l = 0;
+  while ((1ll << l) < v) l++;
+  return l;
+}
+
+// Shared implementation; `fixed_table` (nullable) replaces the context's table.
 int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
                             int32_t ncols, const int32_t* key_cols, int32_t nkeys,
                             const ghb_agg_desc* aggs, int32_t naggs, ghb_out_column* out,
@@ -511,6 +689,18 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
     if (!out[0].data) return set_error(ctx, GHB_ERR_INVALID, "key output data is NULL");
   }
 
+  // columns the kernel reads: predicate leaves, the key, aggregate inputs
+  bool used[kMaxCols] = {false};
+  for (int k = 0; k < p.pred.n_nodes; k++) {
+    const ghb_pred_node& nd = p.pred.nodes[k];
+    if (nd.mode == GHB_FILTER_AND || nd.mode == GHB_FILTER_OR) continue;
+    used[nd.col] = true;
+    if (nd.col2 >= 0) used[nd.col2] = true;
+  }
+  if (nkeys) used[key_cols[0]] = true;
+  for (int a = 0; a < p.acc.n_acc; a++)
+    if (p.acc.col[a] >= 0) used[p.acc.col[a]] = true;
+
   int64_t max_groups = (cfg && cfg->max_groups > 0) ? cfg->max_groups : out_capacity;
   if (nkeys == 0) max_groups = 1;
   max_groups = std::min<int64_t>(max_groups, std::max<int64_t>(n, 1));
@@ -521,15 +711,46 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   else if (cfg && cfg->smem_slots > 0) S = (int)next_pow2(cfg->smem_slots);
   else S = (int)std::min<int64_t>(4096, next_pow2(std::max<int64_t>(2 * max_groups, 64)));
   if (nkeys == 0) S = 64;
-  int threads = (cfg && cfg->block_threads > 0) ? cfg->block_threads : 1024;
-  threads = std::max(64, std::min(1024, threads / 32 * 32));
-  size_t smem = (size_t)(S + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8;
-  while (smem > 200 * 1024 && S > 64) {
-    S /= 2;
-    smem = (size_t)(S + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8;
-  }
+  const int threads = kGbThreads;
+
+  // tile rows: as large as shared memory allows next to the hash table
+  size_t row_bytes = 0;
+  for (int c = 0; c < ncols; c++)
+    if (used[c]) row_bytes += type_width(cols[c].type) + (cols[c].null_mode == GHB_NULLS_BYTEMAP ? 1 : 0);
+  const size_t smem_cap = 225 * 1024;
+  auto table_bytes_smem = [&](int s) {
+    return (size_t)(s + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8 + 64;
+  };
+  int tile_rows = 2048;
+  while (S > 64 && table_bytes_smem(S) + 2 * row_bytes * 1024 > smem_cap) S /= 2;
+  while (tile_rows > threads && table_bytes_smem(S) + 2 * row_bytes * tile_rows > smem_cap) tile_rows /= 2;
+  if (table_bytes_smem(S) + 2 * row_bytes * tile_rows > smem_cap)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "rows of %zu bytes do not fit a shared-memory tile", row_bytes);
   p.smem_slots = S;
   p.warp_agg = (nkeys == 0 || max_groups <= 64) ? 1 : 0;
+  p.tile_rows = tile_rows;
+  p.ntiles = (n + tile_rows - 1) / tile_rows;
+  int32_t off = 0;
+  bool aligned = true;
+  for (int c = 0; c < kMaxCols; c++) {
+    p.col_off[c] = -1;
+    p.null_off[c] = -1;
+  }
+  for (int c = 0; c < ncols; c++) {
+    if (!used[c]) continue;
+    p.col_off[c] = off;
+    off += (int32_t)(tile_rows * type_width(cols[c].type));
+    if ((uintptr_t)cols[c].data % 16) aligned = false;
+    if (cols[c].null_mode == GHB_NULLS_BYTEMAP) {
+      p.null_off[c] = off;
+      off += tile_rows;
+      if ((uintptr_t)cols[c].is_null % 16) aligned = false;
+    }
+  }
+  p.stage_bytes = (off + 127) & ~127;
+  p.tx_bytes = off;
+  p.bulk = aligned ? 1 : 0;
+  size_t smem = 2 * (size_t)p.stage_bytes + table_bytes_smem(S);
 
   size_t table_bytes = (size_t)(C + 2) * 8 * (1 + p.acc.n_acc);
   if (fixed_table) {
@@ -560,6 +781,7 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   }
   p.gacc = p.gkeys + (C + 2);
   p.C = C;
+  p.gshift = 64 - log2_exact(C);
   p.gprobe = (int32_t)std::min<int64_t>(C, 1 << 20);
   p.status = ctx->d_status;
   p.d_out_groups = d_out_groups;
@@ -570,8 +792,7 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kfn, threads, smem));
   blocks_per_sm = std::max(1, blocks_per_sm);
   if (cfg && cfg->ctas_per_sm > 0) blocks_per_sm = std::min(blocks_per_sm, cfg->ctas_per_sm);
-  int64_t want_blocks = (n + threads - 1) / threads;
-  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * blocks_per_sm, want_blocks));
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * blocks_per_sm, p.ntiles));
   kfn<<<grid, threads, smem, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
 
