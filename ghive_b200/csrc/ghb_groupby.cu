@@ -44,6 +44,7 @@ enum AccKind : int8_t {
 constexpr int kMaxAcc = 16;
 constexpr int kMaxAggs = 16;
 constexpr int kGbThreads = 1024;
+constexpr int kGbRows = 2;     // tile rows per thread at most (tile = 1024 or 2048 rows)
 
 struct AccPlan {
   int32_t n_acc;
@@ -198,51 +199,6 @@ __device__ __forceinline__ bool pred_tile(const PredProg& pp, const TileRow& t) 
   return (bits >> (pp.n_nodes - 1)) & 1u;
 }
 
-// Row contribution of accumulator a as a 64-bit word (0 = no contribution).
-__device__ __forceinline__ uint64_t acc_contrib(const GbParams& p, int a, const TileRow& t) {
-  int8_t kind = p.acc.kind[a];
-  if (kind == A_CNT_STAR) return 1;
-  if (kind == A_COMP_F) return 0;
-  const int c = p.acc.col[a];
-  int64_t v = t.raw(c);
-  if (t.null(c, v)) return 0;
-  const int type = p.cols.c[c].type;
-  switch (kind) {
-    case A_CNT_NN: return 1;
-    case A_SUM_I: return (uint64_t)v;
-    case A_SUM_F: return (uint64_t)__double_as_longlong(raw_to_f64(type, v));
-    case A_MAX_O: return order_image(type, v);
-    case A_MIN_O: return ~order_image(type, v);
-  }
-  return 0;
-}
-
-// Folds one row into the accumulators at `slot` (stride = slots per accumulator).
-__device__ __forceinline__ void acc_row(const GbParams& p, uint64_t* acc, int64_t stride, int64_t slot,
-                                        const TileRow& t) {
-  for (int a = 0; a < p.acc.n_acc; a++) {
-    int8_t kind = p.acc.kind[a];
-    if (kind == A_COMP_F) continue;
-    uint64_t w = acc_contrib(p, a, t);
-    uint64_t* cell = acc + a * stride + slot;
-    switch (kind) {
-      case A_CNT_STAR:
-        atomicAdd((unsigned long long*)cell, 1ull);
-        break;
-      case A_CNT_NN:
-      case A_SUM_I:
-        if (w) atomicAdd((unsigned long long*)cell, (unsigned long long)w);
-        break;
-      case A_SUM_F:
-        atomic_add_comp(cell, cell + stride, __longlong_as_double(w));
-        break;
-      default:  // MIN / MAX images: 0 never wins
-        if (w) atomicMax((unsigned long long*)cell, (unsigned long long)w);
-        break;
-    }
-  }
-}
-
 // Merges one partial accumulator word `w` (and its compensation `wc`) into a cell.
 __device__ __forceinline__ void acc_merge(int8_t kind, uint64_t* cell, int64_t stride, uint64_t w,
                                           uint64_t wc) {
@@ -261,50 +217,6 @@ __device__ __forceinline__ void acc_merge(int8_t kind, uint64_t* cell, int64_t s
       if (w) atomicMax((unsigned long long*)cell, (unsigned long long)w);
       break;
     default: break;
-  }
-}
-
-// Warp-cooperative fold: lanes holding the same slot combine their row
-// contributions through a per-warp staging row, then the lowest such lane
-// applies one atomic per accumulator.
-__device__ __forceinline__ void acc_row_warp(const GbParams& p, uint64_t* acc, int64_t stride,
-                                             int64_t slot, const TileRow& t, bool live,
-                                             uint64_t* stage) {
-  const int lane = threadIdx.x & 31;
-  unsigned peers = __match_any_sync(0xffffffffu, live ? slot : -1);
-  int leader = __ffs(peers) - 1;
-  for (int a = 0; a < p.acc.n_acc; a++) {
-    int8_t kind = p.acc.kind[a];
-    if (kind == A_COMP_F) continue;
-    uint64_t w = live ? acc_contrib(p, a, t) : 0;
-    stage[lane] = w;
-    __syncwarp();
-    if (live && lane == leader) {
-      uint64_t tot = 0, comp = 0;
-      double s = 0.0, c = 0.0;
-      for (unsigned m = peers; m; m &= m - 1) {
-        uint64_t x = stage[__ffs(m) - 1];
-        switch (kind) {
-          case A_CNT_STAR:
-          case A_CNT_NN:
-          case A_SUM_I: tot += x; break;
-          case A_SUM_F: {
-            double xv = __longlong_as_double(x);
-            double tt = __dadd_rn(s, xv);
-            c = __dadd_rn(c, two_sum_err(s, xv, tt));
-            s = tt;
-            break;
-          }
-          default: tot = max(tot, x); break;
-        }
-      }
-      if (kind == A_SUM_F) {
-        tot = (uint64_t)__double_as_longlong(s);
-        comp = (uint64_t)__double_as_longlong(c);
-      }
-      acc_merge(kind, acc + a * stride + slot, stride, tot, comp);
-    }
-    __syncwarp();
   }
 }
 
@@ -344,7 +256,7 @@ __device__ __forceinline__ void load_tile_bulk(const GbParams& p, unsigned char*
   }
 }
 
-template <bool KEYED>
+template <bool KEYED, bool NULLABLE>
 __global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int S = p.smem_slots;
@@ -398,17 +310,28 @@ __global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
     }
     const unsigned char* stage = smem_raw + s * p.stage_bytes;
     const int rows = (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows);
-    // warp-uniform trip count so the warp-cooperative path can use all lanes
-    for (int r0 = 0; r0 < p.tile_rows; r0 += blockDim.x) {
-      const int r = r0 + threadIdx.x;
+    // Phase A, per row: predicate, key, slot (shared table, else global).
+    // The trip counts are warp-uniform so the warp-cooperative path can use
+    // all lanes.
+    const int rpt = p.tile_rows / (int)blockDim.x;   // 1 or 2
+    int64_t slot[kGbRows];
+    bool live[kGbRows], in_s[kGbRows];
+    unsigned peers[kGbRows];
+#pragma unroll
+    for (int j = 0; j < kGbRows; j++) {
+      live[j] = in_s[j] = false;
+      slot[j] = -1;
+      peers[j] = 0;
+      if (j >= rpt) continue;
+      const int r = j * blockDim.x + threadIdx.x;
       TileRow t{&p, stage, r};
-      bool live = r < rows && pred_tile(p.pred, t);
+      bool lv = r < rows && pred_tile(p.pred, t);
       uint64_t u = 0;
       int side = -1;  // 0: key INT64_MIN, 1: NULL key / global aggregate
-      if (live) {
+      if (lv) {
         if (KEYED) {
           int64_t raw = t.raw(p.key_col);
-          if (t.null(p.key_col, raw)) side = 1;
+          if (NULLABLE && t.null(p.key_col, raw)) side = 1;
           else {
             u = flip_i64(raw);
             if (u == 0) side = 0;
@@ -417,19 +340,84 @@ __global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
           side = 1;
         }
       }
-      int64_t sslot = -1;
-      if (live && S > 0) sslot = side >= 0 ? S + side : table_insert(skeys, S - 1, smask_shift, u, 8);
-      if (p.warp_agg) {
-        bool in_smem = live && sslot >= 0;
-        if (__any_sync(0xffffffffu, in_smem))
-          acc_row_warp(p, sacc, sstride, in_smem ? sslot : 0, t, in_smem, wstage);
-      } else if (live && sslot >= 0) {
-        acc_row(p, sacc, sstride, sslot, t);
-      }
-      if (live && sslot < 0) {
+      int64_t ss = -1;
+      if (lv && S > 0) ss = side >= 0 ? S + side : table_insert(skeys, S - 1, smask_shift, u, 8);
+      if (lv && ss < 0) {
         int64_t g = side >= 0 ? p.C + side : table_insert(p.gkeys, p.C - 1, p.gshift, u, p.gprobe);
-        if (g < 0) raise_status(p.status, kDevCapacity);
-        else acc_row(p, p.gacc, gstride, g, t);
+        if (g < 0) {
+          raise_status(p.status, kDevCapacity);
+          lv = false;
+        }
+        slot[j] = g;
+      } else {
+        slot[j] = ss;
+      }
+      live[j] = lv;
+      in_s[j] = lv && ss >= 0;
+      if (p.warp_agg) peers[j] = __match_any_sync(0xffffffffu, in_s[j] ? ss : -1);
+    }
+    // Phase B, per accumulator: its kind and column type are the same for
+    // every row, so the branches are uniform; each row adds its contribution.
+    for (int a = 0; a < p.acc.n_acc; a++) {
+      const int8_t kind = p.acc.kind[a];
+      if (kind == A_COMP_F) continue;
+      const int c = p.acc.col[a];
+      const int type = kind == A_CNT_STAR ? GHB_LONG : p.cols.c[c].type;
+      const unsigned char* cb = kind == A_CNT_STAR ? stage : stage + p.col_off[c];
+#pragma unroll
+      for (int j = 0; j < kGbRows; j++) {
+        if (j >= rpt) continue;
+        const int r = j * blockDim.x + threadIdx.x;
+        uint64_t w = 0;
+        if (live[j]) {
+          if (kind == A_CNT_STAR) {
+            w = 1;
+          } else {
+            int64_t v = type == GHB_INT ? (int64_t)((const int32_t*)cb)[r] : ((const long long*)cb)[r];
+            TileRow t{&p, stage, r};
+            if (!(NULLABLE && t.null(c, v))) {
+              switch (kind) {
+                case A_CNT_NN: w = 1; break;
+                case A_SUM_I: w = (uint64_t)v; break;
+                case A_SUM_F: w = (uint64_t)__double_as_longlong(raw_to_f64(type, v)); break;
+                case A_MAX_O: w = order_image(type, v); break;
+                default: w = ~order_image(type, v); break;  // A_MIN_O
+              }
+            }
+          }
+        }
+        if (p.warp_agg) {
+          // lanes of one shared slot combine first; the lowest applies it
+          wstage[threadIdx.x & 31] = in_s[j] ? w : 0;
+          __syncwarp();
+          if (in_s[j] && (threadIdx.x & 31) == __ffs(peers[j]) - 1) {
+            uint64_t tot = 0, comp = 0;
+            double sf = 0.0, cf = 0.0;
+            for (unsigned m = peers[j]; m; m &= m - 1) {
+              uint64_t x = wstage[__ffs(m) - 1];
+              if (kind == A_SUM_F) {
+                double xv = __longlong_as_double(x);
+                double tt = __dadd_rn(sf, xv);
+                cf = __dadd_rn(cf, two_sum_err(sf, xv, tt));
+                sf = tt;
+              } else if (kind == A_MAX_O || kind == A_MIN_O) {
+                tot = max(tot, x);
+              } else {
+                tot += x;
+              }
+            }
+            if (kind == A_SUM_F) {
+              tot = (uint64_t)__double_as_longlong(sf);
+              comp = (uint64_t)__double_as_longlong(cf);
+            }
+            acc_merge(kind, sacc + a * sstride + slot[j], sstride, tot, comp);
+          }
+          __syncwarp();
+          if (live[j] && !in_s[j]) acc_merge(kind, p.gacc + a * gstride + slot[j], gstride, w, 0);
+        } else if (live[j]) {
+          uint64_t* cell = in_s[j] ? sacc + a * sstride + slot[j] : p.gacc + a * gstride + slot[j];
+          acc_merge(kind, cell, in_s[j] ? sstride : gstride, w, 0);
+        }
       }
     }
     __syncthreads();  // every thread is done with this stage
@@ -787,7 +775,10 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   p.d_out_groups = d_out_groups;
 
   int blocks_per_sm = 0;
-  auto kfn = nkeys ? gb_fold_kernel<true> : gb_fold_kernel<false>;
+  bool nullable = false;
+  for (int c = 0; c < ncols; c++) nullable |= used[c] && cols[c].null_mode != GHB_NULLS_NONE;
+  auto kfn = nkeys ? (nullable ? gb_fold_kernel<true, true> : gb_fold_kernel<true, false>)
+                   : (nullable ? gb_fold_kernel<false, true> : gb_fold_kernel<false, false>);
   GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kfn, threads, smem));
   blocks_per_sm = std::max(1, blocks_per_sm);
