@@ -30,6 +30,11 @@ _PROTOS = {
     "ghb_join_probe": (I32, [P, P, P, I32, P, P, I32, P, P, P, I64, P, P]),
     "ghb_sort": (I32, [P, P, P, P, I32, P, I32, P, P, P, P, P]),
     "ghb_filter_groupby_noalloc": (I32, [P, P, I32, P, I32, P, I32, P, I64, P, P, P]),
+    "ghb_batch_groupby_create": (I32, [P, P, I32, I32, P, I32, P, I32, P, P, P,
+                                       C.POINTER(C.c_void_p)]),
+    "ghb_batch_launch": (I32, [P, P]),
+    "ghb_batch_describe": (I32, [P, C.c_char_p, I64]),
+    "ghb_batch_destroy": (I32, [P]),
     "ghb_filter_host": (I32, [P, P, P, I32, P, I32, P, I64, C.POINTER(I64)]),
     "ghb_filter_groupby_host": (I32, [P, P, P, I32, P, I32, P, I32, P, I64, C.POINTER(I64), P]),
     "ghb_hash_join_host": (I32, [P, P, P, I32, P, I32, P, P, I32, P, P, P, I64,

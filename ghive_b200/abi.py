@@ -86,6 +86,17 @@ class SortCfg(C.Structure):
                 ("items_per_thread", C.c_int32)]
 
 
+class GroupByInstance(C.Structure):
+    _fields_ = [("cols", C.c_void_p), ("pred", C.c_void_p), ("out", C.c_void_p),
+                ("out_capacity", C.c_int64), ("max_groups", C.c_int64)]
+
+
+class BatchCfg(C.Structure):
+    _fields_ = [("autotune", C.c_int32), ("block_threads", C.c_int32),
+                ("smem_slots", C.c_int32), ("load_factor", C.c_float),
+                ("use_graph", C.c_int32)]
+
+
 def agg_out_type(agg_type, in_type):
     """Result type of an aggregate, as Hive's UDAFs produce it."""
     if agg_type == CNT:

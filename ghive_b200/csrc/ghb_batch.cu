@@ -1,0 +1,700 @@
+// ghb_batch.cu — batched fused filter + group-by: many operator instances of
+// one signature in one persistent kernel and one finalize, captured once in
+// a CUDA graph and replayed.
+//
+// GHive runs GroupByPredicate::gpu_execute once per Tez task
+// (GroupByOperator::execute, gpu_impl/src/Operator/GroupByOperator.cu:
+// 101-130), so a vertex with hundreds of small splits pays a launch sequence,
+// a sort and per-aggregate copies for each.  Here the instances share:
+//
+//   fold      gb_batch_fold_kernel: persistent CTAs claim chunks (a run of
+//             tiles of one instance) from a list ordered by estimated cost,
+//             largest first; a CTA keeps its shared-memory table while its
+//             next chunk belongs to the same instance and flushes it into
+//             that instance's global table when the instance changes.  The
+//             per-tile work is fold_tile, the same code as the single call.
+//   finalize  gb_batch_finalize_kernel: warps walk the claimed-slot bitmaps
+//             of all instances at once; the last CTA publishes every
+//             instance's group count and resets the counters.
+//   autotune  candidate settings of the whole batch (CTA size, cap on the
+//             shared-table slots, whether instances with many more groups
+//             than the cap skip the shared table) are each planned and timed
+//             on the batch itself, and the fastest is kept: the shared
+//             reservation fixes every instance's tile size, and a setting
+//             timed on one instance alone (warm in L2) misjudges the batch.
+//   graph     the fold and finalize launches are captured once; a launch is
+//             one cudaGraphLaunch.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "ghb_groupby.cuh"
+
+namespace ghb {
+
+static_assert(sizeof(GbParams) % 8 == 0, "GbParams is copied to shared memory in 8-byte words");
+
+struct BatchChunk {
+  int32_t inst;
+  int32_t ntiles;
+  int64_t tile0;
+};
+
+struct BatchParams {
+  const GbParams* insts;
+  const BatchChunk* chunks;
+  int64_t nchunks;
+  unsigned long long* claim;   // next chunk to hand out (reset by the finalize)
+  int32_t stage_bytes;         // the same for every instance
+  int32_t table_words;         // shared-table words reserved per CTA
+};
+
+struct BatchFinParams {
+  const FinParams* fins;
+  const int64_t* choff;        // [ninst + 1]: first finalize chunk of each instance
+  int32_t ninst;
+  unsigned long long* done;
+  unsigned long long* claim;
+};
+
+template <bool KEYED, bool NULLABLE>
+__global__ void __launch_bounds__(kGbThreads) gb_batch_fold_kernel(BatchParams bp) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // layout: [stage 0][stage 1][mbarriers][instance params][claim][table][warp staging]
+  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)bp.stage_bytes);
+  GbParams* sp = (GbParams*)(bars + 2);
+  long long* sclaim = (long long*)(sp + 1);
+  uint64_t* skeys = (uint64_t*)(sclaim + 2);
+  uint64_t* wstage = skeys + bp.table_words + (threadIdx.x >> 5) * 32;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // The CTA's tile stream: the tiles of the chunk it claimed last.  Every
+  // thread holds the same state, so the barriers inside are uniform.
+  int32_t c_inst = -1;
+  int64_t c_next = 0, c_end = 0;
+  bool exhausted = false;
+  auto next_tile = [&](int32_t* inst, int64_t* tile) -> bool {
+    if (c_next >= c_end) {
+      if (exhausted) return false;
+      if (threadIdx.x == 0) *sclaim = (long long)atomicAdd(bp.claim, 1ull);
+      __syncthreads();
+      const long long c = *sclaim;
+      __syncthreads();
+      if (c >= bp.nchunks) {
+        exhausted = true;
+        return false;
+      }
+      const BatchChunk ch = bp.chunks[c];
+      c_inst = ch.inst;
+      c_next = ch.tile0;
+      c_end = ch.tile0 + ch.ntiles;
+    }
+    *inst = c_inst;
+    *tile = c_next++;
+    return true;
+  };
+  // Starts loading a tile into stage s; true when it arrives by bulk copy.
+  auto issue = [&](int s, int32_t inst, int64_t tile) -> bool {
+    const GbParams& gp = bp.insts[inst];
+    unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
+    if (gp.bulk && (tile + 1) * gp.tile_rows <= gp.n) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        load_tile_bulk(gp, stage, tile, &bars[s]);
+      }
+      return true;
+    }
+    load_tile_plain(gp, stage, tile);
+    return false;
+  };
+
+  int32_t q_inst[2] = {-1, -1};
+  int64_t q_tile[2] = {0, 0};
+  uint32_t valid = 0, pending = 0, phase = 0;
+  for (int s = 0; s < 2; s++) {
+    if (!next_tile(&q_inst[s], &q_tile[s])) break;
+    valid |= 1u << s;
+    if (issue(s, q_inst[s], q_tile[s])) pending |= 1u << s;
+  }
+
+  int32_t active = -1;
+  bool failed = false;
+  for (int64_t it = 0;; it++) {
+    const int s = (int)(it & 1);
+    if (!((valid >> s) & 1u)) break;
+    const int32_t inst = s ? q_inst[1] : q_inst[0];
+    const int64_t tile = s ? q_tile[1] : q_tile[0];
+    if (inst != active) {
+      if (active >= 0) {
+        flush_smem_table(*sp, skeys);
+        __syncthreads();
+      }
+      const uint64_t* src = (const uint64_t*)&bp.insts[inst];
+      for (int k = threadIdx.x; k < (int)(sizeof(GbParams) / 8); k += blockDim.x)
+        ((uint64_t*)sp)[k] = src[k];
+      __syncthreads();
+      smem_table_clear(*sp, skeys);
+      __syncthreads();
+      active = inst;
+    }
+    if ((pending >> s) & 1u) {
+      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      phase ^= 1u << s;
+      pending &= ~(1u << s);
+    }
+    const unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
+    const int rows = (int)min((int64_t)sp->tile_rows, sp->n - tile * sp->tile_rows);
+    fold_tile<KEYED, NULLABLE>(*sp, stage, rows, skeys, wstage);
+    __syncthreads();  // every thread is done with this stage
+    valid &= ~(1u << s);
+    int32_t ni;
+    int64_t nt;
+    if (next_tile(&ni, &nt)) {
+      if (s) {
+        q_inst[1] = ni;
+        q_tile[1] = nt;
+      } else {
+        q_inst[0] = ni;
+        q_tile[0] = nt;
+      }
+      valid |= 1u << s;
+      if (issue(s, ni, nt)) pending |= 1u << s;
+    }
+  }
+  if (failed) {
+    for (int s = 0; s < 2; s++)
+      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
+    return;
+  }
+  __syncthreads();
+  if (active >= 0) flush_smem_table(*sp, skeys);
+}
+
+__global__ void gb_batch_finalize_kernel(BatchFinParams b) {
+  const int64_t total = b.choff[b.ninst];
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t ch = gw; ch < total; ch += nw) {
+    // the instance of chunk ch: the last i with choff[i] <= ch
+    int lo = 0, hi = b.ninst - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (b.choff[mid] <= ch) lo = mid;
+      else hi = mid - 1;
+    }
+    const FinParams& f = b.fins[lo];
+    const int64_t local = ch - b.choff[lo];
+    finalize_chunk(f, local);
+    if (local == 0 && (threadIdx.x & 31) == 0) finalize_sides(f);
+  }
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(b.done, 1ull) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    for (int i = threadIdx.x; i < b.ninst; i += blockDim.x)
+      *b.fins[i].d_out_groups = (int64_t)atomicExch(b.fins[i].growc, 0ull);
+    if (threadIdx.x == 0) {
+      *b.done = 0;
+      *b.claim = 0;
+    }
+  }
+}
+
+using FoldFn = void (*)(BatchParams);
+
+static FoldFn fold_fn(bool keyed, bool nullable) {
+  return keyed ? (nullable ? gb_batch_fold_kernel<true, true> : gb_batch_fold_kernel<true, false>)
+               : (nullable ? gb_batch_fold_kernel<false, true> : gb_batch_fold_kernel<false, false>);
+}
+
+// Device image of a batch: params, chunk list, finalize offsets, counters and
+// the global tables, in one allocation.
+struct BatchImage {
+  void* dev = nullptr;
+  size_t bytes = 0;
+  BatchParams bp{};
+  BatchFinParams bf{};
+  FoldFn fold = nullptr;
+  int threads = kGbThreads;
+  int grid = 1;
+  int fgrid = 1;
+  size_t smem = 0;
+};
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Lays out and uploads a batch.  `tables` (nullable) is where the global
+// tables go; otherwise they are placed in the image itself.  `chunk_tiles[i]`
+// is the chunk length of instance i; `order` the order of instances in the
+// chunk list.
+static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<FinParams>& fs,
+                           const std::vector<int64_t>& chunk_tiles, const std::vector<int32_t>& order,
+                           bool keyed, bool nullable, int threads, size_t smem_fold, int table_words,
+                           cudaStream_t stream, BatchImage* im) {
+  const int ninst = (int)ps.size();
+  std::vector<BatchChunk> chunks;
+  for (int32_t i : order) {
+    const int64_t nt = ps[i].ntiles;
+    const int64_t step = std::max<int64_t>(1, chunk_tiles[i]);
+    for (int64_t t = 0; t < nt; t += step)
+      chunks.push_back(BatchChunk{i, (int32_t)std::min<int64_t>(step, nt - t), t});
+  }
+  std::vector<int64_t> choff(ninst + 1, 0);
+  for (int i = 0; i < ninst; i++) choff[i + 1] = choff[i] + fin_chunks(ps[i].C);
+
+  size_t off = 0;
+  const size_t o_ps = off;
+  off = align256(off + sizeof(GbParams) * ninst);
+  const size_t o_fs = off;
+  off = align256(off + sizeof(FinParams) * ninst);
+  const size_t o_ch = off;
+  off = align256(off + sizeof(BatchChunk) * std::max<size_t>(1, chunks.size()));
+  const size_t o_co = off;
+  off = align256(off + sizeof(int64_t) * (ninst + 1));
+  const size_t o_ctr = off;
+  off = align256(off + 16);
+  std::vector<size_t> o_tab(ninst);
+  for (int i = 0; i < ninst; i++) {
+    o_tab[i] = off;
+    off = align256(off + gb_table_bytes(ps[i].C, ps[i].R));
+  }
+  if (cudaMalloc(&im->dev, off) != cudaSuccess) {
+    cudaGetLastError();
+    im->dev = nullptr;
+    return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes for the batch", off);
+  }
+  im->bytes = off;
+  char* base = (char*)im->dev;
+  for (int i = 0; i < ninst; i++) {
+    gb_table_bind(base + o_tab[i], ps[i].C, ps[i].R, &ps[i], &fs[i]);
+    fs[i].done = nullptr;  // the batched finalize counts CTAs with one counter
+  }
+  // tables and counters start zeroed; the finalize leaves them zeroed
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(base + o_ctr, 0, off - o_ctr, stream));
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_ps, ps.data(), sizeof(GbParams) * ninst, cudaMemcpyHostToDevice, stream));
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_fs, fs.data(), sizeof(FinParams) * ninst, cudaMemcpyHostToDevice, stream));
+  if (!chunks.empty())
+    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_ch, chunks.data(), sizeof(BatchChunk) * chunks.size(),
+                                      cudaMemcpyHostToDevice, stream));
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_co, choff.data(), sizeof(int64_t) * (ninst + 1), cudaMemcpyHostToDevice, stream));
+  // the host vectors go out of scope: the copies must have read them
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+
+  unsigned long long* ctr = (unsigned long long*)(base + o_ctr);
+  im->bp.insts = (const GbParams*)(base + o_ps);
+  im->bp.chunks = (const BatchChunk*)(base + o_ch);
+  im->bp.nchunks = (int64_t)chunks.size();
+  im->bp.claim = ctr;
+  im->bp.stage_bytes = ps.empty() ? 0 : ps[0].stage_bytes;
+  im->bp.table_words = table_words;
+  im->bf.fins = (const FinParams*)(base + o_fs);
+  im->bf.choff = (const int64_t*)(base + o_co);
+  im->bf.ninst = ninst;
+  im->bf.done = ctr + 1;
+  im->bf.claim = ctr;
+  im->fold = fold_fn(keyed, nullable);
+  im->threads = threads;
+  im->smem = smem_fold;
+  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(im->fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fold));
+  int per_sm = 0;
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, im->fold, threads, smem_fold));
+  per_sm = std::max(1, per_sm);
+  im->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * per_sm,
+                                                          std::max<int64_t>(1, (int64_t)chunks.size())));
+  im->fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((choff[ninst] * 32 + 255) / 256, (int64_t)ctx->num_sms * 4));
+  return GHB_OK;
+}
+
+static int32_t image_launch(ghb_ctx* ctx, const BatchImage& im, cudaStream_t stream) {
+  if (im.bp.nchunks > 0) {
+    im.fold<<<im.grid, im.threads, im.smem, stream>>>(im.bp);
+    GHB_LAUNCH_CHECK(ctx);
+  }
+  gb_batch_finalize_kernel<<<im.fgrid, 256, 0, stream>>>(im.bf);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+static void image_free(BatchImage* im) {
+  if (im->dev) cudaFree(im->dev);
+  im->dev = nullptr;
+}
+
+// ------------------------------------------------------------ autotuner
+// A setting of the whole batch.  Shared memory is reserved per CTA for the
+// largest shared table any instance uses, and that reservation fixes the
+// tile size of every instance, so the settings are chosen for the batch as a
+// whole and timed on the batch itself (its real sizes, its real L2 traffic).
+struct BatchSetting {
+  int32_t threads;      // CTA size: 512 or 1024
+  int32_t smem_cap;     // shared-table slots at most; 0 = none (a global aggregate keeps 64)
+  int32_t skip_large;   // 1: instances with more than 16 * smem_cap groups skip the shared table
+  float load_factor;    // global tables
+};
+
+static const char* kRowClass[] = {"<1e4", "1e4-1e5", "1e5-1e6", ">=1e6"};
+static const char* kGroupClass[] = {"<=64", "65-2048", "2049-32768", ">32768"};
+
+static int row_class(int64_t n) { return n < 10000 ? 0 : n < 100000 ? 1 : n < 1000000 ? 2 : 3; }
+static int group_class(int64_t g) { return g <= 64 ? 0 : g <= 2048 ? 1 : g <= 32768 ? 2 : 3; }
+
+}  // namespace ghb
+
+struct ghb_batch {
+  ghb_ctx* ctx = nullptr;
+  ghb::BatchImage im;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string report;
+};
+
+namespace ghb {
+
+struct InstSpec {
+  const ghb_groupby_instance* in;
+  int64_t rows;
+  int64_t groups;
+  int cls;
+};
+
+// Shared-table slots of one instance under a setting (-1: none).
+static int32_t inst_slots(const InstSpec& s, int32_t nkeys, const BatchSetting& bs) {
+  if (nkeys == 0) return 64;
+  if (bs.smem_cap <= 0) return -1;
+  if (bs.skip_large && s.groups > 16 * (int64_t)bs.smem_cap) return -1;
+  return (int32_t)std::min<int64_t>(bs.smem_cap, std::max<int64_t>(64, next_pow2_i64(2 * s.groups)));
+}
+
+static int32_t setup_inst(ghb_ctx* ctx, const InstSpec& s, int32_t ncols, const int32_t* key_cols,
+                          int32_t nkeys, const ghb_agg_desc* aggs, int32_t naggs, int64_t* d_count,
+                          const BatchSetting& bs, int tile_rows, int reserve, GbParams* p,
+                          FinParams* f, size_t* tb, size_t* smem) {
+  GbSetup su{};
+  su.max_groups = s.groups;
+  su.smem_slots = inst_slots(s, nkeys, bs);
+  su.load_factor = bs.load_factor;
+  su.threads = bs.threads;
+  su.tile_rows = tile_rows;
+  su.smem_table_slots = reserve;
+  su.warp_agg = -1;
+  su.extra_smem = (int32_t)(sizeof(GbParams) + 16);
+  return gb_setup(ctx, s.in->pred, s.in->cols, ncols, key_cols, nkeys, aggs, naggs, s.in->out,
+                  s.in->out_capacity, d_count, su, p, f, tb, smem);
+}
+
+static size_t batch_smem(size_t fold_smem) { return fold_smem + sizeof(GbParams) + 16; }
+
+struct BatchSig {
+  int32_t ncols;
+  const int32_t* key_cols;
+  int32_t nkeys;
+  const ghb_agg_desc* aggs;
+  int32_t naggs;
+  int64_t* d_out_groups;
+  bool nullable;
+};
+
+// Sets every instance up under `bs` (one stage layout and shared reservation
+// for all), orders and chunks the work and builds the device image.
+static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const BatchSig& sig,
+                          const BatchSetting& bs, cudaStream_t stream, BatchImage* im,
+                          std::vector<GbParams>* ps_out) {
+  const int ninst = (int)spec.size();
+  std::vector<GbParams> ps(ninst);
+  std::vector<FinParams> fs(ninst);
+  int reserve = 0;
+  for (int i = 0; i < ninst; i++) {
+    size_t tb = 0, smem = 0;
+    int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
+                            sig.d_out_groups + i, bs, 0, 0, &ps[i], &fs[i], &tb, &smem);
+    if (st) return st;
+    reserve = std::max(reserve, ps[i].smem_slots);
+  }
+  int tile_rows = 2 * bs.threads;
+  size_t smem_fold = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    bool ok = true;
+    smem_fold = 0;
+    for (int i = 0; i < ninst && ok; i++) {
+      size_t tb = 0, smem = 0;
+      int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
+                              sig.d_out_groups + i, bs, tile_rows, reserve, &ps[i], &fs[i], &tb, &smem);
+      if (st) {
+        if (attempt == 1) return st;
+        ok = false;
+        ctx->last_error.clear();
+      }
+      smem_fold = std::max(smem_fold, smem);
+    }
+    if (ok) break;
+    tile_rows = bs.threads;
+  }
+  for (int i = 1; i < ninst; i++) {
+    bool same = ps[i].stage_bytes == ps[0].stage_bytes && ps[i].tile_rows == ps[0].tile_rows &&
+                ps[i].acc.n_acc == ps[0].acc.n_acc && ps[i].key_col == ps[0].key_col;
+    for (int c = 0; c < kMaxCols; c++) same = same && ps[i].col_off[c] == ps[0].col_off[c];
+    if (!same)
+      return set_error(ctx, GHB_ERR_INVALID,
+                       "instance %d: predicate or aggregates read other columns than instance 0", i);
+  }
+  const int table_words = (reserve + 2) * (1 + ps[0].acc.n_acc);
+
+  // chunk list: instances by size, largest first, each cut into chunks so
+  // that every CTA claims several; a fixed cost per instance stands for its
+  // table flush and finalize
+  std::vector<double> cost(ninst);
+  double total = 0;
+  for (int i = 0; i < ninst; i++) {
+    cost[i] = (double)spec[i].rows + 4096.0;
+    total += cost[i];
+  }
+  std::vector<int32_t> order(ninst);
+  for (int i = 0; i < ninst; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+  int per_sm = 1;
+  FoldFn fn = fold_fn(sig.nkeys == 1, sig.nullable);
+  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem(smem_fold)));
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs.threads, batch_smem(smem_fold)));
+  per_sm = std::max(1, per_sm);
+  const double target = total / ((double)ctx->num_sms * per_sm * 6.0);
+  std::vector<int64_t> chunk_tiles(ninst);
+  for (int i = 0; i < ninst; i++) {
+    const double per_tile = cost[i] / (double)std::max<int64_t>(1, ps[i].ntiles);
+    chunk_tiles[i] = std::max<int64_t>(1, (int64_t)(target / std::max(per_tile, 1e-9)));
+  }
+  int32_t st = image_build(ctx, ps, fs, chunk_tiles, order, sig.nkeys == 1, sig.nullable, bs.threads,
+                           batch_smem(smem_fold), table_words, stream, im);
+  if (st) return st;
+  if (ps_out) *ps_out = ps;
+  return GHB_OK;
+}
+
+// Median-free timing: the best of `reps` launches after one warm-up, in ms.
+static double time_image(ghb_ctx* ctx, const BatchImage& im, cudaStream_t stream, int reps) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 1e300;
+  int32_t st = GHB_OK;
+  for (int rep = 0; rep <= reps && st == GHB_OK; rep++) {
+    cudaEventRecord(a, stream);
+    st = image_launch(ctx, im, stream);
+    cudaEventRecord(b, stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0) best = std::min(best, (double)ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return st == GHB_OK ? best : -1.0;
+}
+
+static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int32_t ninst, int32_t ncols,
+                            const int32_t* key_cols, int32_t nkeys, const ghb_agg_desc* aggs,
+                            int32_t naggs, int64_t* d_out_groups, const ghb_batch_cfg* cfg,
+                            cudaStream_t stream, ghb_batch* b) {
+  if (ninst < 1) return set_error(ctx, GHB_ERR_INVALID, "ninst=%d: a batch needs an instance", ninst);
+  if (!inst) return set_error(ctx, GHB_ERR_INVALID, "instances is NULL");
+  if (!d_out_groups) return set_error(ctx, GHB_ERR_INVALID, "d_out_groups is NULL");
+  if (ncols < 1 || ncols > kMaxCols)
+    return set_error(ctx, GHB_ERR_INVALID, "ncols=%d outside [1,%d]", ncols, kMaxCols);
+  std::vector<InstSpec> spec(ninst);
+  for (int i = 0; i < ninst; i++) {
+    if (!inst[i].cols) return set_error(ctx, GHB_ERR_INVALID, "instance %d: cols is NULL", i);
+    int64_t n = 0;
+    int32_t st = validate_columns(ctx, inst[i].cols, ncols, &n);
+    if (st) return st;
+    int64_t g = inst[i].max_groups > 0 ? inst[i].max_groups : inst[i].out_capacity;
+    if (nkeys == 0) g = 1;
+    g = std::max<int64_t>(1, std::min<int64_t>(g, std::max<int64_t>(n, 1)));
+    spec[i] = InstSpec{&inst[i], n, g, row_class(n) * 4 + group_class(g)};
+  }
+  // one signature: column types and NULL modes as in instance 0
+  bool nullable = false;
+  for (int i = 0; i < ninst; i++)
+    for (int c = 0; c < ncols; c++) {
+      if (inst[i].cols[c].type != inst[0].cols[c].type)
+        return set_error(ctx, GHB_ERR_INVALID, "instance %d: column %d has type %d, instance 0 has %d", i,
+                         c, inst[i].cols[c].type, inst[0].cols[c].type);
+      nullable |= inst[i].cols[c].null_mode != GHB_NULLS_NONE;
+    }
+
+  const BatchSig sig{ncols, key_cols, nkeys, aggs, naggs, d_out_groups, nullable};
+  const bool tune = cfg && cfg->autotune;
+  const int forced_threads =
+      (cfg && (cfg->block_threads == 512 || cfg->block_threads == 1024)) ? cfg->block_threads : 0;
+  const float lf = (cfg && cfg->load_factor > 0.f) ? cfg->load_factor : 0.5f;
+  BatchSetting base{forced_threads ? forced_threads : kGbThreads, 512, 0, lf};
+  if (cfg && cfg->smem_slots < 0) base.smem_cap = 0;
+  if (cfg && cfg->smem_slots > 0) base.smem_cap = (int32_t)next_pow2_i64(cfg->smem_slots);
+  std::vector<BatchSetting> cands{base};
+  if (tune) {
+    cands.clear();
+    for (int th : {1024, 512}) {
+      if (forced_threads && th != forced_threads) continue;
+      std::vector<int> caps{0, 256, 512, 1024, 2048};
+      if (cfg && cfg->smem_slots) caps = {base.smem_cap};
+      for (int cap : caps)
+        for (int skip = 0; skip < (cap > 0 && nkeys == 1 ? 2 : 1); skip++) cands.push_back({th, cap, skip, lf});
+    }
+  }
+  std::string trials = "[";
+  double best_ms = 1e300;
+  BatchSetting best = cands[0];
+  if (cands.size() > 1) {
+    for (const BatchSetting& c : cands) {
+      BatchImage im;
+      int32_t st = plan_image(ctx, spec, sig, c, stream, &im, nullptr);
+      double ms = st ? -1.0 : time_image(ctx, im, stream, 2);
+      cudaStreamSynchronize(stream);
+      image_free(&im);
+      if (st) ctx->last_error.clear();
+      char tb[160];
+      snprintf(tb, sizeof(tb), "%s{\"threads\": %d, \"smem_cap\": %d, \"skip_large\": %d, \"ms\": %.4f}",
+               trials.size() > 1 ? ", " : "", c.threads, c.smem_cap, c.skip_large, ms);
+      trials += tb;
+      if (ms > 0 && ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    // a tuning launch may have raised a device status (a short output): clear it
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t), stream);
+  }
+  trials += "]";
+  std::vector<GbParams> ps;
+  int32_t st = plan_image(ctx, spec, sig, best, stream, &b->im, &ps);
+  if (st) return st;
+
+  // report: the setting, the trials and the shared slots per size class
+  char buf[512];
+  std::string rep_s = "{\"block_threads\": " + std::to_string(best.threads) +
+                      ", \"smem_cap\": " + std::to_string(best.smem_cap) +
+                      ", \"skip_large\": " + std::to_string(best.skip_large) +
+                      ", \"tile_rows\": " + std::to_string(ps[0].tile_rows) +
+                      ", \"grid\": " + std::to_string(b->im.grid) +
+                      ", \"chunks\": " + std::to_string(b->im.bp.nchunks) +
+                      ", \"smem_bytes\": " + std::to_string(b->im.smem) +
+                      ", \"autotuned\": " + (tune ? "true" : "false") + ", \"trials\": " + trials +
+                      ", \"classes\": [";
+  bool first = true;
+  for (int k = 0; k < 16; k++) {
+    int cnt = 0, slots = 0;
+    double rows = 0;
+    for (int i = 0; i < ninst; i++)
+      if (spec[i].cls == k) {
+        cnt++;
+        rows += (double)spec[i].rows;
+        slots = std::max(slots, ps[i].smem_slots);
+      }
+    if (!cnt) continue;
+    snprintf(buf, sizeof(buf),
+             "%s{\"rows\": \"%s\", \"groups\": \"%s\", \"instances\": %d, \"total_rows\": %.0f, "
+             "\"smem_slots\": %d}",
+             first ? "" : ", ", kRowClass[k / 4], kGroupClass[k % 4], cnt, rows, slots);
+    rep_s += buf;
+    first = false;
+  }
+  rep_s += "]}";
+  b->report = rep_s;
+
+  // capture the launches once
+  const bool graph = !cfg || cfg->use_graph != 0;
+  if (graph) {
+    GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+    GHB_CUDA_TRY(ctx, cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = ctx->launches;
+    int32_t lst = image_launch(ctx, b->im, b->cap_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    ctx->launches = before;  // captured, not launched
+    if (lst) {
+      if (g) cudaGraphDestroy(g);
+      return lst;
+    }
+    if (e != cudaSuccess) return set_error(ctx, GHB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) return set_error(ctx, GHB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+  }
+  return GHB_OK;
+}
+
+static void batch_release(ghb_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  image_free(&b->im);
+}
+
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" int32_t ghb_batch_groupby_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int32_t ninst,
+                                            int32_t ncols, const int32_t* key_cols, int32_t nkeys,
+                                            const ghb_agg_desc* aggs, int32_t naggs, int64_t* d_out_groups,
+                                            const ghb_batch_cfg* cfg, void* stream, ghb_batch** out) {
+  if (!ctx || !out) return GHB_ERR_INVALID;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  ghb_batch* b = new ghb_batch();
+  b->ctx = ctx;
+  int32_t st = batch_create(ctx, inst, ninst, ncols, key_cols, nkeys, aggs, naggs, d_out_groups, cfg,
+                            (cudaStream_t)stream, b);
+  if (st) {
+    cudaStreamSynchronize((cudaStream_t)stream);
+    batch_release(b);
+    delete b;
+    return st;
+  }
+  *out = b;
+  return GHB_OK;
+}
+
+extern "C" int32_t ghb_batch_launch(ghb_batch* b, void* stream) {
+  if (!b) return GHB_ERR_INVALID;
+  ghb_ctx* ctx = b->ctx;
+  if (b->exec) {
+    cudaError_t e = cudaGraphLaunch(b->exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_error(ctx, GHB_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(e));
+    ctx->launches += b->im.bp.nchunks > 0 ? 2 : 1;
+    return GHB_OK;
+  }
+  return image_launch(ctx, b->im, (cudaStream_t)stream);
+}
+
+extern "C" int32_t ghb_batch_describe(const ghb_batch* b, char* buf, int64_t len) {
+  if (!b || !buf || len < 1) return GHB_ERR_INVALID;
+  const size_t n = std::min<size_t>((size_t)len - 1, b->report.size());
+  std::memcpy(buf, b->report.data(), n);
+  buf[n] = 0;
+  return b->report.size() < (size_t)len ? GHB_OK : GHB_ERR_CAPACITY;
+}
+
+extern "C" int32_t ghb_batch_destroy(ghb_batch* b) {
+  if (!b) return GHB_OK;
+  cudaSetDevice(b->ctx->device);
+  batch_release(b);
+  delete b;
+  return GHB_OK;
+}

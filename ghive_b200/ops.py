@@ -155,6 +155,42 @@ class JoinTable:
             pass
 
 
+class GroupByBatch:
+    """A captured batch of filter + group-by instances (ghb_batch).
+
+    outs[i] holds instance i's output columns and groups[i] its group count
+    after launch() and a sync; results(i) slices them."""
+
+    def __init__(self, ctx, handle, outs, groups, nkeys, keep):
+        self.ctx, self.handle, self.outs, self.groups = ctx, handle, outs, groups
+        self.nkeys, self._keep = nkeys, keep
+
+    def launch(self, stream=None):
+        self.ctx._check(lib().ghb_batch_launch(self.handle, _stream(stream)))
+
+    def describe(self):
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        self.ctx._check(lib().ghb_batch_describe(self.handle, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def results(self, i, counts=None):
+        g = int(self.groups[i]) if counts is None else int(counts[i])
+        res = self.outs[i].rows(min(g, len(self.outs[i].cols[0][0])))
+        return res[:self.nkeys], res[self.nkeys:], g
+
+    def free(self):
+        if self.handle:
+            lib().ghb_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Context:
     """One ghb_ctx: device scratch, error state and kernel-launch counter."""
 
@@ -238,6 +274,44 @@ class Context:
         g = int(d_groups.item())
         res = outs.rows(min(g, cap))
         return res[:len(keys)], res[len(keys):], g
+
+    def batch_groupby(self, instances, keys, aggs, autotune=True, block_threads=0, smem_slots=0,
+                      load_factor=0.0, use_graph=True, stream=None):
+        """Many filter + group-by instances of one signature in one captured launch.
+
+        instances: [(pred, cols, capacity, max_groups)], cols device columns of
+        the same types in every instance.  Returns a GroupByBatch; call
+        launch() (and sync) to run it, as often as wanted."""
+        nin = len(instances)
+        arr = (abi.GroupByInstance * max(1, nin))()
+        keep, outs = [], []
+        ncols = None
+        for i, (pred, cols, cap, mg) in enumerate(instances):
+            cs = _Cols(cols)
+            ncols = cs.n if ncols is None else ncols
+            if cs.n != ncols:
+                raise ValueError("instance %d has %d columns, instance 0 has %d" % (i, cs.n, ncols))
+            types = [cs[k].type for k in keys]
+            types += [abi.agg_out_type(t, cs[c].type if c >= 0 else abi.LONG) for t, c in aggs]
+            o = _Outs(types, cap, self.torch_device)
+            pp, pk = _pred(pred)
+            arr[i].cols, arr[i].pred, arr[i].out = cs.ptr, pp, o.ptr
+            arr[i].out_capacity, arr[i].max_groups = cap, mg or 0
+            keep += [cs, pk, o]
+            outs.append(o)
+        ka = (C.c_int32 * max(1, len(keys)))(*keys)
+        ag = (abi.AggDesc * max(1, len(aggs)))()
+        for i, (t, c) in enumerate(aggs):
+            ag[i].type, ag[i].col = t, c
+        cfg = abi.BatchCfg()
+        cfg.autotune, cfg.block_threads, cfg.smem_slots = int(autotune), block_threads, smem_slots
+        cfg.load_factor, cfg.use_graph = load_factor, int(use_graph)
+        groups = torch.zeros(max(1, nin), dtype=torch.int64, device=self.torch_device)
+        h = C.c_void_p()
+        self._check(lib().ghb_batch_groupby_create(self.h, arr, nin, ncols or 0, ka, len(keys), ag,
+                                                   len(aggs), groups.data_ptr(), C.byref(cfg),
+                                                   _stream(stream), C.byref(h)))
+        return GroupByBatch(self, h.value, outs, groups, len(keys), keep + [arr, ka, ag])
 
     def join_build(self, key, build_payload=(), load_factor=0.0, l2_persist=False, stream=None):
         """Builds the device hash table; it keeps the build payload columns

@@ -74,23 +74,93 @@ def sort_table(n=60_000_000, zipf=False, seed_idx=2, days=2526):
     return d, k, rowid
 
 
-def batched_instances(count=512, seed_idx=3, min_rows=1_000, max_rows=10_000_000,
-                      scale=1.0):
-    """Independent filter + group-by instances: rows log-U[min_rows,max_rows]
-    (times scale), groups log-U[10,10^6], int64 keys Zipf(theta U[0,1.2]) over
-    the groups, qty/price as the fact table, d int32 U[0,2526) with predicate
-    d < round(s*2526), s U[0.01,0.9].  Yields dicts per instance."""
+_MIX1, _MIX2 = 0xBF58476D1CE4E5B9, 0x94D049BB133111EB
+
+
+def mix64_np(x):
+    """splitmix64's finalizer, a bijection on 64-bit words: spreads group
+    ranks over the int64 range so keys are not small consecutive integers."""
+    x = np.asarray(x).astype(np.uint64)
+    x ^= x >> np.uint64(30)
+    x *= np.uint64(_MIX1)
+    x ^= x >> np.uint64(27)
+    x *= np.uint64(_MIX2)
+    x ^= x >> np.uint64(31)
+    return x.view(np.int64)
+
+
+def mix64_torch(x):
+    """mix64_np on an int64 tensor (wrapping multiplies, logical shifts)."""
+    def srl(v, k):
+        return (v >> k) & ((1 << (64 - k)) - 1)
+
+    def signed(c):
+        return c - (1 << 64) if c >= 1 << 63 else c
+
+    x = x ^ srl(x, 30)
+    x = x * signed(_MIX1)
+    x = x ^ srl(x, 27)
+    x = x * signed(_MIX2)
+    return x ^ srl(x, 31)
+
+
+def batched_specs(count=512, seed_idx=3, min_rows=1_000, max_rows=10_000_000, scale=1.0):
+    """Per instance: rows log-U[min_rows,max_rows] (times scale), groups
+    log-U[10,10^6], Zipf theta U[0,1.2], selectivity s U[0.01,0.9] and the
+    predicate cut d < round(s*2526)."""
     g = rng(seed_idx)
-    for i in range(count):
-        rows = int(np.exp(g.uniform(np.log(min_rows), np.log(max_rows))) * scale)
-        rows = max(rows, 1)
+    out = []
+    for _ in range(count):
+        rows = max(int(np.exp(g.uniform(np.log(min_rows), np.log(max_rows))) * scale), 1)
         groups = int(np.exp(g.uniform(np.log(10), np.log(1_000_000))))
         theta = g.uniform(0.0, 1.2)
         sel = g.uniform(0.01, 0.9)
+        out.append({"rows": rows, "groups": groups, "theta": theta, "cut": int(round(sel * 2526))})
+    return out
+
+
+def batched_instances(count=512, seed_idx=3, min_rows=1_000, max_rows=10_000_000,
+                      scale=1.0):
+    """Independent filter + group-by instances (host columns): int64 keys
+    Zipf(theta) over the instance's groups, qty/price as the fact table, d
+    int32 U[0,2526) filtered by d < cut.  Yields the spec dicts with "cols"."""
+    for i, s in enumerate(batched_specs(count, seed_idx, min_rows, max_rows, scale)):
         ig = rng(seed_idx, 10 + i)
-        keys = zipf_ranks(ig, rows, groups, theta)
+        rows = s["rows"]
+        keys = mix64_np(zipf_ranks(ig, rows, s["groups"], s["theta"]))
         qty = ig.integers(1, 51, rows, dtype=np.int64)
         price = ig.integers(90000, 10500001, rows, dtype=np.int64) / 100.0
         d = ig.integers(0, 2526, rows, dtype=np.int32)
-        yield {"rows": rows, "groups": groups, "theta": theta, "cut": int(round(sel * 2526)),
-               "cols": [keys, qty, price, d]}
+        yield dict(s, cols=[keys, qty, price, d])
+
+
+def batched_instances_device(specs, device, seed_idx=3):
+    """The same instances generated on the device with torch's generator
+    (same distributions, a different random stream): for batches too large
+    to build on the host."""
+    import torch
+    out = []
+    for i, s in enumerate(specs):
+        gen = torch.Generator(device=device)
+        gen.manual_seed(SEED + seed_idx * 1000 + i)
+        rows, G, theta = s["rows"], s["groups"], s["theta"]
+        if theta <= 0.0:
+            ranks = torch.randint(0, G, (rows,), generator=gen, device=device, dtype=torch.int64)
+        else:
+            w = torch.arange(1, G + 1, device=device, dtype=torch.float64).pow(-theta)
+            cdf = torch.cumsum(w, 0)
+            cdf /= cdf[-1].clone()
+            u = torch.rand(rows, generator=gen, device=device, dtype=torch.float64)
+            ranks = torch.clamp(torch.searchsorted(cdf, u, right=True), max=G - 1)
+        keys = mix64_torch(ranks)
+        qty = torch.randint(1, 51, (rows,), generator=gen, device=device, dtype=torch.int64)
+        price = torch.randint(90000, 10500001, (rows,), generator=gen, device=device,
+                              dtype=torch.int64).to(torch.float64) / 100.0
+        d = torch.randint(0, 2526, (rows,), generator=gen, device=device, dtype=torch.int32)
+        out.append(dict(s, cols=[keys, qty, price, d]))
+    return out
+
+
+def batched_predicate(cut):
+    """d < cut on column 3 of a batched instance."""
+    return abi.Pred.leaf(abi.FILTER_LT, 3, a=cut)

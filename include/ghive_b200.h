@@ -296,11 +296,11 @@ int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
  * device status word live in a file-scope __device__ array of
  * GHB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * exit; nothing is allocated or freed.  The table needs
- * (2 + next_pow2(max(2 * max_groups, 64))) * 8 * (1 + accumulator words)
- * bytes (one accumulator word per COUNT/SUM/MIN/MAX state, two per double
- * SUM/AVG, plus COUNT(*)); a call that would need more than the array holds
- * returns GHB_ERR_CAPACITY before launching.  About 30,000 groups fit with
- * the fact-table aggregates.
+ * (C + 2) * 8 * (1 + accumulator words) + 16 + C / 8 bytes, with
+ * C = next_pow2(max(2 * max_groups + 1, 64)) (one accumulator word per
+ * COUNT/SUM/MIN/MAX state, two per double SUM/AVG, plus COUNT(*)); a call
+ * that would need more than the array holds returns GHB_ERR_CAPACITY before
+ * launching.  About 60,000 groups fit with the fact-table aggregates.
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture.  Each call clears the part of the
  * array it uses, runs on `stream`, waits for it and returns the device
@@ -315,6 +315,53 @@ int32_t ghb_filter_groupby_noalloc(const ghb_predicate* pred,
                                    ghb_out_column* out, int64_t out_capacity,
                                    int64_t* d_out_groups,
                                    const ghb_groupby_cfg* cfg, void* stream);
+
+/* ---- batched filter + group-by -------------------------------------------
+ * GHive runs one GroupByPredicate::gpu_execute per Tez task
+ * (GroupByOperator::execute, gpu_impl/src/Operator/GroupByOperator.cu:
+ * 101-130), one launch sequence per split.  A batch runs many instances of
+ * one operator signature (the same key column, aggregates and column types;
+ * each instance with its own columns, row count, predicate literals, output
+ * columns and group count) in one persistent fold kernel and one finalize,
+ * captured once in a CUDA graph.  ghb_batch_groupby_create validates the
+ * instances, optionally autotunes (CTA size per batch; shared-table size,
+ * load factor and warp combining per size class of rows x groups, timed on
+ * the class's largest instance), sizes one global table per instance and
+ * captures the launches; it synchronises `stream`.  ghb_batch_launch
+ * replays them on `stream`: every instance's output columns and
+ * d_out_groups[i] are rewritten from the current contents of its columns
+ * (the same device addresses as at creation).  Results are those of
+ * ghb_filter_groupby on each instance alone.  Errors raised on the device
+ * (GHB_ERR_CAPACITY when an instance has more groups than max_groups allows
+ * or than its out_capacity) are reported by ghb_sync. */
+typedef struct ghb_groupby_instance {
+  const ghb_column* cols;      /* ncols device columns of one length        */
+  const ghb_predicate* pred;   /* NULL: every row passes                    */
+  ghb_out_column* out;         /* nkeys + naggs device output columns       */
+  int64_t out_capacity;
+  int64_t max_groups;          /* groups expected; 0 = out_capacity         */
+} ghb_groupby_instance;
+
+typedef struct ghb_batch_cfg {
+  int32_t autotune;            /* 1: time candidate settings at creation    */
+  int32_t block_threads;       /* 512 or 1024; 0 = tuned, else 1024         */
+  int32_t smem_slots;          /* 0 = tuned / automatic, -1 = no shared table */
+  float load_factor;           /* 0 = tuned / 0.5                           */
+  int32_t use_graph;           /* 0: plain launches; otherwise a CUDA graph */
+} ghb_batch_cfg;
+
+typedef struct ghb_batch ghb_batch;
+int32_t ghb_batch_groupby_create(ghb_ctx* ctx, const ghb_groupby_instance* inst,
+                                 int32_t ninst, int32_t ncols,
+                                 const int32_t* key_cols, int32_t nkeys,
+                                 const ghb_agg_desc* aggs, int32_t naggs,
+                                 int64_t* d_out_groups, const ghb_batch_cfg* cfg,
+                                 void* stream, ghb_batch** out);
+int32_t ghb_batch_launch(ghb_batch* batch, void* stream);
+/* The settings the batch runs with (JSON text: block size, grid, chunks and
+ * per size class the shared slots, load factor and measured ns per row). */
+int32_t ghb_batch_describe(const ghb_batch* batch, char* buf, int64_t len);
+int32_t ghb_batch_destroy(ghb_batch* batch);
 
 /* ---- host-buffer entry points (end-to-end) -------------------------------
  * Same operators with every column in HOST memory (pageable or pinned).

@@ -33,10 +33,11 @@ def test_struct_layout_matches_header(tmp_path):
 #include <stddef.h>
 #include "ghive_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(ghb_column), sizeof(ghb_out_column),
-         sizeof(ghb_pred_node), sizeof(ghb_predicate), sizeof(ghb_agg_desc),
-         sizeof(ghb_groupby_cfg), sizeof(ghb_join_cfg), sizeof(ghb_sort_cfg),
-         offsetof(ghb_pred_node, lit_d));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(ghb_column),
+         sizeof(ghb_out_column), sizeof(ghb_pred_node), sizeof(ghb_predicate),
+         sizeof(ghb_agg_desc), sizeof(ghb_groupby_cfg), sizeof(ghb_join_cfg),
+         sizeof(ghb_sort_cfg), offsetof(ghb_pred_node, lit_d), sizeof(ghb_groupby_instance),
+         sizeof(ghb_batch_cfg), offsetof(ghb_batch_cfg, load_factor));
   return 0;
 }
 """)
@@ -46,8 +47,22 @@ int main(void) {
                                           check=True).stdout.split()]
     exp = [C.sizeof(abi.Column), C.sizeof(abi.OutColumn), C.sizeof(abi.PredNode),
            C.sizeof(abi.Predicate), C.sizeof(abi.AggDesc), C.sizeof(abi.GroupByCfg),
-           C.sizeof(abi.JoinCfg), C.sizeof(abi.SortCfg), abi.PredNode.lit_d.offset]
+           C.sizeof(abi.JoinCfg), C.sizeof(abi.SortCfg), abi.PredNode.lit_d.offset,
+           C.sizeof(abi.GroupByInstance), C.sizeof(abi.BatchCfg), abi.BatchCfg.load_factor.offset]
     assert got == exp
+
+
+def test_key_mixer_is_the_same_bijection_in_numpy_and_torch():
+    import numpy as np
+    import torch
+
+    from ghive_b200 import workloads
+    x = np.concatenate([np.arange(0, 5000, dtype=np.int64),
+                        np.array([-1, np.iinfo(np.int64).min, np.iinfo(np.int64).max])])
+    a = workloads.mix64_np(x)
+    b = workloads.mix64_torch(torch.from_numpy(x)).numpy()
+    assert np.array_equal(a, b)
+    assert len(np.unique(a)) == len(x)
 
 
 def test_enum_values_are_ghives():
