@@ -33,6 +33,14 @@ _PROTOS = {
     "ghb_batch_groupby_create": (I32, [P, P, I32, I32, P, I32, P, I32, P, P, P,
                                        C.POINTER(C.c_void_p)]),
     "ghb_batch_launch": (I32, [P, P]),
+    "ghb_server_create": (I32, [I32, P, C.POINTER(C.c_void_p)]),
+    "ghb_server_add_join_table": (I32, [P, P, P, I32, C.c_float, C.POINTER(I32)]),
+    "ghb_server_submit": (I32, [P, P, C.POINTER(C.c_uint64)]),
+    "ghb_server_wait": (I32, [P, C.c_uint64, P]),
+    "ghb_server_release": (I32, [P, C.c_uint64]),
+    "ghb_server_stats": (I32, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
+    "ghb_server_last_error": (C.c_char_p, [P]),
+    "ghb_server_destroy": (I32, [P]),
     "ghb_batch_describe": (I32, [P, C.c_char_p, I64]),
     "ghb_batch_destroy": (I32, [P]),
     "ghb_filter_host": (I32, [P, P, P, I32, P, I32, P, I64, C.POINTER(I64)]),

@@ -91,6 +91,29 @@ class GroupByInstance(C.Structure):
                 ("out_capacity", C.c_int64), ("max_groups", C.c_int64)]
 
 
+OP_FILTER, OP_GROUPBY, OP_JOIN_PROBE, OP_SORT = 0, 1, 2, 3
+MAX_RESULT_COLS = 16
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("reserved", C.c_int32), ("hbm_budget", C.c_int64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("op", C.c_int32), ("ncols", C.c_int32), ("cols", C.c_void_p),
+                ("pred", C.c_void_p), ("idx", C.c_void_p), ("nidx", C.c_int32),
+                ("naggs", C.c_int32), ("aggs", C.c_void_p), ("max_groups", C.c_int64),
+                ("table", C.c_int32), ("join_type", C.c_int32), ("nkeys", C.c_int32),
+                ("want_rowid", C.c_int32), ("orders", C.c_void_p), ("null_orders", C.c_void_p)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int32), ("ncols", C.c_int32),
+                ("cols", OutColumn * MAX_RESULT_COLS), ("rowid", C.c_void_p),
+                ("rowid2", C.c_void_p), ("rows", C.c_int64), ("submit_ns", C.c_int64),
+                ("admit_ns", C.c_int64), ("done_ns", C.c_int64)]
+
+
 class BatchCfg(C.Structure):
     _fields_ = [("autotune", C.c_int32), ("block_threads", C.c_int32),
                 ("smem_slots", C.c_int32), ("load_factor", C.c_float),

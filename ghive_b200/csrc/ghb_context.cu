@@ -28,21 +28,38 @@ int32_t scratch_reset(ghb_ctx* ctx) {
   return GHB_OK;
 }
 
+int32_t regrow(ghb_ctx* ctx, void** buf, size_t* bytes, size_t want, cudaStream_t stream, bool zero) {
+  if (ctx->stream_ordered) {
+    // the old buffer is only used on this stream: free and allocate in its order
+    if (*buf) cudaFreeAsync(*buf, stream);
+    *buf = nullptr;
+    *bytes = 0;
+    if (cudaMallocAsync(buf, want, stream) != cudaSuccess) {
+      cudaGetLastError();
+      *buf = nullptr;
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes of device memory", want);
+    }
+  } else {
+    // the old buffer may still be read by work queued on any stream
+    GHB_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *bytes = 0;
+    if (cudaMalloc(buf, want) != cudaSuccess) {
+      cudaGetLastError();
+      *buf = nullptr;
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes of device memory", want);
+    }
+  }
+  *bytes = want;
+  if (zero) GHB_CUDA_TRY(ctx, cudaMemsetAsync(*buf, 0, want, stream));
+  return GHB_OK;
+}
+
 int32_t scratch_reserve(ghb_ctx* ctx, size_t total, cudaStream_t stream) {
   if (total <= ctx->scratch_bytes) return GHB_OK;
   size_t want = std::max(total, ctx->scratch_bytes * 2);
-  // the old arena may still be read by work queued on any stream
-  GHB_CUDA_TRY(ctx, cudaDeviceSynchronize());
-  if (ctx->scratch) cudaFree(ctx->scratch);
-  ctx->scratch = nullptr;
-  ctx->scratch_bytes = 0;
-  if (cudaMalloc((void**)&ctx->scratch, want) != cudaSuccess) {
-    cudaGetLastError();
-    return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes of device scratch", want);
-  }
-  ctx->scratch_bytes = want;
-  (void)stream;
-  return GHB_OK;
+  return regrow(ctx, (void**)&ctx->scratch, &ctx->scratch_bytes, want, stream, false);
 }
 
 int32_t scratch_alloc(ghb_ctx* ctx, size_t bytes, void** out, cudaStream_t stream) {
@@ -61,16 +78,10 @@ int32_t scratch_alloc(ghb_ctx* ctx, size_t bytes, void** out, cudaStream_t strea
 int32_t lookback_prepare(ghb_ctx* ctx, int64_t tiles, uint32_t* epoch, cudaStream_t stream) {
   if (tiles > ctx->lb_tiles) {
     int64_t want = std::max<int64_t>(tiles, 1 << 16);
-    GHB_CUDA_TRY(ctx, cudaDeviceSynchronize());
-    if (ctx->lb_status) cudaFree(ctx->lb_status);
-    ctx->lb_status = nullptr;
+    size_t bytes = (size_t)ctx->lb_tiles * sizeof(uint64_t);
     ctx->lb_tiles = 0;
-    if (cudaMalloc((void**)&ctx->lb_status, want * sizeof(uint64_t)) != cudaSuccess) {
-      cudaGetLastError();
-      return set_error(ctx, GHB_ERR_OOM, "cannot allocate look-back state for %lld tiles",
-                       (long long)want);
-    }
-    GHB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->lb_status, 0, want * sizeof(uint64_t), stream));
+    int32_t st = regrow(ctx, (void**)&ctx->lb_status, &bytes, want * sizeof(uint64_t), stream, true);
+    if (st) return st;
     ctx->lb_tiles = want;
     ctx->epoch = 0;
   }

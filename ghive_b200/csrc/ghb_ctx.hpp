@@ -47,7 +47,19 @@ struct ghb_ctx {
   // pinned staging for the host-buffer entry points
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
+
+  // Every call of this context runs on one stream (a server slot): its
+  // device buffers grow with stream-ordered frees and allocations instead of
+  // a device-wide synchronisation, so other streams keep running.
+  bool stream_ordered = false;
 };
+
+namespace ghb {
+// Replaces *buf (of *bytes) with a zeroed or uninitialised buffer of `want`
+// bytes: stream-ordered on `stream` for a stream_ordered context, else after a
+// device synchronisation.
+int32_t regrow(ghb_ctx* ctx, void** buf, size_t* bytes, size_t want, cudaStream_t stream, bool zero);
+}  // namespace ghb
 
 struct ghb_join_table {
   unsigned long long* kimg = nullptr;  // per slot: key image (0 = empty)

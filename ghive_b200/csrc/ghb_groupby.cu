@@ -376,16 +376,9 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   } else {
     if (table_bytes > ctx->gb_bytes || ctx->gb_dirty || !ctx->gb_table) {
       if (table_bytes > ctx->gb_bytes) {
-        GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
-        if (ctx->gb_table) cudaFree(ctx->gb_table);
-        ctx->gb_table = nullptr;
-        ctx->gb_bytes = 0;
-        size_t want = std::max(table_bytes, (size_t)1 << 20);
-        if (cudaMalloc(&ctx->gb_table, want) != cudaSuccess) {
-          cudaGetLastError();
-          return set_error(ctx, GHB_ERR_OOM, "cannot allocate a %zu-byte group-by table", want);
-        }
-        ctx->gb_bytes = want;
+        int32_t gst = regrow(ctx, &ctx->gb_table, &ctx->gb_bytes, std::max(table_bytes, (size_t)1 << 20),
+                             stream, false);
+        if (gst) return gst;
       }
       GHB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->gb_table, 0, ctx->gb_bytes, stream));
       ctx->gb_dirty = false;

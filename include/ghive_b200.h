@@ -363,6 +363,85 @@ int32_t ghb_batch_launch(ghb_batch* batch, void* stream);
 int32_t ghb_batch_describe(const ghb_batch* batch, char* buf, int64_t len);
 int32_t ghb_batch_destroy(ghb_batch* batch);
 
+/* ---- serving: concurrent operator requests ------------------------------
+ * GHive's JNI entry point (GPUProcess, gpu_impl/src/ghive_JNIInterface.cu:
+ * 13-340) runs one Tez task's plan alone: every call re-uploads its inputs,
+ * rebuilds its join tables and owns the GPU until it returns.  A server is
+ * long-lived and shared by many host threads (Hive tasks): a request is
+ * queued on submit and admitted as soon as one of `slots` execution slots is
+ * free and its HBM footprint (outputs + working memory) fits the budget;
+ * admitted requests run concurrently, one CUDA stream and one context per
+ * slot, so a request that arrives while others are on the GPU overlaps with
+ * them (continuous batching).  Join build tables registered with the server
+ * stay resident across requests.  Inputs are device columns that must stay
+ * valid until the request is done; outputs are device buffers owned by the
+ * server until ghb_server_release.  Results are those of the plain operator
+ * on the same inputs.  All functions are thread-safe. */
+#define GHB_OP_FILTER 0
+#define GHB_OP_GROUPBY 1
+#define GHB_OP_JOIN_PROBE 2
+#define GHB_OP_SORT 3
+#define GHB_MAX_RESULT_COLS 16
+
+typedef struct ghb_server_cfg {
+  int32_t slots;               /* requests on the device at once (0 = 8)    */
+  int32_t reserved;
+  int64_t hbm_budget;          /* bytes admitted at once (0 = 40% of free)  */
+} ghb_server_cfg;
+
+typedef struct ghb_request {
+  int32_t op;                  /* GHB_OP_*                                    */
+  int32_t ncols;
+  const ghb_column* cols;      /* FILTER/GROUPBY inputs; JOIN_PROBE: cols[0] =
+                                  probe key; SORT: keys then payload          */
+  const ghb_predicate* pred;   /* FILTER, GROUPBY (NULL = all rows)           */
+  const int32_t* idx;          /* FILTER: projection (NULL = all columns);
+                                  GROUPBY: key columns                        */
+  int32_t nidx;
+  int32_t naggs;               /* GROUPBY                                     */
+  const ghb_agg_desc* aggs;
+  int64_t max_groups;          /* GROUPBY: output capacity in groups          */
+  int32_t table;               /* JOIN_PROBE: id from ghb_server_add_join_table */
+  int32_t join_type;
+  int32_t nkeys;               /* SORT: leading key columns                   */
+  int32_t want_rowid;          /* SORT: emit input row ids; JOIN_PROBE: also
+                                  emit build row ids                          */
+  const int32_t* orders;       /* SORT (NULL = all ASC)                       */
+  const int32_t* null_orders;  /* SORT (NULL = Hive defaults)                 */
+} ghb_request;
+
+typedef struct ghb_result {
+  int32_t status;              /* GHB_OK or the operator's error              */
+  int32_t ncols;
+  ghb_out_column cols[GHB_MAX_RESULT_COLS];  /* FILTER: projected columns;
+                                  GROUPBY: keys then aggregates; JOIN_PROBE:
+                                  the table's payload columns; SORT: keys
+                                  then payload                                */
+  int32_t* rowid;              /* JOIN_PROBE: probe row ids; SORT: row ids    */
+  int32_t* rowid2;             /* JOIN_PROBE: build row ids (want_rowid)      */
+  int64_t rows;                /* rows (groups) in the outputs                */
+  int64_t submit_ns;           /* CLOCK_MONOTONIC: submitted, admitted, done  */
+  int64_t admit_ns;
+  int64_t done_ns;
+} ghb_result;
+
+typedef struct ghb_server ghb_server;
+int32_t ghb_server_create(int32_t device, const ghb_server_cfg* cfg, ghb_server** out);
+/* Builds a join table on the device and keeps it (with its payload columns,
+ * which must stay valid) until the server is destroyed. */
+int32_t ghb_server_add_join_table(ghb_server* server, const ghb_column* build_key,
+                                  const ghb_column* payload, int32_t npayload,
+                                  float load_factor, int32_t* table_id);
+int32_t ghb_server_submit(ghb_server* server, const ghb_request* req, uint64_t* ticket);
+/* Waits until the request is done and copies its result. */
+int32_t ghb_server_wait(ghb_server* server, uint64_t ticket, ghb_result* out);
+/* Frees the request's outputs and its share of the budget. */
+int32_t ghb_server_release(ghb_server* server, uint64_t ticket);
+int32_t ghb_server_stats(ghb_server* server, int64_t* completed, int64_t* running,
+                         int64_t* queued, int64_t* bytes_admitted);
+const char* ghb_server_last_error(ghb_server* server);
+int32_t ghb_server_destroy(ghb_server* server);
+
 /* ---- host-buffer entry points (end-to-end) -------------------------------
  * Same operators with every column in HOST memory (pageable or pinned).
  * These copy the inputs in, run the operator, copy the result out and
