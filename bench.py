@@ -286,6 +286,8 @@ def run_ours(args, world, rank, local):
         ops["sort"] = bench_sort(ctx, args, dev, stream, peak)
         if not args.skip_batched:
             ops["batched_groupby"] = bench_batched(ctx, args, dev, stream, peak)
+        if not args.skip_served:
+            ops["served_mix"] = bench_served(ctx, args, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -492,6 +494,218 @@ def bench_batched(ctx, args, dev, stream, peak, count=512):
     return out
 
 
+def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.8, 0.95)):
+    """Served mixed operator stream against serial per-call execution."""
+    import itertools
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from ghive_b200 import abi, workloads
+    from ghive_b200.serve import Server
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(workloads.SEED + 4)
+
+    def ri(lo, hi, n, dt):
+        return torch.randint(lo, hi, (n,), generator=g, device=dev, dtype=dt)
+
+    # resident column pools (requests are slices) and 8 build tables
+    fact = [ri(0, 1000, max_rows, torch.int32), ri(1, 51, max_rows, torch.int64),
+            ri(90000, 10500001, max_rows, torch.int64).to(torch.float64) / 100.0,
+            ri(0, 2526, max_rows, torch.int32)]
+    sortc = [ri(0, 2526, max_rows, torch.int32), ri(0, 1 << 40, max_rows, torch.int64),
+             torch.arange(max_rows, dtype=torch.int32, device=dev)]
+    sizes = [int(x) for x in np.exp(workloads.rng(4, 1).uniform(np.log(1e5), np.log(1e7), 8))]
+    builds, probes = [], []
+    for sz in sizes:
+        key = torch.randperm(sz, generator=g, device=dev, dtype=torch.int64) + 1
+        builds.append((key, [ri(0, 1 << 62, sz, torch.int64),
+                             torch.rand(sz, generator=g, device=dev, dtype=torch.float64)]))
+        pk = ri(1, sz + 1, max_rows, torch.int64)
+        miss = torch.rand(max_rows, generator=g, device=dev) < 0.05
+        probes.append(torch.where(miss, pk + sz, pk))
+    specs = workloads.served_specs(n_req, seed_idx=4, max_rows=max_rows)
+    rows_total = sum(s["rows"] for s in specs)
+    aggs = workloads.AGGS_FACT
+
+    def sl(cols, s):
+        return [c[s["offset"]:s["offset"] + s["rows"]] for c in cols]
+
+    def run_plain(s):
+        pred = workloads.fact_predicate(s["cut"])
+        if s["op"] == "groupby":
+            ctx.filter_groupby(pred, sl(fact, s), [0], aggs, capacity=1000, max_groups=1000)
+        elif s["op"] == "filter":
+            ctx.filter(pred, sl(fact, s), proj=[0, 1, 2])
+        elif s["op"] == "sort":
+            ctx.sort(sl(sortc[:2], s), payload=sl(sortc[2:], s))
+        else:
+            key, pay = builds[s["table"]]
+            t = ctx.join_build(key, build_payload=pay)
+            ctx.join_probe(t, sl([probes[s["table"]]], s)[0], abi.INNER_JOIN, capacity=s["rows"],
+                           rowids=True)
+            t.free()
+
+    # serial per-call execution: one request at a time, each returning its
+    # result; a full untimed pass first so the allocators hold their sizes
+    for s in specs:
+        run_plain(s)
+    torch.cuda.synchronize()
+    service = []
+    t0 = time.perf_counter()
+    for s in specs:
+        a = time.perf_counter()
+        run_plain(s)
+        service.append(time.perf_counter() - a)
+    serial_s = time.perf_counter() - t0
+    serial_rate = len(specs) / serial_s
+
+    # per call through the host-buffer entry points, the way a Hive task calls
+    # GHive's JNI path: pageable host inputs in, results copied back into host
+    # arrays made per call; a bounded sample of the requests
+    hfact = [c.cpu().numpy() for c in fact]
+    hsort = [c.cpu().numpy() for c in sortc]
+    hprobe = [p.cpu().numpy() for p in probes]
+    hbuild = [(k.cpu().numpy(), [x.cpu().numpy() for x in p]) for k, p in builds]
+
+    def run_host(s):
+        pred = workloads.fact_predicate(s["cut"])
+        if s["op"] == "groupby":
+            ctx.filter_groupby_host(pred, sl(hfact, s), [0], aggs, 1000, max_groups=1000)
+        elif s["op"] == "filter":
+            ctx.filter_host(pred, sl(hfact, s), proj=[0, 1, 2])
+        elif s["op"] == "sort":
+            ctx.sort_host(sl(hsort[:2], s), payload=sl(hsort[2:], s))
+        else:
+            key, pay = hbuild[s["table"]]
+            ctx.hash_join_host(key, sl([hprobe[s["table"]]], s)[0], abi.INNER_JOIN,
+                               build_payload=pay, capacity=s["rows"])
+
+    host_sample = specs[:100]
+    for s in host_sample[:5]:
+        run_host(s)
+    t0 = time.perf_counter()
+    for s in host_sample:
+        run_host(s)
+    host_s = time.perf_counter() - t0
+    host_rows = sum(s["rows"] for s in host_sample)
+    del hfact, hsort, hprobe, hbuild
+
+    srv = Server(dev.index, slots=8)
+    try:
+        tids = [srv.add_join_table(k, p) for k, p in builds]
+
+        def submit(i):
+            s = specs[i]
+            pred = workloads.fact_predicate(s["cut"])
+            if s["op"] == "groupby":
+                return srv.submit_groupby(pred, sl(fact, s), [0], aggs, 1000)
+            if s["op"] == "filter":
+                return srv.submit_filter(pred, sl(fact, s), proj=[0, 1, 2])
+            if s["op"] == "sort":
+                return srv.submit_sort(sl(sortc[:2], s), payload=sl(sortc[2:], s))
+            return srv.submit_join(tids[s["table"]], sl([probes[s["table"]]], s)[0])
+
+        def closed(clients):
+            it = itertools.count()
+            lat = [0.0] * len(specs)
+
+            def client():
+                while True:
+                    i = next(it)
+                    if i >= len(specs):
+                        return
+                    t = submit(i)
+                    try:
+                        lat[i] = srv.wait(t).latency_ms
+                    finally:
+                        srv.release(t)
+
+            a = time.perf_counter()
+            ths = [threading.Thread(target=client) for _ in range(clients)]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            return time.perf_counter() - a, lat
+
+        def pct(v):
+            v = np.asarray(v)
+            return {"p50_ms": float(np.percentile(v, 50)), "p95_ms": float(np.percentile(v, 95)),
+                    "p99_ms": float(np.percentile(v, 99))}
+
+        closed(64)   # warm-up: slot arenas grow to their working sizes
+        sat = {}
+        for c in (1, 8, 64):
+            dt, lat = closed(c)
+            sat["clients_%d" % c] = dict(rows_per_s=rows_total / dt, ms=dt * 1e3, **pct(lat))
+        best = max(v["rows_per_s"] for v in sat.values())
+
+        load = {}
+        arr_rng = workloads.rng(4, 2)
+        for frac in loads:
+            rate = frac * serial_rate
+            arrivals = np.cumsum(arr_rng.exponential(1.0 / rate, len(specs)))
+            lat = [0.0] * len(specs)
+            qwait = [0.0] * len(specs)
+            first, last = [None], [0]
+
+            def waiter(i, t):
+                try:
+                    r = srv.wait(t)
+                    lat[i] = r.latency_ms
+                    qwait[i] = (r.admit_ns - r.submit_ns) / 1e6
+                    last[0] = max(last[0], r.done_ns)
+                    if first[0] is None or r.submit_ns < first[0]:
+                        first[0] = r.submit_ns
+                finally:
+                    srv.release(t)
+
+            with ThreadPoolExecutor(64) as ex:
+                a = time.perf_counter()
+                futs = []
+                for i, at in enumerate(arrivals):
+                    d = a + at - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    futs.append(ex.submit(waiter, i, submit(i)))
+                for f in futs:
+                    f.result()
+            span = (last[0] - first[0]) / 1e9
+            # serial execution under the same arrivals: a FIFO single server with
+            # the service times measured above
+            fin, slat = 0.0, []
+            for at, sv in zip(arrivals, service):
+                fin = max(at, fin) + sv
+                slat.append((fin - at) * 1e3)
+            name = "%d%%" % round(frac * 100)
+            load[name if name not in load else name + "_again"] = {
+                "offered_requests_per_s": rate,
+                "served": dict(rows_per_s=rows_total / span, queue_wait_p50_ms=float(np.median(qwait)),
+                               queue_wait_p99_ms=float(np.percentile(qwait, 99)), **pct(lat)),
+                "serial": dict(rows_per_s=rows_total / max(fin, 1e-9), **pct(slat))}
+    finally:
+        srv.close()
+    out = {"workload": "%d requests: 40%% filter+group-by, 30%% join probe against 8 resident build "
+                       "tables (1e5-1e7 keys), 20%% sort, 10%% filter; rows log-U[1e4,1e8] "
+                       "(%d in all), device-resident inputs" % (n_req, rows_total),
+           "requests": n_req, "rows": rows_total, "slots": 8,
+           "serial": {"rows_per_s": rows_total / serial_s, "ms": serial_s * 1e3,
+                      "note": "one plain operator call at a time, each synchronised; a probe "
+                              "builds its table first"},
+           "serial_host_buffers": {"rows_per_s": host_rows / host_s, "ms": host_s * 1e3,
+                                   "sample": "first %d requests (%d rows)" % (len(host_sample), host_rows),
+                                   "note": "ghb_*_host per call: pageable host inputs, results "
+                                           "copied back, a probe builds its table first"},
+           "served_saturation": sat, "speedup_vs_serial": best / (rows_total / serial_s),
+           "speedup_vs_serial_host_buffers": best / (host_rows / host_s),
+           "latency_under_load": load}
+    del fact, sortc, builds, probes
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,6 +715,7 @@ def main():
     ap.add_argument("--headline-only", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-served", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

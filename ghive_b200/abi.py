@@ -111,7 +111,8 @@ class Result(C.Structure):
     _fields_ = [("status", C.c_int32), ("ncols", C.c_int32),
                 ("cols", OutColumn * MAX_RESULT_COLS), ("rowid", C.c_void_p),
                 ("rowid2", C.c_void_p), ("rows", C.c_int64), ("submit_ns", C.c_int64),
-                ("admit_ns", C.c_int64), ("done_ns", C.c_int64)]
+                ("admit_ns", C.c_int64), ("done_ns", C.c_int64), ("launched_ns", C.c_int64),
+                ("slot", C.c_int32), ("reserved", C.c_int32)]
 
 
 class BatchCfg(C.Structure):

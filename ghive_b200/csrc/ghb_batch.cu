@@ -312,7 +312,7 @@ static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<
   im->fold = fold_fn(keyed, nullable);
   im->threads = threads;
   im->smem = smem_fold;
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(im->fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fold));
+  if (int32_t ast = ensure_dyn_smem(ctx, (const void*)im->fold, smem_fold)) return ast;
   int per_sm = 0;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, im->fold, threads, smem_fold));
   per_sm = std::max(1, per_sm);
@@ -471,7 +471,7 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
   int per_sm = 1;
   FoldFn fn = fold_fn(sig.nkeys == 1, sig.nullable);
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem(smem_fold)));
+  if (int32_t ast = ensure_dyn_smem(ctx, (const void*)fn, batch_smem(smem_fold))) return ast;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs.threads, batch_smem(smem_fold)));
   per_sm = std::max(1, per_sm);
   const double target = total / ((double)ctx->num_sms * per_sm * 6.0);

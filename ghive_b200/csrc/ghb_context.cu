@@ -6,6 +6,8 @@
 // convention (gpu_impl/src/ghive_JNIInterface.cu:111-118) with status codes.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "ghb_ctx.hpp"
 
@@ -34,7 +36,9 @@ int32_t regrow(ghb_ctx* ctx, void** buf, size_t* bytes, size_t want, cudaStream_
     if (*buf) cudaFreeAsync(*buf, stream);
     *buf = nullptr;
     *bytes = 0;
-    if (cudaMallocAsync(buf, want, stream) != cudaSuccess) {
+    cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(buf, want, ctx->pool, stream)
+                              : cudaMallocAsync(buf, want, stream);
+    if (e != cudaSuccess) {
       cudaGetLastError();
       *buf = nullptr;
       return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes of device memory", want);
@@ -53,6 +57,29 @@ int32_t regrow(ghb_ctx* ctx, void** buf, size_t* bytes, size_t want, cudaStream_
   }
   *bytes = want;
   if (zero) GHB_CUDA_TRY(ctx, cudaMemsetAsync(*buf, 0, want, stream));
+  return GHB_OK;
+}
+
+int32_t ensure_dyn_smem(ghb_ctx* ctx, const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> done;
+  int dev = 0;
+  GHB_CUDA_TRY(ctx, cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(dev, fn);
+  auto it = done.find(key);
+  if (it != done.end() && (size_t)it->second >= bytes) return GHB_OK;
+  int optin = 0;
+  GHB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  GHB_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, fn));
+  // the dynamic limit is what the opt-in maximum leaves beside the static part
+  const int limit = optin - (int)fa.sharedSizeBytes;
+  if (bytes > (size_t)limit)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED,
+                     "kernel needs %zu bytes of dynamic shared memory, at most %d are available", bytes, limit);
+  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  done[key] = limit;
   return GHB_OK;
 }
 

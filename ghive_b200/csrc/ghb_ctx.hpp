@@ -52,6 +52,9 @@ struct ghb_ctx {
   // device buffers grow with stream-ordered frees and allocations instead of
   // a device-wide synchronisation, so other streams keep running.
   bool stream_ordered = false;
+  // Pool for those stream-ordered allocations (nullptr = the device's
+  // default pool).
+  cudaMemPool_t pool = nullptr;
 };
 
 namespace ghb {
@@ -59,6 +62,11 @@ namespace ghb {
 // bytes: stream-ordered on `stream` for a stream_ordered context, else after a
 // device synchronisation.
 int32_t regrow(ghb_ctx* ctx, void** buf, size_t* bytes, size_t want, cudaStream_t stream, bool zero);
+// Lets kernel `fn` use up to `bytes` of dynamic shared memory on the current
+// device.  The attribute is set once per kernel and device (to the device's
+// opt-in maximum): changing a kernel's attributes on every call would put a
+// runtime call that may wait on running work into every launch path.
+int32_t ensure_dyn_smem(ghb_ctx* ctx, const void* fn, size_t bytes);
 }  // namespace ghb
 
 struct ghb_join_table {

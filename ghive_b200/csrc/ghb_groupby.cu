@@ -393,7 +393,7 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
                    : (nullable ? gb_fold_kernel<false, true> : gb_fold_kernel<false, false>);
   const int threads = su.threads;
   int blocks_per_sm = 0;
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (int32_t ast = ensure_dyn_smem(ctx, (const void*)kfn, smem)) return ast;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kfn, threads, smem));
   blocks_per_sm = std::max(1, blocks_per_sm);
   if (cfg && cfg->ctas_per_sm > 0) blocks_per_sm = std::min(blocks_per_sm, cfg->ctas_per_sm);

@@ -75,7 +75,6 @@ struct Req {
   int64_t out_rows = 0;          // capacity in rows
   size_t out_bytes = 0, work_bytes = 0;
   void* block = nullptr;
-  cudaStream_t block_stream = nullptr;
   ghb_result res{};
   bool admitted = false, done = false;
 };
@@ -93,6 +92,7 @@ struct ghb_server;
 
 namespace {
 struct Slot {
+  int32_t id = 0;
   ghb_server* srv = nullptr;
   ghb_ctx* ctx = nullptr;
   cudaStream_t stream = nullptr;
@@ -117,6 +117,13 @@ struct ghb_server {
   std::vector<Table> tables;
   ghb_ctx* table_ctx = nullptr;
   cudaStream_t table_stream = nullptr;
+  // Request outputs and the slots' working memory come from this pool, which
+  // never makes one stream wait on another to reuse a block (it grows
+  // instead); a released request's outputs are freed on free_stream, which
+  // runs nothing, so the block is reusable at once rather than after whatever
+  // its slot started next.
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t free_stream = nullptr;
   std::string last_error;
 };
 
@@ -226,6 +233,7 @@ void try_admit(ghb_server* s) {
       s->admitted_bytes += need;
       q->admitted = true;
       q->res.admit_ns = t;
+      q->res.slot = idle->id;
       s->running++;
       idle->cur = q;
       idle->cv.notify_one();
@@ -243,12 +251,11 @@ void execute(ghb_server* s, Slot* sl, Req* q) {
   cudaStream_t st = sl->stream;
   ghb_result& r = q->res;
   int32_t rc = GHB_OK;
-  if (cudaMallocAsync(&q->block, q->out_bytes, st) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync(&q->block, q->out_bytes, s->pool, st) != cudaSuccess) {
     cudaGetLastError();
     q->block = nullptr;
     rc = GHB_ERR_OOM;
   }
-  q->block_stream = st;
   int64_t* d_count = (int64_t*)q->block;
   if (rc == GHB_OK) {
     // carve the outputs
@@ -299,6 +306,7 @@ void execute(ghb_server* s, Slot* sl, Req* q) {
       }
     }
   }
+  r.launched_ns = now_ns();
   if (rc == GHB_OK) {
     cudaMemcpyAsync(&sl->pinned[0], d_count, 8, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&sl->pinned[1], ctx->d_status, 4, cudaMemcpyDeviceToHost, st);
@@ -359,14 +367,43 @@ extern "C" int32_t ghb_server_create(int32_t device, const ghb_server_cfg* cfg, 
   cudaMemGetInfo(&free_b, &total_b);
   s->budget = (cfg && cfg->hbm_budget > 0) ? cfg->hbm_budget : (int64_t)(free_b * 0.4);
   int32_t st = ghb_ctx_create(device, 0, &s->table_ctx);
-  if (st == GHB_OK && cudaStreamCreateWithFlags(&s->table_stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (st == GHB_OK && (cudaStreamCreateWithFlags(&s->table_stream, cudaStreamNonBlocking) != cudaSuccess ||
+                       cudaStreamCreateWithFlags(&s->free_stream, cudaStreamNonBlocking) != cudaSuccess))
     st = GHB_ERR_CUDA;
+  if (st == GHB_OK) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    int no = 0;
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no) != cudaSuccess ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+      cudaGetLastError();
+      st = GHB_ERR_CUDA;
+    }
+  }
+  if (st == GHB_OK) {
+    // Map the whole budget into the pool now: growing a pool maps physical
+    // memory under a driver lock, which stalls every other slot's calls
+    // while it runs.
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, (size_t)s->budget, s->pool, s->table_stream) != cudaSuccess ||
+        cudaFreeAsync(p, s->table_stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->table_stream) != cudaSuccess) {
+      cudaGetLastError();
+      st = GHB_ERR_OOM;
+    }
+  }
   for (int i = 0; i < nslots && st == GHB_OK; i++) {
     auto sl = std::make_unique<Slot>();
     sl->srv = s;
+    sl->id = i;
     st = ghb_ctx_create(device, 0, &sl->ctx);
     if (st) break;
     sl->ctx->stream_ordered = true;
+    sl->ctx->pool = s->pool;
     if (cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost((void**)&sl->pinned, 16) != cudaSuccess) {
       cudaGetLastError();
@@ -492,7 +529,8 @@ extern "C" int32_t ghb_server_release(ghb_server* s, uint64_t ticket) {
   }
   if (q->block) {
     cudaSetDevice(s->device);
-    cudaFreeAsync(q->block, q->block_stream);
+    // the request is done: free on the idle stream, reusable immediately
+    cudaFreeAsync(q->block, s->free_stream);
   }
   delete q;
   return GHB_OK;
@@ -547,7 +585,10 @@ extern "C" int32_t ghb_server_destroy(ghb_server* s) {
     if (sl->ctx) ghb_ctx_destroy(sl->ctx);
   }
   if (s->table_stream) cudaStreamDestroy(s->table_stream);
+  if (s->free_stream) cudaStreamDestroy(s->free_stream);
   if (s->table_ctx) ghb_ctx_destroy(s->table_ctx);
+  cudaDeviceSynchronize();
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   return GHB_OK;
 }

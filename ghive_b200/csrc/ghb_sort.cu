@@ -480,7 +480,10 @@ static void launch_pass(int src, int dst, int grid, size_t dyn, cudaStream_t s, 
 template <typename V>
 static int32_t set_smem(ghb_ctx* ctx, size_t dyn) {
 #define GHB_ATTR(S, D) \
-  GHB_CUDA_TRY(ctx, cudaFuncSetAttribute(sort_pass_kernel<V, S, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn))
+  do {                                                                      \
+    int32_t _st = ensure_dyn_smem(ctx, (const void*)sort_pass_kernel<V, S, D>, dyn); \
+    if (_st) return _st;                                                    \
+  } while (0)
   GHB_ATTR(kSrcPacked, kDstPacked);
   GHB_ATTR(kSrcPacked, kDstDecode);
   GHB_ATTR(kSrcPacked, kDstGather);

@@ -36,6 +36,7 @@ class ServedResult:
     def __init__(self, res, device):
         self.status, self.rows = res.status, res.rows
         self.submit_ns, self.admit_ns, self.done_ns = res.submit_ns, res.admit_ns, res.done_ns
+        self.launched_ns, self.slot = res.launched_ns, res.slot
         n = max(0, res.rows)
         self.cols = []
         for j in range(res.ncols):

@@ -161,6 +161,25 @@ def batched_instances_device(specs, device, seed_idx=3):
     return out
 
 
+SERVED_MIX = (("groupby", 0.4), ("join", 0.3), ("sort", 0.2), ("filter", 0.1))
+
+
+def served_specs(count, seed_idx=4, min_rows=10_000, max_rows=100_000_000, tables=8):
+    """Requests of the served mixed stream: operator by SERVED_MIX, rows
+    log-U[min_rows,max_rows], an offset into the resident column pools, a
+    predicate cut (d < cut) and a build table id for probes."""
+    g = rng(seed_idx)
+    names = [m for m, _ in SERVED_MIX]
+    p = np.array([w for _, w in SERVED_MIX])
+    out = []
+    for _ in range(count):
+        op = names[int(g.choice(len(names), p=p))]
+        rows = int(np.exp(g.uniform(np.log(min_rows), np.log(max_rows))))
+        out.append({"op": op, "rows": rows, "offset": int(g.integers(0, max_rows - rows + 1)),
+                    "cut": int(g.integers(126, 2400)), "table": int(g.integers(0, tables))})
+    return out
+
+
 def batched_predicate(cut):
     """d < cut on column 3 of a batched instance."""
     return abi.Pred.leaf(abi.FILTER_LT, 3, a=cut)

@@ -386,7 +386,9 @@ int32_t ghb_batch_destroy(ghb_batch* batch);
 typedef struct ghb_server_cfg {
   int32_t slots;               /* requests on the device at once (0 = 8)    */
   int32_t reserved;
-  int64_t hbm_budget;          /* bytes admitted at once (0 = 40% of free)  */
+  int64_t hbm_budget;          /* bytes admitted at once (0 = 40% of free);
+                                  mapped into the server's memory pool when
+                                  it is created, so serving never grows it */
 } ghb_server_cfg;
 
 typedef struct ghb_request {
@@ -423,6 +425,9 @@ typedef struct ghb_result {
   int64_t submit_ns;           /* CLOCK_MONOTONIC: submitted, admitted, done  */
   int64_t admit_ns;
   int64_t done_ns;
+  int64_t launched_ns;         /* the operator's launches had all returned   */
+  int32_t slot;                /* the slot that ran it                        */
+  int32_t reserved;
 } ghb_result;
 
 typedef struct ghb_server ghb_server;
