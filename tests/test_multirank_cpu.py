@@ -1,0 +1,131 @@
+"""Multi-rank host logic on CPU: world_size-2 gloo process groups.
+
+Each rank runs the oracle on its shard (the device kernels' results equal the
+oracle's, as the GPU tests show), the ranks exchange their partial results
+with a collective, and the merged result must equal the oracle over all rows:
+bit-exact for keys, counts, integer sums, MIN/MAX and join pairs, DOUBLE
+SUM/AVG within REL_TOL.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from ghive_b200 import abi, shard, workloads
+
+REL_TOL = 1e-12
+WORLD = 2
+
+
+def _port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _groupby_rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    from oracle import oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cols = workloads.fact_table(200_003, seed_idx=51, groups=700)
+        lo, hi = shard.shard_range(len(cols[0]), rank, world)
+        part, _ = shard.partial_aggs(workloads.AGGS_FACT)
+        k, v = oracle.filter_groupby(workloads.fact_predicate(), [c[lo:hi] for c in cols], [0], part)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (k[0], v))
+        if rank == 0:
+            q.put(gathered)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _join_rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    from oracle import oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        (bkey, bpay), (fk, _) = workloads.join_tables(50_000, 300_001, seed_idx=52)
+        lo, hi = shard.shard_range(len(fk), rank, world)
+        prow, outs = oracle.hash_join_mt(2, bkey, fk[lo:hi], bpay)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (np.asarray(prow) + lo, [np.asarray(o) for o in outs]))
+        if rank == 0:
+            q.put(gathered)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _spawn(fn):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    procs = [ctx.Process(target=fn, args=(r, WORLD, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    out = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    return out
+
+
+def test_shard_ranges_cover_rows_once():
+    for n in (0, 1, 7, 1000, 1001):
+        for w in (1, 2, 3, 8):
+            got = [shard.shard_range(n, r, w) for r in range(w)]
+            assert got[0][0] == 0 and got[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(got, got[1:]))
+            assert max(h - l for l, h in got) - min(h - l for l, h in got) <= 1
+
+
+def test_sharded_groupby_merges_to_the_whole():
+    from oracle import oracle
+    gathered = _spawn(_groupby_rank)
+    key, vals = shard.merge_groupby([(k, v) for k, v in gathered], workloads.AGGS_FACT)
+    cols = workloads.fact_table(200_003, seed_idx=51, groups=700)
+    ek, ev = oracle.filter_groupby(workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT)
+    assert np.array_equal(key[0], ek[0][0]) and np.array_equal(key[1], ek[0][1])
+    for j, ((gv, gn), (xv, xn)) in enumerate(zip(vals, ev)):
+        assert np.array_equal(gn, xn), j
+        if xv.dtype.kind == "f":
+            assert np.all(np.abs(gv[~gn] - xv[~xn]) <= REL_TOL * np.abs(xv[~xn])), j
+        else:
+            assert np.array_equal(gv[~gn].astype(xv.dtype), xv[~xn]), j
+
+
+def test_sharded_join_probe_unions_to_the_whole():
+    from oracle import oracle
+    gathered = _spawn(_join_rank)
+    (bkey, bpay), (fk, _) = workloads.join_tables(50_000, 300_001, seed_idx=52)
+    prow, outs = oracle.hash_join_mt(2, bkey, fk, bpay)
+    got = sorted(zip(np.concatenate([g[0] for g in gathered]).tolist(),
+                     *[np.concatenate([g[1][j] for g in gathered]).tolist() for j in range(len(bpay))]))
+    exp = sorted(zip(np.asarray(prow).tolist(), *[np.asarray(o).tolist() for o in outs]))
+    assert got == exp
+
+
+def test_global_aggregate_partials_merge():
+    parts = []
+    g = np.random.default_rng(3)
+    allv = []
+    for _ in range(3):
+        v = g.integers(-10, 10, 100).astype(np.int64)
+        allv.append(v)
+        parts.append((None, [(np.array([v.sum()]), np.array([False])),
+                             (np.array([v.min()]), np.array([False]))]))
+    _, vals = shard.merge_groupby(parts, [(abi.SUM, 0), (abi.MIN, 0)], has_key=False)
+    a = np.concatenate(allv)
+    assert vals[0][0][0] == a.sum() and vals[1][0][0] == a.min()
+
+
+if __name__ == "__main__":
+    pytest.main([__file__, "-q"])
