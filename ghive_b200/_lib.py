@@ -33,6 +33,8 @@ _PROTOS = {
     "ghb_batch_groupby_create": (I32, [P, P, I32, I32, P, I32, P, I32, P, P, P,
                                        C.POINTER(C.c_void_p)]),
     "ghb_batch_launch": (I32, [P, P]),
+    "ghb_jit_groupby_source": (I32, [P, P, I32, P, I32, P, I32, I32, C.c_char_p, I64]),
+    "ghb_jit_compile_source": (I32, [C.c_char_p, C.POINTER(I64), C.c_char_p, I64]),
     "ghb_server_create": (I32, [I32, P, C.POINTER(C.c_void_p)]),
     "ghb_server_add_join_table": (I32, [P, P, P, I32, C.c_float, C.POINTER(I32)]),
     "ghb_server_submit": (I32, [P, P, C.POINTER(C.c_uint64)]),

@@ -47,15 +47,50 @@ def _stale(obj, src, hdr_mtime):
     return m < os.path.getmtime(src) or m < hdr_mtime
 
 
+# Headers the run-time compiler (NVRTC) needs for the specialised group-by
+# kernels, embedded in the library under the names their #includes use.
+JIT_HEADERS = [("ghb_gb_sig.cuh", os.path.join(CSRC, "ghb_gb_sig.cuh")),
+               ("ghb_groupby.cuh", os.path.join(CSRC, "ghb_groupby.cuh")),
+               ("ghb_internal.cuh", os.path.join(CSRC, "ghb_internal.cuh")),
+               ("../../include/ghive_b200.h", os.path.join(ROOT, "include", "ghive_b200.h"))]
+
+
+def _jit_headers_source(path):
+    """Writes a C++ file defining the embedded header table (when stale)."""
+    newest = max(os.path.getmtime(f) for _, f in JIT_HEADERS)
+    if os.path.exists(path) and os.path.getmtime(path) >= newest:
+        return path
+    out = ["// generated by ghive_b200/build.py: headers for run-time compilation"]
+    names, srcs = [], []
+    for name, f in JIT_HEADERS:
+        text = open(f).read()
+        delim = "GHBJIT"
+        assert ")" + delim + '"' not in text
+        names.append('"%s"' % name)
+        srcs.append('R"%s(%s)%s"' % (delim, text, delim))
+    out.append("extern const int ghb_jit_nheaders = %d;" % len(JIT_HEADERS))
+    out.append("extern const char* const ghb_jit_header_names[] = {%s};" % ", ".join(names))
+    out.append("extern const char* const ghb_jit_header_srcs[] = {\n%s};" % ",\n".join(srcs))
+    with open(path + ".tmp", "w") as fh:
+        fh.write("\n".join(out) + "\n")
+    os.replace(path + ".tmp", path)
+    return path
+
+
+def _cuda_lib_dir(cc):
+    return os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(cc))), "lib64")
+
+
 def build(jobs=None, verbose=False, extra_flags=()):
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs.append(_jit_headers_source(os.path.join(BUILD, "ghb_jit_headers.cpp")))
     hdr_mtime = max(os.path.getmtime(h) for h in _headers())
     cc = nvcc()
     objs, todo = [], []
     for s in srcs:
-        o = os.path.join(BUILD, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(BUILD, os.path.splitext(os.path.basename(s))[0] + ".o")
         objs.append(o)
         if _stale(o, s, hdr_mtime) or extra_flags:
             todo.append((s, o))
@@ -75,7 +110,8 @@ def build(jobs=None, verbose=False, extra_flags=()):
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count()) as ex:
         list(ex.map(compile_one, todo))
     if todo or not os.path.exists(LIB):
-        cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + \
+            ["-lcudart", "-lnvrtc", "-Xlinker", "-rpath," + _cuda_lib_dir(cc)]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -36,21 +36,6 @@ namespace ghb {
 
 static_assert(sizeof(GbParams) % 8 == 0, "GbParams is copied to shared memory in 8-byte words");
 
-struct BatchChunk {
-  int32_t inst;
-  int32_t ntiles;
-  int64_t tile0;
-};
-
-struct BatchParams {
-  const GbParams* insts;
-  const BatchChunk* chunks;
-  int64_t nchunks;
-  unsigned long long* claim;   // next chunk to hand out (reset by the finalize)
-  int32_t stage_bytes;         // the same for every instance
-  int32_t table_words;         // shared-table words reserved per CTA
-};
-
 struct BatchFinParams {
   const FinParams* fins;
   const int64_t* choff;        // [ninst + 1]: first finalize chunk of each instance
@@ -61,125 +46,7 @@ struct BatchFinParams {
 
 template <bool KEYED, bool NULLABLE>
 __global__ void __launch_bounds__(kGbThreads) gb_batch_fold_kernel(BatchParams bp) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  // layout: [stage 0][stage 1][mbarriers][instance params][claim][table][warp staging]
-  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)bp.stage_bytes);
-  GbParams* sp = (GbParams*)(bars + 2);
-  long long* sclaim = (long long*)(sp + 1);
-  uint64_t* skeys = (uint64_t*)(sclaim + 2);
-  uint64_t* wstage = skeys + bp.table_words + (threadIdx.x >> 5) * 32;
-
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  // The CTA's tile stream: the tiles of the chunk it claimed last.  Every
-  // thread holds the same state, so the barriers inside are uniform.
-  int32_t c_inst = -1;
-  int64_t c_next = 0, c_end = 0;
-  bool exhausted = false;
-  auto next_tile = [&](int32_t* inst, int64_t* tile) -> bool {
-    if (c_next >= c_end) {
-      if (exhausted) return false;
-      if (threadIdx.x == 0) *sclaim = (long long)atomicAdd(bp.claim, 1ull);
-      __syncthreads();
-      const long long c = *sclaim;
-      __syncthreads();
-      if (c >= bp.nchunks) {
-        exhausted = true;
-        return false;
-      }
-      const BatchChunk ch = bp.chunks[c];
-      c_inst = ch.inst;
-      c_next = ch.tile0;
-      c_end = ch.tile0 + ch.ntiles;
-    }
-    *inst = c_inst;
-    *tile = c_next++;
-    return true;
-  };
-  // Starts loading a tile into stage s; true when it arrives by bulk copy.
-  auto issue = [&](int s, int32_t inst, int64_t tile) -> bool {
-    const GbParams& gp = bp.insts[inst];
-    unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
-    if (gp.bulk && (tile + 1) * gp.tile_rows <= gp.n) {
-      if (threadIdx.x == 0) {
-        fence_proxy_async_smem();
-        load_tile_bulk(gp, stage, tile, &bars[s]);
-      }
-      return true;
-    }
-    load_tile_plain(gp, stage, tile);
-    return false;
-  };
-
-  int32_t q_inst[2] = {-1, -1};
-  int64_t q_tile[2] = {0, 0};
-  uint32_t valid = 0, pending = 0, phase = 0;
-  for (int s = 0; s < 2; s++) {
-    if (!next_tile(&q_inst[s], &q_tile[s])) break;
-    valid |= 1u << s;
-    if (issue(s, q_inst[s], q_tile[s])) pending |= 1u << s;
-  }
-
-  int32_t active = -1;
-  bool failed = false;
-  for (int64_t it = 0;; it++) {
-    const int s = (int)(it & 1);
-    if (!((valid >> s) & 1u)) break;
-    const int32_t inst = s ? q_inst[1] : q_inst[0];
-    const int64_t tile = s ? q_tile[1] : q_tile[0];
-    if (inst != active) {
-      if (active >= 0) {
-        flush_smem_table(*sp, skeys);
-        __syncthreads();
-      }
-      const uint64_t* src = (const uint64_t*)&bp.insts[inst];
-      for (int k = threadIdx.x; k < (int)(sizeof(GbParams) / 8); k += blockDim.x)
-        ((uint64_t*)sp)[k] = src[k];
-      __syncthreads();
-      smem_table_clear(*sp, skeys);
-      __syncthreads();
-      active = inst;
-    }
-    if ((pending >> s) & 1u) {
-      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
-      phase ^= 1u << s;
-      pending &= ~(1u << s);
-    }
-    const unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
-    const int rows = (int)min((int64_t)sp->tile_rows, sp->n - tile * sp->tile_rows);
-    fold_tile<KEYED, NULLABLE>(*sp, stage, rows, skeys, wstage);
-    __syncthreads();  // every thread is done with this stage
-    valid &= ~(1u << s);
-    int32_t ni;
-    int64_t nt;
-    if (next_tile(&ni, &nt)) {
-      if (s) {
-        q_inst[1] = ni;
-        q_tile[1] = nt;
-      } else {
-        q_inst[0] = ni;
-        q_tile[0] = nt;
-      }
-      valid |= 1u << s;
-      if (issue(s, ni, nt)) pending |= 1u << s;
-    }
-  }
-  if (failed) {
-    for (int s = 0; s < 2; s++)
-      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
-    return;
-  }
-  __syncthreads();
-  if (active >= 0) flush_smem_table(*sp, skeys);
+  batch_fold_body<GenericFolder<KEYED, NULLABLE>>(bp);
 }
 
 __global__ void gb_batch_finalize_kernel(BatchFinParams b) {
@@ -217,11 +84,14 @@ __global__ void gb_batch_finalize_kernel(BatchFinParams b) {
   }
 }
 
-using FoldFn = void (*)(BatchParams);
+const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch);
+std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch);
 
-static FoldFn fold_fn(bool keyed, bool nullable) {
-  return keyed ? (nullable ? gb_batch_fold_kernel<true, true> : gb_batch_fold_kernel<true, false>)
-               : (nullable ? gb_batch_fold_kernel<false, true> : gb_batch_fold_kernel<false, false>);
+static const void* fold_fn(bool keyed, bool nullable) {
+  return keyed ? (nullable ? (const void*)gb_batch_fold_kernel<true, true>
+                           : (const void*)gb_batch_fold_kernel<true, false>)
+               : (nullable ? (const void*)gb_batch_fold_kernel<false, true>
+                           : (const void*)gb_batch_fold_kernel<false, false>);
 }
 
 // Device image of a batch: params, chunk list, finalize offsets, counters and
@@ -231,7 +101,7 @@ struct BatchImage {
   size_t bytes = 0;
   BatchParams bp{};
   BatchFinParams bf{};
-  FoldFn fold = nullptr;
+  const void* fold = nullptr;   // the fold kernel (specialised or generic)
   int threads = kGbThreads;
   int grid = 1;
   int fgrid = 1;
@@ -246,7 +116,7 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 // chunk list.
 static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<FinParams>& fs,
                            const std::vector<int64_t>& chunk_tiles, const std::vector<int32_t>& order,
-                           bool keyed, bool nullable, int threads, size_t smem_fold, int table_words,
+                           const void* fold, int threads, size_t smem_fold, int table_words,
                            cudaStream_t stream, BatchImage* im) {
   const int ninst = (int)ps.size();
   std::vector<BatchChunk> chunks;
@@ -309,7 +179,7 @@ static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<
   im->bf.ninst = ninst;
   im->bf.done = ctr + 1;
   im->bf.claim = ctr;
-  im->fold = fold_fn(keyed, nullable);
+  im->fold = fold;
   im->threads = threads;
   im->smem = smem_fold;
   if (int32_t ast = ensure_dyn_smem(ctx, (const void*)im->fold, smem_fold)) return ast;
@@ -324,7 +194,9 @@ static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<
 
 static int32_t image_launch(ghb_ctx* ctx, const BatchImage& im, cudaStream_t stream) {
   if (im.bp.nchunks > 0) {
-    im.fold<<<im.grid, im.threads, im.smem, stream>>>(im.bp);
+    BatchParams bp = im.bp;
+    void* args[] = {&bp};
+    GHB_CUDA_TRY(ctx, cudaLaunchKernel(im.fold, dim3(im.grid), dim3(im.threads), args, im.smem, stream));
     GHB_LAUNCH_CHECK(ctx);
   }
   gb_batch_finalize_kernel<<<im.fgrid, 256, 0, stream>>>(im.bf);
@@ -469,9 +341,18 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
   std::vector<int32_t> order(ninst);
   for (int i = 0; i < ninst; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+  // one kernel specialised for the batch's signature when every instance has
+  // the same one (predicate shape, NULL modes), else the generic kernel
+  const void* fn = nullptr;
+  {
+    const std::string s0 = jit_groupby_source(ps[0], sig.nkeys == 1, true);
+    bool same = true;
+    for (int i = 1; i < ninst && same; i++) same = jit_groupby_source(ps[i], sig.nkeys == 1, true) == s0;
+    if (same) fn = jit_groupby_kernel(ps[0], sig.nkeys == 1, true);
+    if (!fn) fn = fold_fn(sig.nkeys == 1, sig.nullable);
+  }
   int per_sm = 1;
-  FoldFn fn = fold_fn(sig.nkeys == 1, sig.nullable);
-  if (int32_t ast = ensure_dyn_smem(ctx, (const void*)fn, batch_smem(smem_fold))) return ast;
+  if (int32_t ast = ensure_dyn_smem(ctx, fn, batch_smem(smem_fold))) return ast;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs.threads, batch_smem(smem_fold)));
   per_sm = std::max(1, per_sm);
   const double target = total / ((double)ctx->num_sms * per_sm * 6.0);
@@ -480,8 +361,8 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
     const double per_tile = cost[i] / (double)std::max<int64_t>(1, ps[i].ntiles);
     chunk_tiles[i] = std::max<int64_t>(1, (int64_t)(target / std::max(per_tile, 1e-9)));
   }
-  int32_t st = image_build(ctx, ps, fs, chunk_tiles, order, sig.nkeys == 1, sig.nullable, bs.threads,
-                           batch_smem(smem_fold), table_words, stream, im);
+  int32_t st = image_build(ctx, ps, fs, chunk_tiles, order, fn, bs.threads, batch_smem(smem_fold), table_words,
+                           stream, im);
   if (st) return st;
   if (ps_out) *ps_out = ps;
   return GHB_OK;

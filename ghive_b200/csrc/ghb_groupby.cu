@@ -28,77 +28,11 @@
 
 namespace ghb {
 
+const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch);
+
 template <bool KEYED, bool NULLABLE>
 __global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  // layout: [stage 0][stage 1][mbarriers][hash keys + accumulators][warp staging]
-  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)p.stage_bytes);
-  uint64_t* skeys = bars + 2;
-  uint64_t* wstage = skeys + (int64_t)(p.smem_slots + 2) * (1 + p.acc.n_acc) + (threadIdx.x >> 5) * 32;
-
-  smem_table_clear(p, skeys);
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  // stage s holds tile blockIdx.x + i * gridDim.x for the i with i % 2 == s
-  auto full = [&](int64_t tile) { return (tile + 1) * p.tile_rows <= p.n; };
-  uint32_t pending = 0, phase = 0;   // per stage s: bit s = a bulk copy is in flight / its parity
-  bool failed = false;
-  for (int s = 0; s < 2; s++) {
-    int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
-    if (tile >= p.ntiles) break;
-    if (p.bulk && full(tile)) {
-      if (threadIdx.x == 0) load_tile_bulk(p, smem_raw + s * p.stage_bytes, tile, &bars[s]);
-      pending |= 1u << s;
-    } else {
-      load_tile_plain(p, smem_raw + s * p.stage_bytes, tile);
-    }
-  }
-
-  for (int64_t it = 0;; it++) {
-    const int64_t tile = blockIdx.x + it * gridDim.x;
-    if (tile >= p.ntiles) break;
-    const int s = (int)(it & 1);
-    if ((pending >> s) & 1u) {
-      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
-      // one decision for the whole CTA: every thread leaves or none does
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
-      phase ^= 1u << s;
-      pending &= ~(1u << s);
-    }
-    const unsigned char* stage = smem_raw + s * p.stage_bytes;
-    const int rows = (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows);
-    fold_tile<KEYED, NULLABLE>(p, stage, rows, skeys, wstage);
-    __syncthreads();  // every thread is done with this stage
-    const int64_t next = tile + 2 * (int64_t)gridDim.x;
-    if (next < p.ntiles) {
-      if (p.bulk && full(next)) {
-        if (threadIdx.x == 0) {
-          fence_proxy_async_smem();
-          load_tile_bulk(p, smem_raw + s * p.stage_bytes, next, &bars[s]);
-        }
-        pending |= 1u << s;
-      } else {
-        load_tile_plain(p, smem_raw + s * p.stage_bytes, next);
-      }
-    }
-  }
-  if (failed) {
-    // a bulk copy never completed: wait (bounded) for the other stage's copy
-    // before the CTA's shared memory goes away
-    for (int s = 0; s < 2; s++)
-      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
-    return;
-  }
-  __syncthreads();
-  flush_smem_table(p, skeys);
+  fold_kernel_body<GenericFolder<KEYED, NULLABLE>>(p);
 }
 
 __global__ void gb_finalize_kernel(FinParams f) {
@@ -389,16 +323,22 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
 
   bool nullable = false;
   for (int c = 0; c < ncols; c++) nullable |= p.col_off[c] >= 0 && cols[c].null_mode != GHB_NULLS_NONE;
-  auto kfn = nkeys ? (nullable ? gb_fold_kernel<true, true> : gb_fold_kernel<true, false>)
-                   : (nullable ? gb_fold_kernel<false, true> : gb_fold_kernel<false, false>);
+  // the kernel specialised for this signature when it compiles (not for the
+  // allocation-free entry point: loading a kernel allocates), else the
+  // generic one
+  const void* kfn = fixed_table ? nullptr : jit_groupby_kernel(p, nkeys == 1, false);
+  if (!kfn)
+    kfn = nkeys ? (nullable ? (const void*)gb_fold_kernel<true, true> : (const void*)gb_fold_kernel<true, false>)
+                : (nullable ? (const void*)gb_fold_kernel<false, true> : (const void*)gb_fold_kernel<false, false>);
   const int threads = su.threads;
   int blocks_per_sm = 0;
-  if (int32_t ast = ensure_dyn_smem(ctx, (const void*)kfn, smem)) return ast;
+  if (int32_t ast = ensure_dyn_smem(ctx, kfn, smem)) return ast;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kfn, threads, smem));
   blocks_per_sm = std::max(1, blocks_per_sm);
   if (cfg && cfg->ctas_per_sm > 0) blocks_per_sm = std::min(blocks_per_sm, cfg->ctas_per_sm);
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * blocks_per_sm, p.ntiles));
-  kfn<<<grid, threads, smem, stream>>>(p);
+  void* args[] = {&p};
+  GHB_CUDA_TRY(ctx, cudaLaunchKernel(kfn, dim3(grid), dim3(threads), args, smem, stream));
   GHB_LAUNCH_CHECK(ctx);
 
   const int fthreads = 256;

@@ -24,7 +24,11 @@
 // and each bitmap word it reads.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include "ghb_ctx.hpp"
+#else
+#include "ghb_internal.cuh"
+#endif
 
 namespace ghb {
 
@@ -100,6 +104,7 @@ struct FinParams {
   int32_t* status;
 };
 
+#ifndef __CUDACC_RTC__
 // Bytes of the global table of C hashed slots and R words per record.
 inline size_t gb_table_bytes(int64_t C, int32_t R) {
   return (size_t)(C + 2) * R * 8 + 16 + (size_t)(C / 32) * 4;
@@ -118,6 +123,8 @@ inline void gb_table_bind(void* base, int64_t C, int32_t R, GbParams* p, FinPara
   f->C = C;
   f->R = R;
 }
+
+#endif
 
 // ---------------------------------------------------------------- device
 __device__ __forceinline__ double two_sum_err(double a, double b, double s) {
@@ -552,6 +559,237 @@ __device__ __forceinline__ void finalize_sides(const FinParams& f) {
 // Warp chunks of the finalize for a table of C hashed slots.
 __host__ __device__ inline int64_t fin_chunks(int64_t C) { return (C / 32 + 31) / 32; }
 
+// The generic folder: fold_tile interprets the predicate program, the key
+// and the accumulator plan for every row.
+template <bool KEYED, bool NULLABLE>
+struct GenericFolder {
+  __device__ __forceinline__ static void fold(const GbParams& p, const unsigned char* stage, int rows,
+                                              uint64_t* skeys, uint64_t* wstage) {
+    fold_tile<KEYED, NULLABLE>(p, stage, rows, skeys, wstage);
+  }
+};
+
+// Body of the single-call fold kernel: persistent CTAs stream tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ... through two shared-memory stages; Folder::fold
+// folds one tile.
+template <class Folder>
+__device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // layout: [stage 0][stage 1][mbarriers][hash keys + accumulators][warp staging]
+  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)p.stage_bytes);
+  uint64_t* skeys = bars + 2;
+  uint64_t* wstage = skeys + (int64_t)(p.smem_slots + 2) * (1 + p.acc.n_acc) + (threadIdx.x >> 5) * 32;
+
+  smem_table_clear(p, skeys);
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // stage s holds tile blockIdx.x + i * gridDim.x for the i with i % 2 == s
+  auto full = [&](int64_t tile) { return (tile + 1) * p.tile_rows <= p.n; };
+  uint32_t pending = 0, phase = 0;   // per stage s: bit s = a bulk copy is in flight / its parity
+  bool failed = false;
+  for (int s = 0; s < 2; s++) {
+    int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
+    if (tile >= p.ntiles) break;
+    if (p.bulk && full(tile)) {
+      if (threadIdx.x == 0) load_tile_bulk(p, smem_raw + s * p.stage_bytes, tile, &bars[s]);
+      pending |= 1u << s;
+    } else {
+      load_tile_plain(p, smem_raw + s * p.stage_bytes, tile);
+    }
+  }
+
+  for (int64_t it = 0;; it++) {
+    const int64_t tile = blockIdx.x + it * gridDim.x;
+    if (tile >= p.ntiles) break;
+    const int s = (int)(it & 1);
+    if ((pending >> s) & 1u) {
+      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
+      // one decision for the whole CTA: every thread leaves or none does
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      phase ^= 1u << s;
+      pending &= ~(1u << s);
+    }
+    const unsigned char* stage = smem_raw + s * p.stage_bytes;
+    const int rows = (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows);
+    Folder::fold(p, stage, rows, skeys, wstage);
+    __syncthreads();  // every thread is done with this stage
+    const int64_t next = tile + 2 * (int64_t)gridDim.x;
+    if (next < p.ntiles) {
+      if (p.bulk && full(next)) {
+        if (threadIdx.x == 0) {
+          fence_proxy_async_smem();
+          load_tile_bulk(p, smem_raw + s * p.stage_bytes, next, &bars[s]);
+        }
+        pending |= 1u << s;
+      } else {
+        load_tile_plain(p, smem_raw + s * p.stage_bytes, next);
+      }
+    }
+  }
+  if (failed) {
+    // a bulk copy never completed: wait (bounded) for the other stage's copy
+    // before the CTA's shared memory goes away
+    for (int s = 0; s < 2; s++)
+      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
+    return;
+  }
+  __syncthreads();
+  flush_smem_table(p, skeys);
+}
+
+
+struct BatchChunk {
+  int32_t inst;
+  int32_t ntiles;
+  int64_t tile0;
+};
+
+struct BatchParams {
+  const GbParams* insts;
+  const BatchChunk* chunks;
+  int64_t nchunks;
+  unsigned long long* claim;   // next chunk to hand out (reset by the finalize)
+  int32_t stage_bytes;         // the same for every instance
+  int32_t table_words;         // shared-table words reserved per CTA
+};
+
+// Body of the batched fold kernel: persistent CTAs claim chunks (a run of
+// tiles of one instance) from a global counter; a CTA keeps the current
+// instance's parameters and shared table in shared memory and flushes the
+// table when the instance changes.  Folder::fold folds one tile.
+template <class Folder>
+__device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // layout: [stage 0][stage 1][mbarriers][instance params][claim][table][warp staging]
+  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)bp.stage_bytes);
+  GbParams* sp = (GbParams*)(bars + 2);
+  long long* sclaim = (long long*)(sp + 1);
+  uint64_t* skeys = (uint64_t*)(sclaim + 2);
+  uint64_t* wstage = skeys + bp.table_words + (threadIdx.x >> 5) * 32;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // The CTA's tile stream: the tiles of the chunk it claimed last.  Every
+  // thread holds the same state, so the barriers inside are uniform.
+  int32_t c_inst = -1;
+  int64_t c_next = 0, c_end = 0;
+  bool exhausted = false;
+  auto next_tile = [&](int32_t* inst, int64_t* tile) -> bool {
+    if (c_next >= c_end) {
+      if (exhausted) return false;
+      if (threadIdx.x == 0) *sclaim = (long long)atomicAdd(bp.claim, 1ull);
+      __syncthreads();
+      const long long c = *sclaim;
+      __syncthreads();
+      if (c >= bp.nchunks) {
+        exhausted = true;
+        return false;
+      }
+      const BatchChunk ch = bp.chunks[c];
+      c_inst = ch.inst;
+      c_next = ch.tile0;
+      c_end = ch.tile0 + ch.ntiles;
+    }
+    *inst = c_inst;
+    *tile = c_next++;
+    return true;
+  };
+  // Starts loading a tile into stage s; true when it arrives by bulk copy.
+  auto issue = [&](int s, int32_t inst, int64_t tile) -> bool {
+    const GbParams& gp = bp.insts[inst];
+    unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
+    if (gp.bulk && (tile + 1) * gp.tile_rows <= gp.n) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        load_tile_bulk(gp, stage, tile, &bars[s]);
+      }
+      return true;
+    }
+    load_tile_plain(gp, stage, tile);
+    return false;
+  };
+
+  int32_t q_inst[2] = {-1, -1};
+  int64_t q_tile[2] = {0, 0};
+  uint32_t valid = 0, pending = 0, phase = 0;
+  for (int s = 0; s < 2; s++) {
+    if (!next_tile(&q_inst[s], &q_tile[s])) break;
+    valid |= 1u << s;
+    if (issue(s, q_inst[s], q_tile[s])) pending |= 1u << s;
+  }
+
+  int32_t active = -1;
+  bool failed = false;
+  for (int64_t it = 0;; it++) {
+    const int s = (int)(it & 1);
+    if (!((valid >> s) & 1u)) break;
+    const int32_t inst = s ? q_inst[1] : q_inst[0];
+    const int64_t tile = s ? q_tile[1] : q_tile[0];
+    if (inst != active) {
+      if (active >= 0) {
+        flush_smem_table(*sp, skeys);
+        __syncthreads();
+      }
+      const uint64_t* src = (const uint64_t*)&bp.insts[inst];
+      for (int k = threadIdx.x; k < (int)(sizeof(GbParams) / 8); k += blockDim.x)
+        ((uint64_t*)sp)[k] = src[k];
+      __syncthreads();
+      smem_table_clear(*sp, skeys);
+      __syncthreads();
+      active = inst;
+    }
+    if ((pending >> s) & 1u) {
+      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      phase ^= 1u << s;
+      pending &= ~(1u << s);
+    }
+    const unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
+    const int rows = (int)min((int64_t)sp->tile_rows, sp->n - tile * sp->tile_rows);
+    Folder::fold(*sp, stage, rows, skeys, wstage);
+    __syncthreads();  // every thread is done with this stage
+    valid &= ~(1u << s);
+    int32_t ni;
+    int64_t nt;
+    if (next_tile(&ni, &nt)) {
+      if (s) {
+        q_inst[1] = ni;
+        q_tile[1] = nt;
+      } else {
+        q_inst[0] = ni;
+        q_tile[0] = nt;
+      }
+      valid |= 1u << s;
+      if (issue(s, ni, nt)) pending |= 1u << s;
+    }
+  }
+  if (failed) {
+    for (int s = 0; s < 2; s++)
+      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
+    return;
+  }
+  __syncthreads();
+  if (active >= 0) flush_smem_table(*sp, skeys);
+}
+
+
+#ifndef __CUDACC_RTC__
 // ---------------------------------------------------------------- host
 struct GbSetup {
   int64_t max_groups;   // table sizing: groups expected (0 = out_capacity)
@@ -573,5 +811,7 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
                  const GbSetup& su, GbParams* p, FinParams* f, size_t* table_bytes, size_t* smem);
 
 int64_t next_pow2_i64(int64_t v);
+
+#endif
 
 }  // namespace ghb

@@ -5,10 +5,14 @@
 // decoupled look-back used by every order-preserving compaction.
 #pragma once
 
+// Also compiled at run time by NVRTC (specialised group-by kernels), which
+// has no host headers: those are included only for the offline build.
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
+#endif
 
 #include "../../include/ghive_b200.h"
 

@@ -363,6 +363,24 @@ int32_t ghb_batch_launch(ghb_batch* batch, void* stream);
 int32_t ghb_batch_describe(const ghb_batch* batch, char* buf, int64_t len);
 int32_t ghb_batch_destroy(ghb_batch* batch);
 
+/* ---- specialised group-by kernels ----------------------------------------
+ * No counterpart in the reference.  A fused filter + group-by call compiles
+ * (NVRTC, sm_100a) and caches a fold kernel specialised for its signature:
+ * the used columns' types and NULL modes, the predicate tree's shape, the key
+ * column and the aggregates; literal values stay run-time parameters.  The
+ * cache is per process and on disk ($GHB_JIT_CACHE, default
+ * ~/.cache/ghive_b200/jit); GHB_JIT=0 in the environment runs the generic
+ * kernel instead.  These two functions need no GPU: one writes the kernel
+ * source a call would compile (batch != 0: the batched fold), the other
+ * compiles a source and reports the cubin size and the compiler log, to
+ * check or pre-build kernels ahead of the first call. */
+int32_t ghb_jit_groupby_source(const ghb_predicate* pred, const ghb_column* cols,
+                               int32_t ncols, const int32_t* key_cols, int32_t nkeys,
+                               const ghb_agg_desc* aggs, int32_t naggs, int32_t batch,
+                               char* buf, int64_t len);
+int32_t ghb_jit_compile_source(const char* source, int64_t* cubin_bytes, char* log,
+                               int64_t len);
+
 /* ---- serving: concurrent operator requests ------------------------------
  * GHive's JNI entry point (GPUProcess, gpu_impl/src/ghive_JNIInterface.cu:
  * 13-340) runs one Tez task's plan alone: every call re-uploads its inputs,
