@@ -355,7 +355,8 @@ def bench_groupby(ctx, args, dev, stream, peak):
                         "AVG(price), MIN(d), MAX(d) over 6M rows",
             "rows_per_s": N_FACT / (ms / 1e3), "ms": ms, "groups": groups,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "bytes": nbytes, "l2": "flushed before each launch"}}
+                         "frac": ach / peak, "bytes": nbytes, "l2": "flushed before each launch",
+                         "traffic": profile_traffic("groupby_fold_fact6M.md")}}
 
 
 def bench_sort(ctx, args, dev, stream, peak):
