@@ -196,19 +196,36 @@ __global__ void __launch_bounds__(TH) join_count_kernel(ProbeParams p) {
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;   // every key once: a match is one output row
   const int woff = warp * (32 * kJItems) + lane;
+  // The keys of the CTA's next chunk are loaded while this chunk probes the
+  // table, so the DRAM latency of the key stream overlaps the table loads.
+  auto load_chunk_keys = [&](int64_t c, long long* raw) {
+    const int64_t cbase = c * kChunk;
+    const int left = (int)min((int64_t)kChunk, p.n - cbase);
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) {
+      const int off = woff + k * 32;
+      raw[k] = 0;
+      if (c < p.nchunks && off < left)
+        raw[k] = KEY_INT ? (long long)__ldcs((const int*)p.pkey.data + cbase + off)
+                         : __ldcs((const long long*)p.pkey.data + cbase + off);
+    }
+  };
+  long long next_raw[kJItems];
+  load_chunk_keys(blockIdx.x, next_raw);
   for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
     const int64_t cbase = c * kChunk;
     // rows of this chunk left (a full chunk unless it is the last one)
     const int left = (int)min((int64_t)kChunk, p.n - cbase);
+    long long cur_raw[kJItems];
+#pragma unroll
+    for (int k = 0; k < kJItems; k++) cur_raw[k] = next_raw[k];
+    load_chunk_keys(c + gridDim.x, next_raw);
     unsigned long long u[kJItems];
     bool valid[kJItems];
 #pragma unroll
     for (int k = 0; k < kJItems; k++) {
       const int off = woff + k * 32;
-      long long raw = 0;
-      if (off < left)
-        raw = KEY_INT ? (long long)__ldcs((const int*)p.pkey.data + cbase + off)
-                      : __ldcs((const long long*)p.pkey.data + cbase + off);
+      const long long raw = cur_raw[k];
       valid[k] = off < left && !(NULLABLE && raw_is_null(p.pkey, raw, cbase + off));
       u[k] = flip_i64(raw);
     }
@@ -298,37 +315,101 @@ __device__ __forceinline__ void put_word(const ghb_out_column& o, int64_t pos, i
   if (o.is_null) o.is_null[pos] = null ? 1 : 0;
 }
 
-// One output row: probe row `prow`, build row `brow` (-1 for an outer miss /
-// semi), with the first-row payload words `w0`, `w1` when `inl` is set.
-__device__ __forceinline__ void emit_row(const ProbeParams& p, int64_t pos, int64_t prow, int32_t brow,
-                                         bool inl, unsigned long long w0, unsigned long long w1) {
-  if (p.out_prow) __stcs(p.out_prow + pos, (int)prow);
-  if (p.out_brow) __stcs(p.out_brow + pos, brow);
-  if (p.lean) {
-    // every payload non-NULL and brow >= 0 (INNER); the first row of a key
-    // reads the slot's copy, later rows of a duplicated key the build column
-    for (int j = 0; j < p.nbp; j++) {
-      unsigned long long w = inl ? (j == 0 ? w0 : w1) : (unsigned long long)ld_raw(p.bpay[j], brow);
-      if (p.bpay[j].type == GHB_INT) __stcs((int*)p.obp[j].data + pos, (int)w);
-      else __stcs((unsigned long long*)p.obp[j].data + pos, w);
-      if (p.obp[j].is_null) p.obp[j].is_null[pos] = 0;
-    }
-    return;
+// The payload descriptors and output pointers of a probe, copied to shared
+// memory once per CTA for the general emit path below.
+struct EmitDesc {
+  ghb_column bpay[kMaxPay];
+  ghb_out_column obp[kMaxPay];
+  ghb_column ppay[kMaxPay];
+  ghb_out_column opp[kMaxPay];
+  int32_t* out_prow;
+  int32_t* out_brow;
+  int32_t nbp, npp, n_inline;
+};
+
+__device__ __forceinline__ void load_emit_desc(const ProbeParams& p, EmitDesc* d) {
+  if (threadIdx.x < kMaxPay) {
+    const int j = threadIdx.x;
+    d->bpay[j] = p.bpay[j];
+    d->obp[j] = p.obp[j];
+    d->ppay[j] = p.ppay[j];
+    d->opp[j] = p.opp[j];
   }
-  for (int j = 0; j < p.nbp; j++) {
-    const ghb_column& c = p.bpay[j];
+  if (threadIdx.x == 0) {
+    d->out_prow = p.out_prow;
+    d->out_brow = p.out_brow;
+    d->nbp = p.nbp;
+    d->npp = p.npp;
+    d->n_inline = p.n_inline;
+  }
+  __syncthreads();
+}
+
+// One output row: probe row `prow`, build row `brow` (-1 for an outer miss /
+// semi), with the first-row payload words `w0`, `w1` when `inl` is set.  Out
+// of line, reading its descriptors from shared memory: the write kernel's hot
+// path is emit_lean, and inlined copies of this general loop would crowd its
+// registers.
+__device__ __noinline__ void emit_row(const EmitDesc* d, int64_t pos, int64_t prow, int32_t brow, bool inl,
+                                      unsigned long long w0, unsigned long long w1) {
+  if (d->out_prow) __stcs(d->out_prow + pos, (int)prow);
+  if (d->out_brow) __stcs(d->out_brow + pos, brow);
+  for (int j = 0; j < d->nbp; j++) {
+    const ghb_column& c = d->bpay[j];
     if (brow < 0) {
-      put_word(p.obp[j], pos, c.type, 0, true);
+      put_word(d->obp[j], pos, c.type, 0, true);
       continue;
     }
-    int64_t raw = (inl && j < p.n_inline) ? (int64_t)(j == 0 ? w0 : w1) : ld_raw(c, brow);
+    int64_t raw = (inl && j < d->n_inline) ? (int64_t)(j == 0 ? w0 : w1) : ld_raw(c, brow);
     bool null = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, brow);
-    put_word(p.obp[j], pos, c.type, raw, null);
+    put_word(d->obp[j], pos, c.type, raw, null);
   }
-  for (int j = 0; j < p.npp; j++) {
-    const ghb_column& c = p.ppay[j];
+  for (int j = 0; j < d->npp; j++) {
+    const ghb_column& c = d->ppay[j];
     int64_t raw = ld_raw(c, prow);
-    put_word(p.opp[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, prow));
+    put_word(d->opp[j], pos, c.type, raw, c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, prow));
+  }
+}
+
+// The lean case (INNER, no probe payloads, at most two build payloads, all
+// inline and non-NULL): the output descriptors are read once into registers
+// and a row is a few stores.  Constant indices keep the descriptors in the
+// parameter space; the general emit_row loops over them with a run-time
+// index.
+struct LeanOut {
+  int32_t* prow;
+  int32_t* brow;
+  void* data[kInline];
+  uint8_t* nul[kInline];
+  bool is_int[kInline];
+  int nbp;
+};
+
+__device__ __forceinline__ LeanOut lean_out(const ProbeParams& p) {
+  LeanOut o;
+  o.prow = p.out_prow;
+  o.brow = p.out_brow;
+  o.nbp = p.nbp;
+#pragma unroll
+  for (int j = 0; j < kInline; j++) {
+    o.data[j] = p.obp[j].data;
+    o.nul[j] = p.obp[j].is_null;
+    o.is_int[j] = p.bpay[j].type == GHB_INT;
+  }
+  return o;
+}
+
+__device__ __forceinline__ void emit_lean(const LeanOut& o, int64_t pos, int64_t prow, int32_t brow,
+                                          unsigned long long w0, unsigned long long w1) {
+  if (o.prow) __stcs(o.prow + pos, (int)prow);
+  if (o.brow) __stcs(o.brow + pos, brow);
+#pragma unroll
+  for (int j = 0; j < kInline; j++) {
+    if (j >= o.nbp) break;
+    const unsigned long long w = j == 0 ? w0 : w1;
+    if (o.is_int[j]) __stcs((int*)o.data[j] + pos, (int)w);
+    else __stcs((unsigned long long*)o.data[j] + pos, w);
+    if (o.nul[j]) o.nul[j][pos] = 0;
   }
 }
 
@@ -343,13 +424,24 @@ __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
   const bool unique = p.stats[1] <= 1;
   // the row's (first row, count) is needed for duplicates and build row ids
   const bool need_meta = !unique || p.out_brow != nullptr || !p.lean;
+  const LeanOut lo = lean_out(p);
+  __shared__ EmitDesc s_desc;
+  load_emit_desc(p, &s_desc);
+  // the next chunk's slots load while this chunk gathers and writes
+  int32_t next_s[kJItems];
+#pragma unroll
+  for (int k = 0; k < kJItems; k++) {
+    const int64_t row = (int64_t)blockIdx.x * kChunk + (int64_t)warp * (32 * kJItems) + k * 32 + lane;
+    next_s[k] = row < p.n ? __ldcs(p.slot_of_row + row) : -1;
+  }
   for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
     const int64_t wbase = c * kChunk + (int64_t)warp * (32 * kJItems);
     int32_t s[kJItems];
 #pragma unroll
     for (int k = 0; k < kJItems; k++) {
-      int64_t row = wbase + k * 32 + lane;
-      s[k] = row < p.n ? __ldcs(p.slot_of_row + row) : -1;
+      s[k] = next_s[k];
+      const int64_t nrow = wbase + (int64_t)gridDim.x * kChunk + k * 32 + lane;
+      next_s[k] = nrow < p.n ? __ldcs(p.slot_of_row + nrow) : -1;
     }
     ulonglong2 w[kJItems];
     int32_t first[kJItems], cnt[kJItems];
@@ -411,14 +503,15 @@ __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
         continue;
       }
       if (s[k] < 0 || p.join_type == GHB_LEFT_SEMI_JOIN) {
-        emit_row(p, pos, row, -1, false, 0, 0);
+        emit_row(&s_desc, pos, row, -1, false, 0, 0);
         continue;
       }
-      emit_row(p, pos, row, first[k] - 1, true, p.nbp > 0 ? w[k].x : 0, p.nbp > 0 ? w[k].y : 0);
+      if (p.lean) emit_lean(lo, pos, row, first[k] - 1, p.nbp > 0 ? w[k].x : 0, p.nbp > 0 ? w[k].y : 0);
+      else emit_row(&s_desc, pos, row, first[k] - 1, true, p.nbp > 0 ? w[k].x : 0, p.nbp > 0 ? w[k].y : 0);
       if (mult[k] > 1) {
         int32_t b = p.chain_p1[s[k]] - 1;
         for (int j = 1; j < mult[k]; j++) {
-          emit_row(p, pos + j, row, b, false, 0, 0);
+          emit_row(&s_desc, pos + j, row, b, false, 0, 0);
           if (j + 1 < mult[k]) b = p.next_p1[b] - 1;
         }
       }
