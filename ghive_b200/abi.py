@@ -73,7 +73,7 @@ class AggDesc(C.Structure):
 class GroupByCfg(C.Structure):
     _fields_ = [("block_threads", C.c_int32), ("smem_slots", C.c_int32),
                 ("global_slots_log2", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("max_groups", C.c_int64)]
+                ("max_groups", C.c_int64), ("tile_rows", C.c_int32), ("nstages", C.c_int32)]
 
 
 class JoinCfg(C.Structure):

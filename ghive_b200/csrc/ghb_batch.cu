@@ -38,7 +38,7 @@ static_assert(sizeof(GbParams) % 8 == 0, "GbParams is copied to shared memory in
 
 struct BatchFinParams {
   const FinParams* fins;
-  const int64_t* choff;        // [ninst + 1]: first finalize chunk of each instance
+  const int64_t* choff;        // [ninst + 1]: first finalize unit of each instance
   int32_t ninst;
   unsigned long long* done;
   unsigned long long* claim;
@@ -49,12 +49,11 @@ __global__ void __launch_bounds__(kGbThreads) gb_batch_fold_kernel(BatchParams b
   batch_fold_body<GenericFolder<KEYED, NULLABLE>>(bp);
 }
 
-__global__ void gb_batch_finalize_kernel(BatchFinParams b) {
+__global__ void __launch_bounds__(kFinThreads) gb_batch_finalize_kernel(BatchFinParams b) {
+  __shared__ uint64_t rb[kFinThreads * (kMaxAcc + 1)];
   const int64_t total = b.choff[b.ninst];
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t ch = gw; ch < total; ch += nw) {
-    // the instance of chunk ch: the last i with choff[i] <= ch
+  for (int64_t ch = blockIdx.x; ch < total; ch += gridDim.x) {
+    // the instance of unit ch: the last i with choff[i] <= ch
     int lo = 0, hi = b.ninst - 1;
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
@@ -63,8 +62,8 @@ __global__ void gb_batch_finalize_kernel(BatchFinParams b) {
     }
     const FinParams& f = b.fins[lo];
     const int64_t local = ch - b.choff[lo];
-    finalize_chunk(f, local);
-    if (local == 0 && (threadIdx.x & 31) == 0) finalize_sides(f);
+    finalize_unit(f, local, rb);
+    if (local == 0 && threadIdx.x == 0) finalize_sides(f, rb);
   }
   __shared__ int last;
   __syncthreads();
@@ -84,8 +83,8 @@ __global__ void gb_batch_finalize_kernel(BatchFinParams b) {
   }
 }
 
-const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch);
-std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch);
+const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch, int threads);
+std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch, int threads);
 
 static const void* fold_fn(bool keyed, bool nullable) {
   return keyed ? (nullable ? (const void*)gb_batch_fold_kernel<true, true>
@@ -127,7 +126,7 @@ static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<
       chunks.push_back(BatchChunk{i, (int32_t)std::min<int64_t>(step, nt - t), t});
   }
   std::vector<int64_t> choff(ninst + 1, 0);
-  for (int i = 0; i < ninst; i++) choff[i + 1] = choff[i] + fin_chunks(ps[i].C);
+  for (int i = 0; i < ninst; i++) choff[i + 1] = choff[i] + fin_units(ps[i].C);
 
   size_t off = 0;
   const size_t o_ps = off;
@@ -188,7 +187,7 @@ static int32_t image_build(ghb_ctx* ctx, std::vector<GbParams>& ps, std::vector<
   per_sm = std::max(1, per_sm);
   im->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * per_sm,
                                                           std::max<int64_t>(1, (int64_t)chunks.size())));
-  im->fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((choff[ninst] * 32 + 255) / 256, (int64_t)ctx->num_sms * 4));
+  im->fgrid = (int)std::max<int64_t>(1, std::min<int64_t>(choff[ninst], (int64_t)ctx->num_sms * 8));
   return GHB_OK;
 }
 
@@ -199,7 +198,7 @@ static int32_t image_launch(ghb_ctx* ctx, const BatchImage& im, cudaStream_t str
     GHB_CUDA_TRY(ctx, cudaLaunchKernel(im.fold, dim3(im.grid), dim3(im.threads), args, im.smem, stream));
     GHB_LAUNCH_CHECK(ctx);
   }
-  gb_batch_finalize_kernel<<<im.fgrid, 256, 0, stream>>>(im.bf);
+  gb_batch_finalize_kernel<<<im.fgrid, kFinThreads, 0, stream>>>(im.bf);
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;
 }
@@ -268,6 +267,7 @@ static int32_t setup_inst(ghb_ctx* ctx, const InstSpec& s, int32_t ncols, const 
   su.smem_table_slots = reserve;
   su.warp_agg = -1;
   su.extra_smem = (int32_t)(sizeof(GbParams) + 16);
+  su.nstages = 2;   // the batched fold double-buffers its tiles
   return gb_setup(ctx, s.in->pred, s.in->cols, ncols, key_cols, nkeys, aggs, naggs, s.in->out,
                   s.in->out_capacity, d_count, su, p, f, tb, smem);
 }
@@ -345,10 +345,10 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
   // the same one (predicate shape, NULL modes), else the generic kernel
   const void* fn = nullptr;
   {
-    const std::string s0 = jit_groupby_source(ps[0], sig.nkeys == 1, true);
+    const std::string s0 = jit_groupby_source(ps[0], sig.nkeys == 1, true, bs.threads);
     bool same = true;
-    for (int i = 1; i < ninst && same; i++) same = jit_groupby_source(ps[i], sig.nkeys == 1, true) == s0;
-    if (same) fn = jit_groupby_kernel(ps[0], sig.nkeys == 1, true);
+    for (int i = 1; i < ninst && same; i++) same = jit_groupby_source(ps[i], sig.nkeys == 1, true, bs.threads) == s0;
+    if (same) fn = jit_groupby_kernel(ps[0], sig.nkeys == 1, true, bs.threads);
     if (!fn) fn = fold_fn(sig.nkeys == 1, sig.nullable);
   }
   int per_sm = 1;

@@ -8,7 +8,7 @@
 // none of those branches.  A signature is a type built from the templates
 // below, e.g.
 //
-//   SigFolder<true, ColT<0, GHB_INT, GHB_NULLS_NONE>,
+//   SigFolder<2, 0, true, ColT<0, GHB_INT, GHB_NULLS_NONE>,
 //             PLeaf<0, GHB_FILTER_LT, ColT<3, GHB_INT, GHB_NULLS_NONE>, false>,
 //             AccT<A_CNT_STAR, NoCol>, AccT<A_SUM_I, ColT<1, GHB_LONG, GHB_NULLS_NONE>>, ...>
 //
@@ -110,11 +110,30 @@ struct POr {
 };
 
 // ---------------------------------------------------------------- accumulators
-// One accumulator word: kind fixed, input column fixed (NoCol for COUNT(*)).
+// How an accumulator is kept in the shared table.  The global table keeps
+// every accumulator as one 64-bit word; a CTA's shared table uses the
+// narrowest form whose shared atomics are fast (a B200 SM retires about six
+// 32-bit shared atomics for each 64-bit one):
+//   R_CNT    u32 count (the kernel flushes the table before a count can wrap)
+//   R_PAIR   64-bit wrapping sum as a u32 low word and a u32 high word: the
+//            low add returns the old word, a carry out goes to the high word
+//   R_F64    double (sum, or its compensation word)
+//   R_IMG32  u32 order image of an INT value (MAX; MIN stores its complement)
+//   R_IMG64  u64 order image (MAX; MIN stores its complement)
+enum AccRep : int { R_CNT = 0, R_PAIR = 1, R_F64 = 2, R_IMG32 = 3, R_IMG64 = 4 };
+
+// One accumulator: kind fixed, input column fixed (NoCol for COUNT(*)).
 template <int KIND, class C>
 struct AccT {
   static constexpr int kind = KIND;
-  // The row's contribution (0 = none).
+  static constexpr int rep = (KIND == A_CNT_STAR || KIND == A_CNT_NN) ? R_CNT
+                             : KIND == A_SUM_I                         ? R_PAIR
+                             : (KIND == A_SUM_F || KIND == A_COMP_F)   ? R_F64
+                             : C::type == GHB_INT                      ? R_IMG32
+                                                                       : R_IMG64;
+  static constexpr int words = (rep == R_CNT || rep == R_IMG32) ? 1 : 2;   // u32 words per slot
+
+  // The row's contribution as a global-table word (0 = none).
   __device__ __forceinline__ static uint64_t contrib(const GbParams& p, const unsigned char* stage, int r) {
     if constexpr (KIND == A_CNT_STAR) {
       return 1;
@@ -130,30 +149,189 @@ struct AccT {
       else return ~order_image(C::type, v);   // A_MIN_O
     }
   }
+
+  // The row's contribution in the shared table's form (0 = none): a count,
+  // a sum, double bits, or an order image (u32 for R_IMG32, complemented for
+  // MIN).  A u32 image of 0 adds nothing to a maximum, which is what the
+  // value it stands for (INT32_MIN for MAX, INT32_MAX for MIN) would add.
+  __device__ __forceinline__ static uint64_t narrow(const GbParams& p, const unsigned char* stage, int r) {
+    if constexpr (rep == R_IMG32) {
+      const int64_t v = C::raw(p, stage, r);
+      if (C::null(p, stage, r, v)) return 0;
+      const uint32_t u = (uint32_t)(int32_t)v ^ 0x80000000u;
+      return KIND == A_MAX_O ? u : (uint32_t)~u;
+    } else {
+      return contrib(p, stage, r);
+    }
+  }
 };
 
-// Folds one tile: phase A finds each row's slot as fold_tile does, phase B
-// adds each accumulator's contribution with its kind known at compile time.
-template <bool KEYED, class KEY, class PRED, class... ACCS>
+// u32 image of an INT order value back to the global table's 64-bit image.
+__device__ __forceinline__ uint64_t img32_to_64(uint32_t u) {
+  return flip_i64((int64_t)(int32_t)(u ^ 0x80000000u));
+}
+
+template <bool B, class T, class F>
+struct TypeIf {
+  using type = T;
+};
+template <class T, class F>
+struct TypeIf<false, T, F> {
+  using type = F;
+};
+
+// Slot of a key image in the specialised folds' shared table of mask + 1
+// slots: the low bits of the image folded to 32 bits and xor-shifted, so keys
+// of a dense integer range (the common GROUP BY key) land in distinct slots,
+// and keys that differ only in high bits still spread.
+__device__ __forceinline__ int sslot(uint64_t u, int mask) {
+  uint32_t x = (uint32_t)u ^ (uint32_t)(u >> 32);
+  return (int)((x ^ (x >> 16)) & (uint32_t)mask);
+}
+
+// Find-or-insert of a non-zero key image (u32 or u64 words) in the shared
+// table by linear probing from sslot; the slot, or -1 after max_probe probes.
+template <class W>
+__device__ __forceinline__ int sinsert(W* keys, int mask, W u, int max_probe) {
+  int h = sslot((uint64_t)u, mask);
+  for (int q = 0; q < max_probe; q++) {
+    const W cur = keys[h];
+    if (cur == u) return h;
+    if (cur == 0) {
+      const W prev = atomicCAS(keys + h, (W)0, u);
+      if (prev == 0 || prev == u) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+// 64-bit wrapping add into a (low, high) pair of u32 words.
+__device__ __forceinline__ void pair_add(uint32_t* lo, uint32_t* hi, uint64_t w) {
+  const uint32_t l = (uint32_t)w;
+  uint32_t h = (uint32_t)(w >> 32);
+  if (l) {
+    const uint32_t old = atomicAdd(lo, l);
+    h += (old + l < old) ? 1u : 0u;
+  }
+  if (h) atomicAdd(hi, h);
+}
+
+// Error-free sum of (s, c) pairs across the lanes of a warp.
+__device__ __forceinline__ void warp_sum_f64(double& s, double& c) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double so = __shfl_xor_sync(0xffffffffu, s, o);
+    const double co = __shfl_xor_sync(0xffffffffu, c, o);
+    const double t = __dadd_rn(s, so);
+    c = __dadd_rn(__dadd_rn(c, co), two_sum_err(s, so, t));
+    s = t;
+  }
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, (uint64_t)__shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Folds one tile for one operator signature.  ROWS is the tile's rows per
+// thread; WAGG selects combining equal keys within a warp before the shared
+// atomics (few groups): 0 never, 1 always, 2 as p.warp_agg says (a batch whose
+// instances differ in it).  Phase A: per row,
+// predicate, key, slot (shared table, else global).  Phase B: per
+// accumulator, each shared row's contribution in its narrow form.  Phase C
+// (rare, skipped by a warp with no such row): rows whose key is not in the
+// shared table merge every accumulator into their global record.  The shared
+// table (S slots + the two side slots) is laid out as arrays: keys (u32 for an
+// INT key column, else u64), then each accumulator's words in plan order.
+template <int ROWS, int WAGG, bool KEYED, class KEY, class PRED, class... ACCS>
 struct SigFolder {
-  template <int A, class ACC>
-  __device__ __forceinline__ static void acc_pass(const GbParams& p, const unsigned char* stage, int rpt,
-                                                  const int64_t* slot, const bool* live, const bool* in_s,
-                                                  const unsigned* peers, uint64_t* sacc, int64_t sstride,
-                                                  uint64_t* wstage) {
+  static_assert(ROWS >= 1 && ROWS <= kGbRows, "rows per thread");
+  static constexpr bool kNarrow = true;
+  static constexpr bool k32 = KEYED && KEY::type == GHB_INT;
+  static constexpr int kKeyWords = k32 ? 1 : 2;
+  static constexpr int kN = sizeof...(ACCS);
+  static constexpr int kWords[kN] = {ACCS::words...};
+  static constexpr int kKinds[kN] = {ACCS::kind...};
+  static_assert(kKinds[0] == A_CNT_STAR, "accumulator 0 is COUNT(*)");
+
+  // u32 word offset of accumulator I's array, in units of the slot stride.
+  template <int I>
+  __host__ __device__ static constexpr int off() {
+    int s = kKeyWords;
+    for (int k = 0; k < I; k++) s += kWords[k];
+    return s;
+  }
+  static constexpr int kTableWords = off<kN>();   // u32 words per slot
+
+  template <int... I>
+  struct Seq {};
+  template <int N, int... I>
+  struct MakeSeq : MakeSeq<N - 1, N - 1, I...> {};
+  template <int... I>
+  struct MakeSeq<0, I...> {
+    using type = Seq<I...>;
+  };
+  using Accs = typename MakeSeq<kN>::type;
+
+  // Narrow update of shared slot s with a contribution w in the narrow form
+  // (an SUM_F update also takes the compensation word wc).
+  template <int I, class ACC>
+  __device__ __forceinline__ static void shared_merge(uint32_t* tab, int sstride, int s, uint64_t w,
+                                                      uint64_t wc) {
+    uint32_t* a = tab + off<I>() * sstride;
+    if constexpr (ACC::rep == R_CNT) {
+      if (w) atomicAdd(a + s, (uint32_t)w);
+    } else if constexpr (ACC::rep == R_PAIR) {
+      pair_add(a + s, a + sstride + s, w);
+    } else if constexpr (ACC::kind == A_SUM_F) {
+      acc_merge(A_SUM_F, (uint64_t*)a + s, sstride, w, wc);
+    } else if constexpr (ACC::rep == R_IMG32) {
+      if (w) atomicMax(a + s, (uint32_t)w);
+    } else if constexpr (ACC::rep == R_IMG64) {
+      if (w) atomicMax((unsigned long long*)a + s, (unsigned long long)w);
+    }
+  }
+
+  template <int I, class ACC>
+  __device__ __forceinline__ static void acc_pass(const GbParams& p, const unsigned char* stage, const int* slot,
+                                                  const bool* ins, const unsigned* peers, uint32_t* tab,
+                                                  int sstride, uint64_t* wstage) {
     constexpr int kind = ACC::kind;
     if constexpr (kind == A_COMP_F) {
       return;
     } else {
 #pragma unroll
-      for (int j = 0; j < kGbRows; j++) {
-        if (j >= rpt) continue;
+      for (int j = 0; j < ROWS; j++) {
         const int r = j * blockDim.x + threadIdx.x;
-        const uint64_t w = live[j] ? ACC::contrib(p, stage, r) : 0;
-        if (p.warp_agg) {
-          wstage[threadIdx.x & 31] = in_s[j] ? w : 0;
+        if constexpr (!KEYED) {
+          // every live row is in the one group: a warp reduction, one update
+          const int lane = threadIdx.x & 31;
+          uint64_t tot = 0, comp = 0;
+          if constexpr (kind == A_SUM_F) {
+            double sf = ins[j] ? __longlong_as_double(ACC::contrib(p, stage, r)) : 0.0, cf = 0.0;
+            warp_sum_f64(sf, cf);
+            tot = (uint64_t)__double_as_longlong(sf);
+            comp = (uint64_t)__double_as_longlong(cf);
+          } else if constexpr (kind == A_MAX_O || kind == A_MIN_O) {
+            tot = warp_max_u64(ins[j] ? ACC::narrow(p, stage, r) : 0);
+          } else {
+            tot = warp_sum_u64(ins[j] ? ACC::contrib(p, stage, r) : 0);
+          }
+          const unsigned any = __ballot_sync(0xffffffffu, ins[j]);
+          if (any && lane == __ffs(any) - 1) shared_merge<I, ACC>(tab, sstride, slot[j], tot, comp);
+        } else if (WAGG == 1 || (WAGG == 2 && p.warp_agg)) {
+          // lanes of one shared slot combine first; the lowest applies it
+          wstage[threadIdx.x & 31] = ins[j] ? ACC::narrow(p, stage, r) : 0;
           __syncwarp();
-          if (in_s[j] && (threadIdx.x & 31) == __ffs(peers[j]) - 1) {
+          if (ins[j] && (threadIdx.x & 31) == __ffs(peers[j]) - 1) {
             uint64_t tot = 0, comp = 0;
             double sf = 0.0, cf = 0.0;
             for (unsigned m = peers[j]; m; m &= m - 1) {
@@ -173,86 +351,192 @@ struct SigFolder {
               tot = (uint64_t)__double_as_longlong(sf);
               comp = (uint64_t)__double_as_longlong(cf);
             }
-            acc_merge(kind, sacc + A * sstride + slot[j], sstride, tot, comp);
+            shared_merge<I, ACC>(tab, sstride, slot[j], tot, comp);
           }
           __syncwarp();
-          if (live[j] && !in_s[j]) acc_merge(kind, p.grec + slot[j] * p.R + 1 + A, 1, w, 0);
-        } else if (live[j]) {
-          if (in_s[j]) acc_merge(kind, sacc + A * sstride + slot[j], sstride, w, 0);
-          else acc_merge(kind, p.grec + slot[j] * p.R + 1 + A, 1, w, 0);
+        } else {
+          if (ins[j]) shared_merge<I, ACC>(tab, sstride, slot[j], ACC::narrow(p, stage, r), 0);
         }
       }
     }
   }
 
   template <int... I>
-  struct Seq {};
-  template <int N, int... I>
-  struct MakeSeq : MakeSeq<N - 1, N - 1, I...> {};
-  template <int... I>
-  struct MakeSeq<0, I...> {
-    using type = Seq<I...>;
-  };
-
-  template <int... I>
   __device__ __forceinline__ static void all_accs(Seq<I...>, const GbParams& p, const unsigned char* stage,
-                                                  int rpt, const int64_t* slot, const bool* live,
-                                                  const bool* in_s, const unsigned* peers, uint64_t* sacc,
-                                                  int64_t sstride, uint64_t* wstage) {
-    (acc_pass<I, ACCS>(p, stage, rpt, slot, live, in_s, peers, sacc, sstride, wstage), ...);
+                                                  const int* slot, const bool* ins, const unsigned* peers,
+                                                  uint32_t* tab, int sstride, uint64_t* wstage) {
+    (acc_pass<I, ACCS>(p, stage, slot, ins, peers, tab, sstride, wstage), ...);
+  }
+
+  // Every accumulator of row r into global record g.
+  template <int... I>
+  __device__ __forceinline__ static void global_row(Seq<I...>, const GbParams& p, const unsigned char* stage,
+                                                    int r, int64_t g) {
+    uint64_t* rec = p.grec + g * p.R + 1;
+    (acc_merge(ACCS::kind, rec + I, 1, ACCS::contrib(p, stage, r), 0), ...);
+  }
+
+  using KW = typename TypeIf<k32, uint32_t, unsigned long long>::type;
+
+  // The key image of a non-NULL raw key: u32 for an INT key column (0 is
+  // INT32_MIN), else flip_i64 (0 is INT64_MIN).
+  __device__ __forceinline__ static KW image(int64_t raw) {
+    if constexpr (k32) return (uint32_t)(int32_t)raw ^ 0x80000000u;
+    else return (unsigned long long)flip_i64(raw);
   }
 
   __device__ __forceinline__ static void fold(const GbParams& p, const unsigned char* stage, int rows,
                                               uint64_t* skeys, uint64_t* wstage) {
     const int S = p.smem_slots;
-    const int64_t sstride = S + 2;
-    uint64_t* sacc = skeys + sstride;
-    const int smask_shift = S > 0 ? 64 - __ffs(S) + 1 : 0;
-    const int rpt = p.tile_rows / (int)blockDim.x;
-    int64_t slot[kGbRows];
-    bool live[kGbRows], in_s[kGbRows];
-    unsigned peers[kGbRows];
+    const int sstride = S + 2;
+    uint32_t* tab = (uint32_t*)skeys;
+    KW* keys = (KW*)skeys;
+    const int mask = S - 1;
+    int slot[ROWS];       // shared slot
+    int64_t gslot[ROWS];  // global record of a live row without a shared slot
+    bool ins[ROWS];       // live and in the shared table
+    unsigned peers[ROWS];
+    bool need[ROWS];      // live, and not found by the fast probe
+    bool any_need = false, glob = false;
+    // Phase A1: predicate, and a branch-free probe of the key's first two
+    // slots (a key already in the table is there in almost every row).
 #pragma unroll
-    for (int j = 0; j < kGbRows; j++) {
-      live[j] = in_s[j] = false;
-      slot[j] = -1;
-      peers[j] = 0;
-      if (j >= rpt) continue;
+    for (int j = 0; j < ROWS; j++) {
       const int r = j * blockDim.x + threadIdx.x;
-      bool lv = r < rows && PRED::eval(p, stage, r);
-      uint64_t u = 0;
-      int side = -1;
-      if (lv) {
+      const bool lv = r < rows && PRED::eval(p, stage, r);
+      int sl = -1;
+      bool hit = false;
+      if constexpr (KEYED) {
+        const int64_t raw = KEY::raw(p, stage, r);
+        const KW u = image(raw);
+        if (S > 0) {
+          const int h0 = sslot((uint64_t)u, mask), h1 = (h0 + 1) & mask;
+          const KW c0 = keys[h0], c1 = keys[h1];
+          hit = u != 0 && (c0 == u || c1 == u) && !KEY::null(p, stage, r, raw);
+          sl = c0 == u ? h0 : h1;
+        }
+      } else {
+        hit = S > 0;
+        sl = S + 1;   // a global aggregate: the one group
+      }
+      slot[j] = sl;
+      gslot[j] = -1;
+      ins[j] = lv && hit;
+      need[j] = lv && !hit;
+      any_need |= need[j];
+    }
+    // Phase A2 (rows the fast probe missed): NULL key, INT64_MIN, a key new
+    // to this CTA or further along its probe chain, or no room.
+    if (__any_sync(0xffffffffu, any_need)) {
+#pragma unroll
+      for (int j = 0; j < ROWS; j++) {
+        if (!need[j]) continue;
+        const int r = j * blockDim.x + threadIdx.x;
+        int sl = -1;
+        int64_t g = -1;
+        int side = -1;   // 0: key INT64_MIN, 1: NULL key / global aggregate
         if constexpr (KEYED) {
           const int64_t raw = KEY::raw(p, stage, r);
           if (KEY::null(p, stage, r, raw)) {
             side = 1;
           } else {
-            u = flip_i64(raw);
-            if (u == 0) side = 0;
+            const KW u = image(raw);
+            if (u == 0 && !k32) {
+              side = 0;
+            } else {
+              if (u != 0 && S > 0) sl = sinsert<KW>(keys, mask, u, 8);
+              if (sl < 0) g = gtable_insert(p, flip_i64(raw));   // INT32_MIN keys too
+            }
           }
         } else {
           side = 1;
         }
+        if (side >= 0) {
+          if (S > 0) sl = S + side;
+          else g = p.C + side;
+        }
+        if (sl < 0 && g < 0) raise_status(p.status, kDevCapacity);   // the row is dropped
+        slot[j] = sl;
+        gslot[j] = g;
+        ins[j] = sl >= 0;
+        glob |= g >= 0;
       }
-      int64_t ss = -1;
-      if (lv && S > 0) ss = side >= 0 ? S + side : smem_insert(skeys, S - 1, smask_shift, u, 8);
-      if (lv && ss < 0) {
-        const int64_t g = side >= 0 ? p.C + side : gtable_insert(p, u);
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; j++) {
+      peers[j] = 0;
+      if (KEYED && (WAGG == 1 || (WAGG == 2 && p.warp_agg)))
+        peers[j] = __match_any_sync(0xffffffffu, ins[j] ? slot[j] : -1);
+    }
+    all_accs(Accs{}, p, stage, slot, ins, peers, tab, sstride, wstage);
+    if (__any_sync(0xffffffffu, glob)) {
+#pragma unroll
+      for (int j = 0; j < ROWS; j++)
+        if (gslot[j] >= 0) global_row(Accs{}, p, stage, j * blockDim.x + threadIdx.x, gslot[j]);
+    }
+  }
+
+  // The shared table of p fits the words the launch reserved.
+  __device__ __forceinline__ static bool fits(const GbParams& p) {
+    return (int64_t)(p.smem_slots + 2) * kTableWords <= 2 * (int64_t)p.table_words &&
+           p.tile_rows == ROWS * (int)blockDim.x;
+  }
+
+  // Zeroes the shared table (all threads; the caller syncs after).
+  __device__ __forceinline__ static void clear(const GbParams& p, uint64_t* skeys) {
+    const int64_t words = (int64_t)(p.smem_slots + 2) * kTableWords / 2;
+    for (int64_t i = threadIdx.x; i < words; i += blockDim.x) skeys[i] = 0;
+  }
+
+  template <int I, class ACC>
+  __device__ __forceinline__ static void flush_one(const uint32_t* tab, int sstride, int s, uint64_t* rec) {
+    const uint32_t* a = tab + off<I>() * sstride;
+    if constexpr (ACC::rep == R_CNT) {
+      if (a[s]) atomicAdd((unsigned long long*)rec, (unsigned long long)a[s]);
+    } else if constexpr (ACC::rep == R_PAIR) {
+      const uint64_t v = ((uint64_t)a[sstride + s] << 32) | a[s];
+      if (v) atomicAdd((unsigned long long*)rec, (unsigned long long)v);
+    } else if constexpr (ACC::kind == A_SUM_F) {
+      acc_merge(A_SUM_F, rec, 1, ((const uint64_t*)a)[s], ((const uint64_t*)a)[sstride + s]);
+    } else if constexpr (ACC::rep == R_IMG32) {
+      // an untouched word stands for the value that leaves the extreme as it is
+      const uint64_t img = img32_to_64(ACC::kind == A_MAX_O ? a[s] : ~a[s]);
+      atomicMax((unsigned long long*)rec, (unsigned long long)(ACC::kind == A_MAX_O ? img : ~img));
+    } else if constexpr (ACC::rep == R_IMG64) {
+      const uint64_t v = ((const uint64_t*)a)[s];
+      if (v) atomicMax((unsigned long long*)rec, (unsigned long long)v);
+    }
+  }
+
+  template <int... I>
+  __device__ __forceinline__ static void flush_all(Seq<I...>, const uint32_t* tab, int sstride, int s,
+                                                   uint64_t* rec) {
+    (flush_one<I, ACCS>(tab, sstride, s, rec + I), ...);
+  }
+
+  // Merges the shared table into the global one (all threads; the caller
+  // syncs before and after).
+  __device__ __forceinline__ static void flush(const GbParams& p, const uint64_t* skeys) {
+    const int S = p.smem_slots;
+    if (S == 0) return;
+    const int sstride = S + 2;
+    const uint32_t* tab = (const uint32_t*)skeys;
+    const uint32_t* cnt = tab + off<0>() * sstride;
+    for (int s = threadIdx.x; s < sstride; s += blockDim.x) {
+      if (cnt[s] == 0) continue;
+      int64_t g;
+      if (s < S) {
+        const uint64_t u = k32 ? flip_i64((int64_t)(int32_t)(tab[s] ^ 0x80000000u)) : ((const uint64_t*)tab)[s];
+        g = gtable_insert(p, u);
         if (g < 0) {
           raise_status(p.status, kDevCapacity);
-          lv = false;
+          continue;
         }
-        slot[j] = g;
       } else {
-        slot[j] = ss;
+        g = p.C + (s - S);
       }
-      live[j] = lv;
-      in_s[j] = lv && ss >= 0;
-      if (p.warp_agg) peers[j] = __match_any_sync(0xffffffffu, in_s[j] ? ss : -1);
+      flush_all(Accs{}, tab, sstride, s, p.grec + g * p.R + 1);
     }
-    all_accs(typename MakeSeq<sizeof...(ACCS)>::type{}, p, stage, rpt, slot, live, in_s, peers, sacc, sstride,
-             wstage);
   }
 };
 

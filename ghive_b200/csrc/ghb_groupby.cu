@@ -28,19 +28,19 @@
 
 namespace ghb {
 
-const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch);
+const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch, int threads);
+bool jit_enabled();
 
 template <bool KEYED, bool NULLABLE>
 __global__ void __launch_bounds__(kGbThreads) gb_fold_kernel(GbParams p) {
   fold_kernel_body<GenericFolder<KEYED, NULLABLE>>(p);
 }
 
-__global__ void gb_finalize_kernel(FinParams f) {
-  const int64_t nch = fin_chunks(f.C);
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t ch = gw; ch < nch; ch += nw) finalize_chunk(f, ch);
-  if (blockIdx.x == 0 && threadIdx.x == 0) finalize_sides(f);
+__global__ void __launch_bounds__(kFinThreads) gb_finalize_kernel(FinParams f) {
+  __shared__ uint64_t rb[kFinThreads * (kMaxAcc + 1)];
+  const int64_t nu = fin_units(f.C);
+  for (int64_t u = blockIdx.x; u < nu; u += gridDim.x) finalize_unit(f, u, rb);
+  if (blockIdx.x == 0 && threadIdx.x == 0) finalize_sides(f, rb);
   // the last CTA to finish publishes the group count and resets the counters
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -208,27 +208,58 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   const int threads = su.threads == 512 ? 512 : kGbThreads;
   int reserve = std::max(S, su.smem_table_slots);
 
-  // tile rows: twice the block size when shared memory allows next to the table
+  // Shared memory: [stages][control][table][warp staging].  The table keeps
+  // (S + 2) slots of slot_words 32-bit words: the specialised folds' narrow
+  // layout (ghb_gb_sig.cuh: u32 keys of an INT key column, u32 counts and
+  // INT extremes, u32 pairs for integer sums) or one 64-bit word per key and
+  // accumulator.
   size_t row_bytes = 0;
   for (int c = 0; c < ncols; c++)
     if (used[c]) row_bytes += type_width(cols[c].type) + (cols[c].null_mode == GHB_NULLS_BYTEMAP ? 1 : 0);
   const size_t smem_cap = 225 * 1024 - (size_t)std::max(0, su.extra_smem);
+  int slot_words = 2 * (1 + p.acc.n_acc);
+  if (su.narrow) {
+    slot_words = (nkeys && cols[key_cols[0]].type == GHB_INT) ? 1 : 2;
+    for (int a = 0; a < p.acc.n_acc; a++) {
+      const int k = p.acc.kind[a];
+      const bool int_col = p.acc.col[a] >= 0 && cols[p.acc.col[a]].type == GHB_INT;
+      slot_words += (k == A_CNT_STAR || k == A_CNT_NN || ((k == A_MAX_O || k == A_MIN_O) && int_col)) ? 1 : 2;
+    }
+  }
   auto table_bytes_smem = [&](int s) {
-    return (size_t)(s + 2) * 8 * (1 + p.acc.n_acc) + (size_t)(threads / 32) * 32 * 8 + 64;
+    return (size_t)(s + 2) * 4 * slot_words + (size_t)(threads / 32) * 32 * 8 + kGbCtrlBytes;
   };
-  int tile_rows = su.tile_rows > 0 ? su.tile_rows : 2 * threads;
-  if (tile_rows != threads && tile_rows != 2 * threads)
-    return set_error(ctx, GHB_ERR_INVALID, "tile_rows %d: must be the block size or twice it", tile_rows);
+  auto stage_bytes_of = [&](int t) { return (row_bytes * (size_t)t + 127) & ~(size_t)127; };
+  int tile_rows = su.tile_rows > 0 ? su.tile_rows : kGbRows * threads;
+  if (tile_rows != threads && tile_rows != 2 * threads && tile_rows != 4 * threads)
+    return set_error(ctx, GHB_ERR_INVALID, "tile_rows %d: must be the block size times 1, 2 or 4", tile_rows);
+  if (su.nstages != 0 && (su.nstages < 2 || su.nstages > kGbMaxStages))
+    return set_error(ctx, GHB_ERR_INVALID, "nstages %d outside [2,%d]", su.nstages, kGbMaxStages);
   if (su.smem_slots == 0)
-    while (S > 64 && table_bytes_smem(S) + 2 * row_bytes * threads > smem_cap) S /= 2;
+    while (S > 64 && table_bytes_smem(S) + 2 * stage_bytes_of(threads) > smem_cap) S /= 2;
   reserve = std::max(S, su.smem_table_slots);
-  if (su.tile_rows == 0)
-    while (tile_rows > threads && table_bytes_smem(reserve) + 2 * row_bytes * tile_rows > smem_cap)
-      tile_rows /= 2;
-  if (table_bytes_smem(reserve) + 2 * row_bytes * tile_rows > smem_cap)
+  if (table_bytes_smem(reserve) + 2 * stage_bytes_of(threads) > smem_cap)
     return set_error(ctx, GHB_ERR_UNSUPPORTED,
                      "rows of %zu bytes and %d shared slots do not fit a shared-memory tile", row_bytes,
                      reserve);
+  // Tile: the most rows per thread whose two stages fit next to the table
+  // (rows per thread are independent work for a thread, which hides the
+  // latency of its shared-memory atomics); then stages while they fit, up to
+  // about kInflight bytes of copies in flight while one stage is folded.
+  const size_t room = smem_cap - table_bytes_smem(reserve);
+  if (su.tile_rows == 0)
+    while (tile_rows > threads && 2 * stage_bytes_of(tile_rows) > room) tile_rows /= 2;
+  const size_t sb = stage_bytes_of(tile_rows);
+  const size_t kInflight = 64 << 10;
+  int ns = su.nstages ? su.nstages : 2;
+  if (sb > 0 && !su.nstages)
+    while (ns < kGbMaxStages && (size_t)(ns + 1) * sb <= room && (size_t)(ns - 1) * sb < kInflight) ns++;
+  if ((size_t)ns * sb > room)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED,
+                     "rows of %zu bytes and %d shared slots do not fit %d stages of %d rows", row_bytes, reserve,
+                     ns, tile_rows);
+  p.nstages = ns;
+  p.table_words = (int32_t)((size_t)(reserve + 2) * slot_words / 2);
   p.smem_slots = S;
   p.warp_agg = su.warp_agg >= 0 ? su.warp_agg : ((nkeys == 0 || max_groups <= 64) ? 1 : 0);
   p.tile_rows = tile_rows;
@@ -268,7 +299,7 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   f.R = p.R;
 
   *table_bytes = gb_table_bytes(C, p.R);
-  *smem = 2 * (size_t)p.stage_bytes + table_bytes_smem(reserve);
+  *smem = (size_t)p.nstages * p.stage_bytes + table_bytes_smem(reserve);
   return GHB_OK;
 }
 
@@ -285,6 +316,8 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   su.smem_slots = cfg ? cfg->smem_slots : 0;
   su.threads = (cfg && cfg->block_threads == 512) ? 512 : kGbThreads;
   su.warp_agg = -1;
+  su.tile_rows = cfg ? cfg->tile_rows : 0;
+  su.nstages = cfg ? cfg->nstages : 0;
   if (cfg && cfg->global_slots_log2 > 0) {
     // an explicit table size: the load factor that yields it
     if (cfg->global_slots_log2 > 30)
@@ -295,9 +328,22 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   GbParams p;
   FinParams f;
   size_t table_bytes = 0, smem = 0;
+  // the kernel specialised for this signature when it compiles (not for the
+  // allocation-free entry point: loading a kernel allocates), with the narrow
+  // shared table; its u32 counters need fewer than 2^32 rows per CTA
+  int64_t n_rows = 0;
+  for (int c = 0; c < ncols; c++) n_rows = std::max<int64_t>(n_rows, cols ? cols[c].n : 0);
+  su.narrow = !fixed_table && jit_enabled() && n_rows / std::max(1, ctx->num_sms) < (1ll << 31);
   int32_t st = gb_setup(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, out_capacity,
                         d_out_groups, su, &p, &f, &table_bytes, &smem);
   if (st) return st;
+  const void* kfn = su.narrow ? jit_groupby_kernel(p, nkeys == 1, false, su.threads) : nullptr;
+  if (su.narrow && !kfn) {
+    su.narrow = 0;
+    st = gb_setup(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, out_capacity, d_out_groups, su,
+                  &p, &f, &table_bytes, &smem);
+    if (st) return st;
+  }
 
   void* table;
   if (fixed_table) {
@@ -323,10 +369,6 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
 
   bool nullable = false;
   for (int c = 0; c < ncols; c++) nullable |= p.col_off[c] >= 0 && cols[c].null_mode != GHB_NULLS_NONE;
-  // the kernel specialised for this signature when it compiles (not for the
-  // allocation-free entry point: loading a kernel allocates), else the
-  // generic one
-  const void* kfn = fixed_table ? nullptr : jit_groupby_kernel(p, nkeys == 1, false);
   if (!kfn)
     kfn = nkeys ? (nullable ? (const void*)gb_fold_kernel<true, true> : (const void*)gb_fold_kernel<true, false>)
                 : (nullable ? (const void*)gb_fold_kernel<false, true> : (const void*)gb_fold_kernel<false, false>);
@@ -341,10 +383,8 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   GHB_CUDA_TRY(ctx, cudaLaunchKernel(kfn, dim3(grid), dim3(threads), args, smem, stream));
   GHB_LAUNCH_CHECK(ctx);
 
-  const int fthreads = 256;
-  int fgrid = (int)std::min<int64_t>((fin_chunks(p.C) * 32 + fthreads - 1) / fthreads, (int64_t)ctx->num_sms * 4);
-  fgrid = std::max(fgrid, 1);
-  gb_finalize_kernel<<<fgrid, fthreads, 0, stream>>>(f);
+  const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>(fin_units(p.C), (int64_t)ctx->num_sms * 8));
+  gb_finalize_kernel<<<fgrid, kFinThreads, 0, stream>>>(f);
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;
 }

@@ -44,8 +44,10 @@ enum AccKind : int8_t {
 constexpr int kMaxAcc = 16;
 constexpr int kMaxAggs = 16;
 constexpr int kGbThreads = 1024;  // largest CTA of the fold kernels
-constexpr int kGbRows = 2;        // tile rows per thread at most
+constexpr int kGbRows = 4;        // tile rows per thread at most
 constexpr int kGbMaxSlots = 8192; // shared-memory slots per CTA at most
+constexpr int kGbMaxStages = 8;    // tile stages of the single-call fold at most
+constexpr int kGbCtrlBytes = 256;  // fold kernels' control words (mbarriers, counters) in shared memory
 
 struct AccPlan {
   int32_t n_acc;
@@ -77,14 +79,18 @@ struct GbParams {
   int32_t gprobe;        // probe limit in the global table
   int32_t* status;
   // column tiles in shared memory
-  int32_t tile_rows;     // rows per tile: the block size or twice it
+  int32_t tile_rows;     // rows per tile: the block size times 1, 2 or 4
   int32_t stage_bytes;   // bytes of one stage (128-byte multiple)
   int64_t ntiles;
   int32_t tx_bytes;      // bytes the bulk copies of one full tile deliver
   int32_t bulk;          // column bases are 16-byte aligned: full tiles arrive by bulk copy
   int32_t col_off[kMaxCols];   // byte offset of a used column's tile in a stage, -1 unused
   int32_t null_off[kMaxCols];  // byte offset of a BYTEMAP column's null bytes, -1 none
+  int32_t nstages;       // shared-memory stages of the single-call fold (2..kGbMaxStages)
+  int32_t table_words;   // 64-bit words of shared memory reserved for the shared table
 };
+
+static_assert(sizeof(GbParams) % 8 == 0, "the batched fold copies GbParams as 64-bit words");
 
 // Everything the finalize needs for one operator instance.
 struct FinParams {
@@ -477,14 +483,26 @@ __device__ __forceinline__ int64_t decode_order(int type, uint64_t img) {
 }
 
 // Writes the group of record `s` as output row `row` (when it fits) and
-// zeroes the record.
-__device__ __forceinline__ void emit_group(const FinParams& f, int64_t s, int64_t row) {
+// zeroes the record.  `rb` is this thread's row of kMaxAcc + 1 words in
+// shared memory: the record's words are all loaded (independent loads, one
+// round trip) and parked there before the outputs are computed.
+__device__ __forceinline__ void emit_group(const FinParams& f, int64_t s, int64_t row, uint64_t* rb) {
   uint64_t* rec = f.grec + s * f.R;
-  const uint64_t* acc = rec + 1;
+  uint64_t w[kMaxAcc + 1];
+#pragma unroll
+  for (int i = 0; i <= kMaxAcc; i++)
+    if (i < f.R) w[i] = rec[i];
+#pragma unroll
+  for (int i = 0; i <= kMaxAcc; i++)
+    if (i < f.R) {
+      rb[i] = w[i];
+      rec[i] = 0;
+    }
+  const uint64_t* acc = rb + 1;
   if (row < f.cap) {
     if (f.key_type >= 0) {
       bool knull = s == f.C + 1;
-      int64_t raw = s == f.C ? INT64_MIN : (int64_t)(rec[0] ^ 0x8000000000000000ull);
+      int64_t raw = s == f.C ? INT64_MIN : (int64_t)(rb[0] ^ 0x8000000000000000ull);
       write_out(f.key_out, row, knull, raw, __longlong_as_double(raw));
     }
     for (int a = 0; a < f.naggs; a++) {
@@ -520,129 +538,154 @@ __device__ __forceinline__ void emit_group(const FinParams& f, int64_t s, int64_
   } else {
     raise_status(f.status, kDevCapacity);
   }
-  for (int w = 0; w < f.R; w++) rec[w] = 0;
 }
 
-// Called by all 32 lanes of a warp for bitmap words chunk*32 + lane: emits
-// the claimed slots of those words (one atomic per warp hands out their
-// output rows) and clears the words.
-__device__ __forceinline__ void finalize_chunk(const FinParams& f, int64_t chunk) {
+// Slots per finalize unit: one CTA of kFinThreads threads, a thread per slot.
+constexpr int kFinThreads = 256;
+__host__ __device__ inline int64_t fin_units(int64_t C) { return (C + kFinThreads - 1) / kFinThreads; }
+
+// Called by all kFinThreads threads of a CTA for unit `unit` of the table:
+// each warp covers one bitmap word, takes one block of output rows for the
+// word's claimed slots (ballot + one atomic), clears the word, and each lane
+// with a claimed slot emits its group.  `rb` is the CTA's record buffer,
+// [kFinThreads][kMaxAcc + 1] words.
+__device__ __forceinline__ void finalize_unit(const FinParams& f, int64_t unit, uint64_t* rb) {
+  const int64_t s = unit * kFinThreads + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const int64_t w = chunk * 32 + lane;
-  uint32_t bits = w < f.C / 32 ? f.gbits[w] : 0u;
-  const int c = __popc(bits);
-  int incl = c;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const uint32_t word = s < f.C ? f.gbits[s >> 5] : 0u;   // the same word for the whole warp
+  const bool has = (word >> lane) & 1u;
+  const unsigned m = __ballot_sync(0xffffffffu, has);
   unsigned long long base = 0;
-  if (lane == 31 && total) base = atomicAdd(f.growc, (unsigned long long)total);
-  base = __shfl_sync(0xffffffffu, base, 31);
-  int64_t row = (int64_t)base + incl - c;
-  if (bits) f.gbits[w] = 0;
-  for (; bits; bits &= bits - 1) emit_group(f, w * 32 + __ffs(bits) - 1, row++);
+  if (lane == 0 && m) {
+    base = atomicAdd(f.growc, (unsigned long long)__popc(m));
+    f.gbits[s >> 5] = 0;
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (has) emit_group(f, s, (int64_t)base + __popc(m & ((1u << lane) - 1u)), rb + threadIdx.x * (kMaxAcc + 1));
 }
 
 // One thread: the two side records (key INT64_MIN, NULL key); a global
 // aggregate always emits its one group.
-__device__ __forceinline__ void finalize_sides(const FinParams& f) {
+__device__ __forceinline__ void finalize_sides(const FinParams& f, uint64_t* rb) {
   for (int k = 0; k < 2; k++) {
     const int64_t s = f.C + k;
     const bool emit = f.key_type < 0 ? k == 1 : f.grec[s * f.R + 1] != 0;
-    if (emit) emit_group(f, s, (int64_t)atomicAdd(f.growc, 1ull));
+    if (emit) emit_group(f, s, (int64_t)atomicAdd(f.growc, 1ull), rb);
   }
 }
-
-// Warp chunks of the finalize for a table of C hashed slots.
-__host__ __device__ inline int64_t fin_chunks(int64_t C) { return (C / 32 + 31) / 32; }
 
 // The generic folder: fold_tile interprets the predicate program, the key
 // and the accumulator plan for every row.
 template <bool KEYED, bool NULLABLE>
 struct GenericFolder {
+  static constexpr bool kNarrow = false;   // 64-bit shared counters: no flush guard
   __device__ __forceinline__ static void fold(const GbParams& p, const unsigned char* stage, int rows,
                                               uint64_t* skeys, uint64_t* wstage) {
     fold_tile<KEYED, NULLABLE>(p, stage, rows, skeys, wstage);
   }
+  // The shared table of p fits the words the launch reserved.
+  __device__ __forceinline__ static bool fits(const GbParams& p) {
+    return (int64_t)(p.smem_slots + 2) * (1 + p.acc.n_acc) <= p.table_words;
+  }
+  __device__ __forceinline__ static void clear(const GbParams& p, uint64_t* skeys) { smem_table_clear(p, skeys); }
+  __device__ __forceinline__ static void flush(const GbParams& p, const uint64_t* skeys) {
+    flush_smem_table(p, skeys);
+  }
 };
 
-// Body of the single-call fold kernel: persistent CTAs stream tiles blockIdx.x,
-// blockIdx.x + gridDim.x, ... through two shared-memory stages; Folder::fold
-// folds one tile.
+// A folder whose shared counters are 32-bit (kNarrow) has its table flushed
+// and cleared before the rows folded since the last clear could reach 2^32.
+constexpr uint64_t kNarrowRowLimit = 0xFFFFFFFFull;
+
+// Body of the single-call fold kernel.  A persistent CTA owns tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...; full tiles stream through
+// p.nstages shared-memory stages by bulk copies (cp.async.bulk completing on
+// the stage's mbarrier), so up to nstages - 1 tiles are in flight while one
+// is folded.  There is no CTA-wide barrier per tile: each warp folds its rows
+// of a stage as soon as the stage is full and moves on; the last warp to
+// finish a stage issues the copy of the stage's next tile.  A partial last
+// tile, or every tile when a column is not 16-byte aligned, is read with plain
+// loads after the pipeline.  Folder::fold folds one tile.
 template <class Folder>
 __device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  // layout: [stage 0][stage 1][mbarriers][hash keys + accumulators][warp staging]
-  uint64_t* bars = (uint64_t*)(smem_raw + 2 * (size_t)p.stage_bytes);
-  uint64_t* skeys = bars + 2;
-  uint64_t* wstage = skeys + (int64_t)(p.smem_slots + 2) * (1 + p.acc.n_acc) + (threadIdx.x >> 5) * 32;
+  // layout: [nstages stages][control][shared table][warp staging]
+  const int NS = p.nstages;
+  unsigned char* ctrl = smem_raw + (size_t)NS * p.stage_bytes;
+  uint64_t* full = (uint64_t*)ctrl;                    // [kGbMaxStages] stage s holds a tile
+  uint32_t* done = (uint32_t*)(ctrl + 64);             // [kGbMaxStages] warps done with stage s
+  uint32_t* issued = (uint32_t*)(ctrl + 96);           // [kGbMaxStages] copies issued into stage s
+  int32_t* gave_up = (int32_t*)(ctrl + 128);           // a wait ran out
+  uint64_t* skeys = (uint64_t*)(ctrl + kGbCtrlBytes);
+  uint64_t* wstage = skeys + p.table_words + (threadIdx.x >> 5) * 32;
+  if (!Folder::fits(p) || NS < 2 || NS > kGbMaxStages) {   // a layout the host did not reserve
+    if (threadIdx.x == 0) raise_status(p.status, GHB_ERR_INVALID);
+    return;
+  }
 
-  smem_table_clear(p, skeys);
+  Folder::clear(p, skeys);
+  if (threadIdx.x < kGbMaxStages) {
+    done[threadIdx.x] = 0;
+    issued[threadIdx.x] = 0;
+  }
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int s = 0; s < NS; s++) mbar_init(&full[s], 1);
+    *gave_up = 0;
     mbar_fence_init();
   }
   __syncthreads();
 
-  // stage s holds tile blockIdx.x + i * gridDim.x for the i with i % 2 == s
-  auto full = [&](int64_t tile) { return (tile + 1) * p.tile_rows <= p.n; };
-  uint32_t pending = 0, phase = 0;   // per stage s: bit s = a bulk copy is in flight / its parity
-  bool failed = false;
-  for (int s = 0; s < 2; s++) {
-    int64_t tile = blockIdx.x + (int64_t)s * gridDim.x;
-    if (tile >= p.ntiles) break;
-    if (p.bulk && full(tile)) {
-      if (threadIdx.x == 0) load_tile_bulk(p, smem_raw + s * p.stage_bytes, tile, &bars[s]);
-      pending |= 1u << s;
-    } else {
-      load_tile_plain(p, smem_raw + s * p.stage_bytes, tile);
-    }
-  }
+  auto stage = [&](int s) { return smem_raw + (size_t)s * p.stage_bytes; };
+  auto tile_of = [&](int64_t i) { return (int64_t)blockIdx.x + i * (int64_t)gridDim.x; };
+  const int64_t mine = p.ntiles > (int64_t)blockIdx.x ? (p.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  int64_t nfull = p.bulk ? mine : 0;
+  if (nfull > 0 && tile_of(nfull - 1) == p.ntiles - 1 && p.n % p.tile_rows != 0) nfull--;
 
-  for (int64_t it = 0;; it++) {
-    const int64_t tile = blockIdx.x + it * gridDim.x;
-    if (tile >= p.ntiles) break;
-    const int s = (int)(it & 1);
-    if ((pending >> s) & 1u) {
-      bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
-      // one decision for the whole CTA: every thread leaves or none does
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
-      phase ^= 1u << s;
-      pending &= ~(1u << s);
+  if (threadIdx.x == 0)
+    for (int s = 0; s < NS && s < nfull; s++) {
+      load_tile_bulk(p, stage(s), tile_of(s), &full[s]);
+      issued[s] = 1;
     }
-    const unsigned char* stage = smem_raw + s * p.stage_bytes;
-    const int rows = (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows);
-    Folder::fold(p, stage, rows, skeys, wstage);
-    __syncthreads();  // every thread is done with this stage
-    const int64_t next = tile + 2 * (int64_t)gridDim.x;
-    if (next < p.ntiles) {
-      if (p.bulk && full(next)) {
-        if (threadIdx.x == 0) {
-          fence_proxy_async_smem();
-          load_tile_bulk(p, smem_raw + s * p.stage_bytes, next, &bars[s]);
-        }
-        pending |= 1u << s;
-      } else {
-        load_tile_plain(p, smem_raw + s * p.stage_bytes, next);
+
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = blockDim.x >> 5;
+  int s = 0;          // stage of tile i: i % NS
+  uint32_t par = 0;   // parity of its fill: (i / NS) & 1
+  for (int64_t i = 0; i < nfull; i++, s = s + 1 == NS ? 0 : s + 1, par ^= s == 0 ? 1u : 0u) {
+    bool ok = !__any_sync(0xffffffffu, *(volatile int32_t*)gave_up != 0);
+    if (ok) ok = __all_sync(0xffffffffu, mbar_wait(&full[s], par, p.status));
+    if (!ok) {
+      if (lane == 0) atomicExch(gave_up, 1);
+      break;
+    }
+    Folder::fold(p, stage(s), p.tile_rows, skeys, wstage);
+    __syncwarp();
+    __threadfence_block();   // this warp's reads of the stage come before its "done"
+    if (lane == 0 && atomicAdd(&done[s], 1u) == nwarps - 1) {
+      // every warp is done with stage s: refill it
+      atomicExch(&done[s], 0u);
+      if (i + NS < nfull && *(volatile int32_t*)gave_up == 0) {
+        fence_proxy_async_smem();
+        load_tile_bulk(p, stage(s), tile_of(i + NS), &full[s]);
+        issued[s]++;
       }
     }
-  }
-  if (failed) {
-    // a bulk copy never completed: wait (bounded) for the other stage's copy
-    // before the CTA's shared memory goes away
-    for (int s = 0; s < 2; s++)
-      if ((pending >> s) & 1u) mbar_wait(&bars[s], (phase >> s) & 1u, p.status);
-    return;
   }
   __syncthreads();
-  flush_smem_table(p, skeys);
+  if (*(volatile int32_t*)gave_up) {
+    // wait (bounded) for the copies in flight before the CTA's shared memory goes away
+    if (threadIdx.x == 0)
+      for (int s = 0; s < NS; s++)
+        if (issued[s]) mbar_wait(&full[s], (issued[s] - 1) & 1u, p.status);
+    return;
+  }
+  for (int64_t i = nfull; i < mine; i++) {
+    const int64_t tile = tile_of(i);
+    load_tile_plain(p, stage(0), tile);
+    Folder::fold(p, stage(0), (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows), skeys, wstage);
+    __syncthreads();
+  }
+  Folder::flush(p, skeys);
 }
 
 
@@ -733,6 +776,7 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
 
   int32_t active = -1;
   bool failed = false;
+  uint64_t since = 0;   // rows of `active` folded since its shared table was last cleared
   for (int64_t it = 0;; it++) {
     const int s = (int)(it & 1);
     if (!((valid >> s) & 1u)) break;
@@ -740,16 +784,17 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     const int64_t tile = s ? q_tile[1] : q_tile[0];
     if (inst != active) {
       if (active >= 0) {
-        flush_smem_table(*sp, skeys);
+        Folder::flush(*sp, skeys);
         __syncthreads();
       }
       const uint64_t* src = (const uint64_t*)&bp.insts[inst];
       for (int k = threadIdx.x; k < (int)(sizeof(GbParams) / 8); k += blockDim.x)
         ((uint64_t*)sp)[k] = src[k];
       __syncthreads();
-      smem_table_clear(*sp, skeys);
+      Folder::clear(*sp, skeys);
       __syncthreads();
       active = inst;
+      since = 0;
     }
     if ((pending >> s) & 1u) {
       bool ok = mbar_wait(&bars[s], (phase >> s) & 1u, sp->status);
@@ -764,6 +809,16 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     const int rows = (int)min((int64_t)sp->tile_rows, sp->n - tile * sp->tile_rows);
     Folder::fold(*sp, stage, rows, skeys, wstage);
     __syncthreads();  // every thread is done with this stage
+    if constexpr (Folder::kNarrow) {
+      since += (uint64_t)rows;
+      if (since + (uint64_t)sp->tile_rows > kNarrowRowLimit) {
+        Folder::flush(*sp, skeys);
+        __syncthreads();
+        Folder::clear(*sp, skeys);
+        __syncthreads();
+        since = 0;
+      }
+    }
     valid &= ~(1u << s);
     int32_t ni;
     int64_t nt;
@@ -785,7 +840,7 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     return;
   }
   __syncthreads();
-  if (active >= 0) flush_smem_table(*sp, skeys);
+  if (active >= 0) Folder::flush(*sp, skeys);
 }
 
 
@@ -796,10 +851,12 @@ struct GbSetup {
   int32_t smem_slots;   // -1 none, 0 auto, else power of two
   float load_factor;    // hashed slots = next_pow2(groups / load_factor); 0 = 0.5
   int32_t threads;      // CTA size of the fold (512 or 1024)
-  int32_t tile_rows;    // 0 = as large as shared memory allows (threads or 2 * threads)
+  int32_t tile_rows;    // 0 = as large as shared memory allows (threads times 1, 2 or 4)
   int32_t smem_table_slots; // shared-memory slots the layout reserves (0 = smem_slots)
   int32_t warp_agg;     // -1 auto, else 0 / 1
   int32_t extra_smem;   // shared bytes the kernel needs beyond stages, table and staging
+  int32_t narrow;       // 1: shared table in the specialised folds' narrow layout
+  int32_t nstages;      // tile stages; 0 = as many as useful (single call), the batch uses 2
 };
 
 // Validates one instance and fills p and f, except the table pointers (see

@@ -201,11 +201,37 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity` of `bar`; false (and GHB_ERR_TIMEOUT raised)
-// when it did not complete within kSpinLimit polls.
+// As mbar_try_wait, but a thread whose phase is not complete is suspended
+// until it completes or about kWaitHintNs pass, instead of returning at once:
+// a waiting warp then issues nothing while the copy is in flight.
+constexpr uint32_t kWaitHintNs = 20000;
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kWaitHintNs)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for phase `parity` of `bar`: false (and GHB_ERR_TIMEOUT raised)
+// when it did not complete within about one second (or kSpinLimit * 16 polls,
+// whichever ends first).
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* dev_status) {
-  for (int i = 0; i < kSpinLimit; i++)
-    if (mbar_try_wait(bar, parity)) return true;
+  if (mbar_try_wait_hint(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (int i = 0; i < kSpinLimit * 16; i++) {
+    if (mbar_try_wait_hint(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > kWaitLimitNs) break;
+  }
   raise_status(dev_status, kDevTimeout);
   return false;
 }

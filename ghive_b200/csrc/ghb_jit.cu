@@ -111,11 +111,13 @@ bool jit_enabled() {
   return !(e && e[0] == '0');
 }
 
-// The kernel source for a signature: `batch` selects the batched fold.
-std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch) {
+// The kernel source for a signature: `batch` selects the batched fold,
+// `threads` is the CTA size (with p.tile_rows it fixes the rows per thread).
+std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch, int threads) {
   std::ostringstream o;
   o << "#include \"ghb_gb_sig.cuh\"\n";
-  o << "using Sig = ghb::SigFolder<" << (keyed ? "true" : "false") << ", "
+  o << "using Sig = ghb::SigFolder<" << p.tile_rows / std::max(1, threads) << ", "
+    << (!keyed ? 0 : batch ? 2 : p.warp_agg ? 1 : 0) << ", " << (keyed ? "true" : "false") << ", "
     << (keyed ? col_t(p, p.key_col) : std::string("ghb::NoCol")) << ", "
     << (p.pred.n_nodes ? pred_t(p, p.pred.n_nodes - 1) : std::string("ghb::PTrue"));
   for (int a = 0; a < p.acc.n_acc; a++)
@@ -173,14 +175,16 @@ bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* 
 
 // The specialised fold kernel for a signature on the current device, or
 // nullptr (then the caller runs the generic kernel).  Compiles on first use.
-const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch) {
+const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch, int threads) {
   if (!jit_enabled()) return nullptr;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
-  const std::string src = jit_groupby_source(p, keyed, batch);
+  if (threads <= 0 || p.tile_rows % threads || p.tile_rows / threads < 1 || p.tile_rows / threads > kGbRows)
+    return nullptr;
+  const std::string src = jit_groupby_source(p, keyed, batch, threads);
   const std::string key = std::to_string(dev) + "\n" + src;
   std::lock_guard<std::mutex> g(g_mu);
   auto it = g_cache.find(key);
@@ -263,7 +267,7 @@ extern "C" int32_t ghb_jit_groupby_source(const ghb_predicate* pred, const ghb_c
   int32_t st = gb_setup(&local, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, 1 << 20, &d_groups, su, &p,
                         &f, &tb, &smem);
   if (st) return st;
-  const std::string s = jit_groupby_source(p, nkeys == 1, batch != 0);
+  const std::string s = jit_groupby_source(p, nkeys == 1, batch != 0, kGbThreads);
   const size_t n = std::min<size_t>((size_t)len - 1, s.size());
   std::memcpy(buf, s.data(), n);
   buf[n] = 0;

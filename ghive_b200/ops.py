@@ -263,7 +263,7 @@ class Context:
             cfg = abi.GroupByCfg()
         if max_groups:
             cfg.max_groups = max_groups
-        d_groups = torch.zeros(1, dtype=torch.int64, device=self.torch_device)
+        d_groups = torch.empty(1, dtype=torch.int64, device=self.torch_device)  # the finalize writes it
         pp, keep = _pred(pred)
         self._check(lib().ghb_filter_groupby(self.h, pp, cs.ptr, cs.n, ka, len(keys), ag, len(aggs),
                                              outs.ptr, cap, d_groups.data_ptr(), C.byref(cfg),

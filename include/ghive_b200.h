@@ -168,6 +168,10 @@ typedef struct ghb_groupby_cfg {
   int32_t global_slots_log2;  /* log2 of the global table size (0 = from max_groups) */
   int32_t ctas_per_sm;        /* persistent CTAs per SM                       */
   int64_t max_groups;         /* capacity hint = output capacity              */
+  int32_t tile_rows;          /* rows per shared-memory tile: the block size
+                                 or twice it; 0 = chosen with the stages      */
+  int32_t nstages;            /* tile stages, 2..8; 0 = enough for ~64 KB of
+                                 copies in flight                             */
 } ghb_groupby_cfg;
 
 typedef struct ghb_join_cfg {

@@ -491,3 +491,36 @@ def test_host_entry_points_match_device(ctx):
     okk, opp, _ = ctx.sort_host([d, k2], payload=[rowid])
     perm = oracle.sort_perm([d, k2])
     assert np.array_equal(opp[0][0], rowid[perm]) and np.array_equal(okk[1][0], k2[perm])
+
+
+@pytest.mark.parametrize("max_groups", [8, 1000])
+def test_groupby_narrow_shared_accumulators(ctx, max_groups):
+    """The specialised fold keeps COUNT as u32, integer SUM as a u32 pair with
+    carry, INT MIN/MAX as u32 images and INT keys as u32 images in shared
+    memory: extremes of every form, carries out of the low word, all-NULL
+    groups, with and without warp combining (few / many groups), and the
+    keyless warp reduction."""
+    g = np.random.default_rng(31)
+    n = 200_000
+    i32, i64 = np.iinfo(np.int32), np.iinfo(np.int64)
+    kv = np.array([i32.min, i32.min + 1, -1, 0, 1, i32.max - 1, i32.max], dtype=np.int32)
+    k = kv[g.integers(0, len(kv), n)] if max_groups == 8 else \
+        np.concatenate([kv, g.integers(i32.min, i32.max, n - len(kv), dtype=np.int32) % 997 - 498]).astype(np.int32)
+    iv = g.choice(np.array([i32.min, i32.max, -1, 0, 1, 12345], dtype=np.int32), n)
+    ivn = g.random(n) < 0.2
+    ivn[k == 1] = True  # an all-NULL group for the INT aggregates
+    lv = g.choice(np.array([0xFFFFFFFF, 0x100000000, -1, -0xFFFFFFFF, i64.max, i64.min, 7], dtype=np.int64), n)
+    dv = g.random(n) * 1000 - 300
+    aggs = [(abi.CNT, -1), (abi.CNT, 1), (abi.SUM, 1), (abi.MIN, 1), (abi.MAX, 1), (abi.AVG, 1),
+            (abi.SUM, 2), (abi.MIN, 2), (abi.MAX, 2), (abi.SUM, 3), (abi.AVG, 3)]
+    cols = [k, (iv, ivn), lv, dv]
+    _check_groupby(ctx, None, cols, [0], aggs, max_groups=max_groups)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_GT, 3, a=0.0), cols, [0], aggs, max_groups=max_groups)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_GT, 3, a=0.0), cols, [], aggs)
+    # INT values without NULLs: an extreme that is the only value of its group
+    only = np.array([i32.min] * 50 + [i32.max] * 50, dtype=np.int32)
+    kk = np.array([5] * 50 + [6] * 50, dtype=np.int32)
+    _check_groupby(ctx, None, [kk, only], [0], [(abi.MIN, 1), (abi.MAX, 1), (abi.SUM, 1)],
+                   max_groups=max_groups)
+    _check_groupby(ctx, None, [kk[:50], only[:50]], [], [(abi.MIN, 1), (abi.MAX, 1)])
+    _check_groupby(ctx, None, [kk[50:], only[50:]], [], [(abi.MIN, 1), (abi.MAX, 1)])
