@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kFinThreads) gb_batch_finalize_kernel(BatchFin
 }
 
 const void* jit_groupby_kernel(const GbParams& p, bool keyed, bool batch, int threads);
+bool jit_enabled();
 std::string jit_groupby_source(const GbParams& p, bool keyed, bool batch, int threads);
 
 static const void* fold_fn(bool keyed, bool nullable) {
@@ -105,6 +106,7 @@ struct BatchImage {
   int grid = 1;
   int fgrid = 1;
   size_t smem = 0;
+  bool specialised = false;   // the fold specialised for the batch's signature (else the generic one)
 };
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -256,7 +258,7 @@ static int32_t inst_slots(const InstSpec& s, int32_t nkeys, const BatchSetting& 
 
 static int32_t setup_inst(ghb_ctx* ctx, const InstSpec& s, int32_t ncols, const int32_t* key_cols,
                           int32_t nkeys, const ghb_agg_desc* aggs, int32_t naggs, int64_t* d_count,
-                          const BatchSetting& bs, int tile_rows, int reserve, GbParams* p,
+                          const BatchSetting& bs, int tile_rows, int reserve, bool narrow, GbParams* p,
                           FinParams* f, size_t* tb, size_t* smem) {
   GbSetup su{};
   su.max_groups = s.groups;
@@ -266,13 +268,14 @@ static int32_t setup_inst(ghb_ctx* ctx, const InstSpec& s, int32_t ncols, const 
   su.tile_rows = tile_rows;
   su.smem_table_slots = reserve;
   su.warp_agg = -1;
-  su.extra_smem = (int32_t)(sizeof(GbParams) + 16);
+  su.extra_smem = (int32_t)batch_extra_smem();
   su.nstages = 2;   // the batched fold double-buffers its tiles
+  su.narrow = narrow ? 1 : 0;
   return gb_setup(ctx, s.in->pred, s.in->cols, ncols, key_cols, nkeys, aggs, naggs, s.in->out,
                   s.in->out_capacity, d_count, su, p, f, tb, smem);
 }
 
-static size_t batch_smem(size_t fold_smem) { return fold_smem + sizeof(GbParams) + 16; }
+static size_t batch_smem(size_t fold_smem) { return fold_smem + batch_extra_smem(); }
 
 struct BatchSig {
   int32_t ncols;
@@ -285,49 +288,82 @@ struct BatchSig {
 };
 
 // Sets every instance up under `bs` (one stage layout and shared reservation
-// for all), orders and chunks the work and builds the device image.
+// for all) with the narrow shared table of the specialised folds or the wide
+// one of the generic fold.  Returns GHB_ERR_UNSUPPORTED (with no error set)
+// when `narrow` cannot be used.
+static int32_t setup_all(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const BatchSig& sig,
+                         const BatchSetting& bs, bool narrow, std::vector<GbParams>& ps,
+                         std::vector<FinParams>& fs, size_t* smem_fold) {
+  const int ninst = (int)spec.size();
+  int reserve = 0;
+  for (int i = 0; i < ninst; i++) {
+    size_t tb = 0, smem = 0;
+    int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
+                            sig.d_out_groups + i, bs, 0, 0, narrow, &ps[i], &fs[i], &tb, &smem);
+    if (st) return st;
+    reserve = std::max(reserve, ps[i].smem_slots);
+  }
+  // the most rows per thread whose stages fit every instance
+  for (int tile_rows = kGbRows * bs.threads;; tile_rows /= 2) {
+    bool ok = true;
+    *smem_fold = 0;
+    for (int i = 0; i < ninst && ok; i++) {
+      size_t tb = 0, smem = 0;
+      int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
+                              sig.d_out_groups + i, bs, tile_rows, reserve, narrow, &ps[i], &fs[i], &tb, &smem);
+      if (st) {
+        if (tile_rows <= bs.threads) return st;
+        ok = false;
+        ctx->last_error.clear();
+      }
+      *smem_fold = std::max(*smem_fold, smem);
+    }
+    if (ok) break;
+  }
+  for (int i = 1; i < ninst; i++) {
+    bool same = ps[i].stage_bytes == ps[0].stage_bytes && ps[i].tile_rows == ps[0].tile_rows &&
+                ps[i].acc.n_acc == ps[0].acc.n_acc && ps[i].key_col == ps[0].key_col &&
+                ps[i].table_words == ps[0].table_words;
+    for (int c = 0; c < kMaxCols; c++) same = same && ps[i].col_off[c] == ps[0].col_off[c];
+    if (!same)
+      return set_error(ctx, GHB_ERR_INVALID,
+                       "instance %d: predicate or aggregates read other columns than instance 0", i);
+  }
+  return GHB_OK;
+}
+
+// Orders and chunks the work of the batch under `bs` and builds the device
+// image: the fold specialised for the batch's signature (narrow shared
+// table) when every instance has the same signature and fewer than 2^31 rows
+// (its shared counters are 32-bit), else the generic fold.
 static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const BatchSig& sig,
                           const BatchSetting& bs, cudaStream_t stream, BatchImage* im,
                           std::vector<GbParams>* ps_out) {
   const int ninst = (int)spec.size();
   std::vector<GbParams> ps(ninst);
   std::vector<FinParams> fs(ninst);
-  int reserve = 0;
-  for (int i = 0; i < ninst; i++) {
-    size_t tb = 0, smem = 0;
-    int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
-                            sig.d_out_groups + i, bs, 0, 0, &ps[i], &fs[i], &tb, &smem);
-    if (st) return st;
-    reserve = std::max(reserve, ps[i].smem_slots);
-  }
-  int tile_rows = 2 * bs.threads;
   size_t smem_fold = 0;
-  for (int attempt = 0; attempt < 2; attempt++) {
+  const void* fn = nullptr;
+  bool specialised = false;
+  if (jit_enabled()) {
+    int32_t st = setup_all(ctx, spec, sig, bs, true, ps, fs, &smem_fold);
+    if (st) return st;
     bool ok = true;
-    smem_fold = 0;
-    for (int i = 0; i < ninst && ok; i++) {
-      size_t tb = 0, smem = 0;
-      int32_t st = setup_inst(ctx, spec[i], sig.ncols, sig.key_cols, sig.nkeys, sig.aggs, sig.naggs,
-                              sig.d_out_groups + i, bs, tile_rows, reserve, &ps[i], &fs[i], &tb, &smem);
-      if (st) {
-        if (attempt == 1) return st;
-        ok = false;
-        ctx->last_error.clear();
-      }
-      smem_fold = std::max(smem_fold, smem);
+    for (int i = 0; i < ninst && ok; i++) ok = ps[i].n < (1ll << 31);
+    if (ok) {
+      const std::string s0 = jit_groupby_source(ps[0], sig.nkeys == 1, true, bs.threads);
+      for (int i = 1; i < ninst && ok; i++) ok = jit_groupby_source(ps[i], sig.nkeys == 1, true, bs.threads) == s0;
     }
-    if (ok) break;
-    tile_rows = bs.threads;
+    if (ok) fn = jit_groupby_kernel(ps[0], sig.nkeys == 1, true, bs.threads);
+    specialised = fn != nullptr;
   }
-  for (int i = 1; i < ninst; i++) {
-    bool same = ps[i].stage_bytes == ps[0].stage_bytes && ps[i].tile_rows == ps[0].tile_rows &&
-                ps[i].acc.n_acc == ps[0].acc.n_acc && ps[i].key_col == ps[0].key_col;
-    for (int c = 0; c < kMaxCols; c++) same = same && ps[i].col_off[c] == ps[0].col_off[c];
-    if (!same)
-      return set_error(ctx, GHB_ERR_INVALID,
-                       "instance %d: predicate or aggregates read other columns than instance 0", i);
+  if (!specialised) {
+    int32_t st = setup_all(ctx, spec, sig, bs, false, ps, fs, &smem_fold);
+    if (st) return st;
+    fn = fold_fn(sig.nkeys == 1, sig.nullable);
   }
-  const int table_words = (reserve + 2) * (1 + ps[0].acc.n_acc);
+  const size_t smem = batch_smem(smem_fold);
+  const int table_words = ps[0].table_words;
 
   // chunk list: instances by size, largest first, each cut into chunks so
   // that every CTA claims several; a fixed cost per instance stands for its
@@ -341,19 +377,9 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
   std::vector<int32_t> order(ninst);
   for (int i = 0; i < ninst; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
-  // one kernel specialised for the batch's signature when every instance has
-  // the same one (predicate shape, NULL modes), else the generic kernel
-  const void* fn = nullptr;
-  {
-    const std::string s0 = jit_groupby_source(ps[0], sig.nkeys == 1, true, bs.threads);
-    bool same = true;
-    for (int i = 1; i < ninst && same; i++) same = jit_groupby_source(ps[i], sig.nkeys == 1, true, bs.threads) == s0;
-    if (same) fn = jit_groupby_kernel(ps[0], sig.nkeys == 1, true, bs.threads);
-    if (!fn) fn = fold_fn(sig.nkeys == 1, sig.nullable);
-  }
   int per_sm = 1;
-  if (int32_t ast = ensure_dyn_smem(ctx, fn, batch_smem(smem_fold))) return ast;
-  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs.threads, batch_smem(smem_fold)));
+  if (int32_t ast = ensure_dyn_smem(ctx, fn, smem)) return ast;
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs.threads, smem));
   per_sm = std::max(1, per_sm);
   const double target = total / ((double)ctx->num_sms * per_sm * 6.0);
   std::vector<int64_t> chunk_tiles(ninst);
@@ -361,9 +387,9 @@ static int32_t plan_image(ghb_ctx* ctx, const std::vector<InstSpec>& spec, const
     const double per_tile = cost[i] / (double)std::max<int64_t>(1, ps[i].ntiles);
     chunk_tiles[i] = std::max<int64_t>(1, (int64_t)(target / std::max(per_tile, 1e-9)));
   }
-  int32_t st = image_build(ctx, ps, fs, chunk_tiles, order, fn, bs.threads, batch_smem(smem_fold), table_words,
-                           stream, im);
+  int32_t st = image_build(ctx, ps, fs, chunk_tiles, order, fn, bs.threads, smem, table_words, stream, im);
   if (st) return st;
+  im->specialised = specialised;
   if (ps_out) *ps_out = ps;
   return GHB_OK;
 }
@@ -424,7 +450,7 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
   const int forced_threads =
       (cfg && (cfg->block_threads == 512 || cfg->block_threads == 1024)) ? cfg->block_threads : 0;
   const float lf = (cfg && cfg->load_factor > 0.f) ? cfg->load_factor : 0.5f;
-  BatchSetting base{forced_threads ? forced_threads : kGbThreads, 512, 0, lf};
+  BatchSetting base{forced_threads ? forced_threads : kGbThreads, 2048, 0, lf};
   if (cfg && cfg->smem_slots < 0) base.smem_cap = 0;
   if (cfg && cfg->smem_slots > 0) base.smem_cap = (int32_t)next_pow2_i64(cfg->smem_slots);
   std::vector<BatchSetting> cands{base};
@@ -432,7 +458,7 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
     cands.clear();
     for (int th : {1024, 512}) {
       if (forced_threads && th != forced_threads) continue;
-      std::vector<int> caps{0, 256, 512, 1024, 2048};
+      std::vector<int> caps{0, 512, 1024, 2048, 4096};
       if (cfg && cfg->smem_slots) caps = {base.smem_cap};
       for (int cap : caps)
         for (int skip = 0; skip < (cap > 0 && nkeys == 1 ? 2 : 1); skip++) cands.push_back({th, cap, skip, lf});
@@ -475,6 +501,7 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
                       ", \"grid\": " + std::to_string(b->im.grid) +
                       ", \"chunks\": " + std::to_string(b->im.bp.nchunks) +
                       ", \"smem_bytes\": " + std::to_string(b->im.smem) +
+                      ", \"kernel\": \"" + (b->im.specialised ? "specialised" : "generic") + "\"" +
                       ", \"autotuned\": " + (tune ? "true" : "false") + ", \"trials\": " + trials +
                       ", \"classes\": [";
   bool first = true;

@@ -444,7 +444,7 @@ struct SigFolder {
             if (u == 0 && !k32) {
               side = 0;
             } else {
-              if (u != 0 && S > 0) sl = sinsert<KW>(keys, mask, u, 8);
+              if (u != 0 && S > 0) sl = sinsert<KW>(keys, mask, u, 4);
               if (sl < 0) g = gtable_insert(p, flip_i64(raw));   // INT32_MIN keys too
             }
           }

@@ -284,7 +284,11 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   p.stage_bytes = (off + 127) & ~127;
   p.tx_bytes = off;
   p.bulk = aligned ? 1 : 0;
+  // words per global record: the key and the accumulators; a table too big
+  // for L2 pads them to 2, 4, 8, 16 or 24 words so that the atomics of one
+  // row touch one aligned 16/32/64-byte block of a DRAM line
   p.R = 1 + p.acc.n_acc;
+  if (C > (1ll << 17)) p.R = p.R <= 2 ? 2 : p.R <= 4 ? 4 : p.R <= 8 ? 8 : p.R <= 16 ? 16 : 24;
   p.C = C;
   p.gshift = 64 - log2_exact(C);
   p.gprobe = (int32_t)std::min<int64_t>(C, 1 << 20);

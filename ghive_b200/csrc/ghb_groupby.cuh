@@ -659,8 +659,11 @@ __device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
       break;
     }
     Folder::fold(p, stage(s), p.tile_rows, skeys, wstage);
+    // Every value the warp read from the stage has been consumed by the fold
+    // (in-order issue waits for a load's result at its first use), so after
+    // __syncwarp the warp's reads are complete.  No memory fence here: one
+    // would also wait for the warp's global-table atomics still in flight.
     __syncwarp();
-    __threadfence_block();   // this warp's reads of the stage come before its "done"
     if (lane == 0 && atomicAdd(&done[s], 1u) == nwarps - 1) {
       // every warp is done with stage s: refill it
       atomicExch(&done[s], 0u);
@@ -704,10 +707,17 @@ struct BatchParams {
   int32_t table_words;         // shared-table words reserved per CTA
 };
 
+// Shared bytes the batched fold adds to the single-call layout: its
+// mbarriers, the active instance's parameters and the claimed chunk.
+inline __host__ __device__ constexpr size_t batch_extra_smem() { return sizeof(GbParams) + 32; }
+
 // Body of the batched fold kernel: persistent CTAs claim chunks (a run of
 // tiles of one instance) from a global counter; a CTA keeps the current
 // instance's parameters and shared table in shared memory and flushes the
-// table when the instance changes.  Folder::fold folds one tile.
+// table when the instance changes; two stages, a CTA barrier per tile (a
+// per-warp pipeline as in the single-call fold measured slower here: the
+// batches' instance switches need the CTA barriers anyway).  Folder::fold
+// folds one tile.
 template <class Folder>
 __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

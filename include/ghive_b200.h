@@ -300,9 +300,10 @@ int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
  * device status word live in a file-scope __device__ array of
  * GHB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * exit; nothing is allocated or freed.  The table needs
- * (C + 2) * 8 * (1 + accumulator words) + 16 + C / 8 bytes, with
- * C = next_pow2(max(2 * max_groups + 1, 64)) (one accumulator word per
- * COUNT/SUM/MIN/MAX state, two per double SUM/AVG, plus COUNT(*)); a call
+ * (C + 2) * 8 * R + 16 + C / 8 bytes, with
+ * C = next_pow2(max(2 * max_groups + 1, 64)) and R = 1 + accumulator words
+ * (one accumulator word per COUNT/SUM/MIN/MAX state, two per double SUM/AVG,
+ * plus COUNT(*)), R rounded up to 2, 4, 8, 16 or 24 when C > 2^17; a call
  * that would need more than the array holds returns GHB_ERR_CAPACITY before
  * launching.  About 60,000 groups fit with the fact-table aggregates.
  * The first call on a device looks up the array's device address; make that
