@@ -545,7 +545,7 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
       return set_error(ctx, GHB_ERR_INVALID, "build payload %d has %lld rows, the key %lld", j,
                        (long long)build_payload[j].n, (long long)build_key->n);
   }
-  float lf = (cfg && cfg->load_factor > 0.f && cfg->load_factor < 0.95f) ? cfg->load_factor : 0.75f;
+  float lf = (cfg && cfg->load_factor > 0.f && cfg->load_factor < 0.95f) ? cfg->load_factor : 0.5f;
   int64_t nb = next_pow2(std::max<int64_t>(16, (int64_t)((double)build_key->n / (4.0 * lf)) + 1));
   ghb_join_table* t = new ghb_join_table();
   t->slots = nb * 4;

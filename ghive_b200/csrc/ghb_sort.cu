@@ -144,6 +144,13 @@ struct HistParams {
   int64_t n;
   int32_t npasses;
   uint32_t* hist;  // [npasses][kBins]
+  // a one-segment key: the packed keys and carried values are written here
+  // too, so every radix pass reads packed keys
+  uint64_t* keys_out;        // nullptr: not written
+  void* vals_out;
+  int32_t vals_wide;         // values are 64-bit (else 32-bit)
+  int32_t carry_rowid;       // value = row index (else the single payload's raw bits)
+  ghb_column pay_src;
 };
 
 __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
@@ -165,8 +172,15 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      if (base + u * stride >= p.n) continue;
+      const int64_t r = base + u * stride;
+      if (r >= p.n) continue;
       for (int q = 0; q < p.npasses; q++) atomicAdd(&sh[q][(k[u] >> (q * kDigitBits)) & (kBins - 1)], 1u);
+      if (p.keys_out) {
+        __stcs((unsigned long long*)p.keys_out + r, (unsigned long long)k[u]);
+        const uint64_t v = p.carry_rowid ? (uint64_t)r : (uint64_t)ld_raw(p.pay_src, r);
+        if (p.vals_wide) __stcs((unsigned long long*)p.vals_out + r, (unsigned long long)v);
+        else __stcs((unsigned int*)p.vals_out + r, (unsigned int)v);
+      }
     }
   }
   __syncthreads();
@@ -197,6 +211,11 @@ struct PassParams {
   ghb_column pay[kMaxSortPay];
   ghb_out_column out_pay[kMaxSortPay];
   int32_t* out_rowid;
+  // decoding a one-segment key, per key: value bits and shift, NULL flag
+  // shift (-1 none)
+  int8_t dec_vbits[kMaxSortKeys];
+  int8_t dec_vshift[kMaxSortKeys];
+  int8_t dec_fshift[kMaxSortKeys];
   uint32_t digit_base[kBins];  // exclusive global offset of each digit
   uint64_t* status;            // [ntiles][kBins] epoch-tagged look-back words
   uint32_t epoch;
@@ -234,18 +253,16 @@ __device__ __forceinline__ void gather_write(const PassParams& p, int64_t row, i
 }
 
 // Unpacks a one-segment key (and the carried value) to output position `pos`.
+// The key loop has constant indices (unrolled over the most keys), so the
+// per-key fields are read straight from the parameter space.
 __device__ __forceinline__ void decode_write(const PassParams& p, uint64_t k, uint64_t v, int64_t pos) {
-  for (int j = 0; j < p.K.nkeys; j++) {
+#pragma unroll
+  for (int j = 0; j < kMaxSortKeys; j++) {
+    if (j >= p.K.nkeys) break;
     const KeyField& kf = p.K.k[j];
-    uint64_t field = 0;
-    bool null = false;
-    for (int i = 0; i < p.seg.n; i++) {
-      const SubField& sf = p.seg.f[i];
-      if (sf.key != j) continue;
-      uint64_t bits = (k >> sf.shift) & (sf.bits >= 64 ? ~0ull : ((1ull << sf.bits) - 1));
-      if (sf.is_flag) null = (bits == 0) == (bool)kf.nulls_first;
-      else field = bits;
-    }
+    const int vb = p.dec_vbits[j];
+    const uint64_t field = vb == 0 ? 0 : (k >> p.dec_vshift[j]) & (vb >= 64 ? ~0ull : ((1ull << vb) - 1));
+    const bool null = p.dec_fshift[j] >= 0 && (((k >> p.dec_fshift[j]) & 1ull) == 0) == (bool)kf.nulls_first;
     uint64_t u = field + kf.umin;
     if (kf.desc) u = ~u;
     int64_t raw = kf.col.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(u) : (int64_t)(u ^ 0x8000000000000000ull);
@@ -496,20 +513,17 @@ static int32_t set_smem(ghb_ctx* ctx, size_t dyn) {
   return GHB_OK;
 }
 
+// kb / vb: key and value ping-pong buffers; packed: kb[0] / vb[0] already
+// hold the packed keys and values of a one-segment key.
 template <typename V>
 static int32_t run_passes(ghb_ctx* ctx, PassParams& pp, const std::vector<Segment>& segs,
                           const std::vector<std::vector<int>>& run, const std::vector<uint32_t>& hist,
-                          cudaStream_t stream) {
+                          uint64_t* const kb[2], void* const vbv[2], bool packed, cudaStream_t stream) {
   int32_t st;
-  const int64_t n = pp.n;
   int total = 0;
   for (auto& r : run) total += (int)r.size();
-  uint64_t* kb[2] = {nullptr, nullptr};
-  V* vb[2] = {nullptr, nullptr};
-  for (int i = 0; i < 2; i++) {
-    if ((st = scratch_alloc(ctx, (size_t)n * 8, (void**)&kb[i], stream))) return st;
-    if ((st = scratch_alloc(ctx, (size_t)n * sizeof(V), (void**)&vb[i], stream))) return st;
-  }
+  const int64_t n = pp.n;
+  V* vb[2] = {(V*)vbv[0], (V*)vbv[1]};
   const bool multi = segs.size() > 1;
   if (total == 0) {
     int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8);
@@ -536,7 +550,7 @@ static int32_t run_passes(ghb_ctx* ctx, PassParams& pp, const std::vector<Segmen
     for (size_t i = 0; i < run[s].size(); i++) {
       int q = run[s][i];
       bool last = ++done == total;
-      int src = i == 0 ? (have_perm ? kSrcPerm : kSrcCols) : kSrcPacked;
+      int src = i == 0 ? (have_perm ? kSrcPerm : packed ? kSrcPacked : kSrcCols) : kSrcPacked;
       int dst = last ? (multi ? kDstGather : kDstDecode) : kDstPacked;
       pp.shift = q * kDigitBits;
       uint32_t acc = 0;
@@ -646,7 +660,20 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   if (segs.size() > (size_t)kMaxSeg) return set_error(ctx, GHB_ERR_UNSUPPORTED, "too many key segments");
   const bool multi = segs.size() > 1;
 
-  // histograms of every segment, one read each, then one sync
+  // the value: the single payload itself, else the row index
+  const bool carry_rowid = multi || out_rowid != nullptr || npayload != 1 ||
+                           payload[0].null_mode == GHB_NULLS_BYTEMAP;
+  const bool wide = !carry_rowid && type_width(payload[0].type) == 8;
+  const size_t vw = wide ? 8 : 4;
+  uint64_t* kb[2] = {nullptr, nullptr};
+  void* vb[2] = {nullptr, nullptr};
+  for (int i = 0; i < 2; i++) {
+    if ((st = scratch_alloc(ctx, (size_t)n * 8, (void**)&kb[i], stream))) return st;
+    if ((st = scratch_alloc(ctx, (size_t)n * vw, &vb[i], stream))) return st;
+  }
+
+  // histograms of every segment, one read each, then one sync; a
+  // one-segment key is packed on the way
   GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_hist, 0, segs.size() * kMaxPasses * kBins * 4, stream));
   for (size_t s = 0; s < segs.size(); s++) {
     int np = (segs[s].bits + kDigitBits - 1) / kDigitBits;
@@ -657,6 +684,11 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     hp.n = n;
     hp.npasses = np;
     hp.hist = d_hist + s * kMaxPasses * kBins;
+    hp.keys_out = multi ? nullptr : kb[0];
+    hp.vals_out = vb[0];
+    hp.vals_wide = wide ? 1 : 0;
+    hp.carry_rowid = carry_rowid ? 1 : 0;
+    hp.pay_src = carry_rowid ? ghb_column{} : payload[0];
     sort_hist_kernel<<<std::min(grid, ctx->num_sms * 4), 256, 0, stream>>>(hp);
     GHB_LAUNCH_CHECK(ctx);
   }
@@ -674,10 +706,22 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     }
   }
 
-  // the value: the single payload itself, else the row index
-  bool carry_rowid = multi || out_rowid != nullptr || npayload != 1 ||
-                     payload[0].null_mode == GHB_NULLS_BYTEMAP;
   pp.carry_rowid = carry_rowid ? 1 : 0;
+  for (int j = 0; j < kMaxSortKeys; j++) {
+    pp.dec_vbits[j] = 0;
+    pp.dec_vshift[j] = 0;
+    pp.dec_fshift[j] = -1;
+  }
+  if (!multi)
+    for (int i = 0; i < segs[0].n; i++) {
+      const SubField& sf = segs[0].f[i];
+      if (sf.is_flag) {
+        pp.dec_fshift[sf.key] = sf.shift;
+      } else {
+        pp.dec_vbits[sf.key] = sf.bits;
+        pp.dec_vshift[sf.key] = sf.shift;
+      }
+    }
   if (!carry_rowid) pp.pay_src = payload[0];
   for (int j = 0; j < nkeys; j++) pp.out_keys[j] = out_keys[j];
   pp.npay = npayload;
@@ -690,9 +734,9 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   pp.ntiles = (n + kSortTile - 1) / kSortTile;
   pp.counters = ctx->d_counters + 2;
   pp.dev_status = ctx->d_status;
-  bool wide = !carry_rowid && type_width(payload[0].type) == 8;
-  if (wide) return run_passes<uint64_t>(ctx, pp, segs, run, hist, stream);
-  return run_passes<uint32_t>(ctx, pp, segs, run, hist, stream);
+  const bool packed = !multi;
+  if (wide) return run_passes<uint64_t>(ctx, pp, segs, run, hist, kb, vb, packed, stream);
+  return run_passes<uint32_t>(ctx, pp, segs, run, hist, kb, vb, packed, stream);
 }
 
 }  // namespace ghb
