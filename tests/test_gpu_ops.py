@@ -524,3 +524,33 @@ def test_groupby_narrow_shared_accumulators(ctx, max_groups):
                    max_groups=max_groups)
     _check_groupby(ctx, None, [kk[:50], only[:50]], [], [(abi.MIN, 1), (abi.MAX, 1)])
     _check_groupby(ctx, None, [kk[50:], only[50:]], [], [(abi.MIN, 1), (abi.MAX, 1)])
+
+
+@pytest.mark.parametrize("dense", [True, False])
+def test_join_direct_and_hashed_tables(ctx, dense):
+    """Dense build keys (a range at most twice the rows) get a direct table
+    (slot = key - min); sparse keys the hashed one.  Both with duplicates,
+    every join type, INT and LONG keys, probe keys outside the range."""
+    g = np.random.default_rng(24 + int(dense))
+    n, m = 50_000, 200_000
+    if dense:
+        bkey = g.permutation(np.arange(-1000, -1000 + n, dtype=np.int64))
+        pkey = g.integers(-3000, n + 2000, m, dtype=np.int64)
+    else:
+        bkey = g.integers(-(1 << 62), 1 << 62, n, dtype=np.int64)
+        hit = bkey[g.integers(0, n, m)]
+        pkey = np.where(g.random(m) < 0.7, hit, g.integers(-(1 << 62), 1 << 62, m, dtype=np.int64))
+    bkey[:500] = bkey[500:1000]  # keys twice in the build
+    pay = [g.integers(0, 1 << 40, n, dtype=np.int64), g.random(n)]
+    for jt in (abi.INNER_JOIN, abi.LEFT_SEMI_JOIN, abi.LEFT_OUTER_JOIN):
+        _check_join(ctx, bkey, pkey, jt, bpay=pay if jt != abi.LEFT_SEMI_JOIN else ())
+    t = ctx.join_build(dev(bkey))
+    rows, dup, slots = t.info()
+    assert rows == n and dup == 2
+    if dense:
+        assert slots == int(bkey.max() - bkey.min() + 1)
+    else:
+        assert slots & (slots - 1) == 0
+    t.free()
+    if dense:  # INT keys
+        _check_join(ctx, bkey.astype(np.int32), pkey.astype(np.int32), bpay=pay)
