@@ -225,8 +225,9 @@ __device__ __forceinline__ int find_in(const unsigned long long k[4], unsigned l
 
 // TH threads x IT rows per thread = one chunk (kChunk rows) per iteration.
 // DIRECT: the table is direct (slot = key - dmin); else hashed buckets.
+// Four 256-thread CTAs per SM (64 registers): more key and table loads in flight.
 template <int TH, int IT, bool KEY_INT, bool NULLABLE, bool DIRECT>
-__global__ void __launch_bounds__(TH) join_count_kernel(ProbeParams p) {
+__global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
   __shared__ uint64_t s_warp[kJThreads / 32];
@@ -332,6 +333,60 @@ __global__ void __launch_bounds__(TH) join_count_kernel(ProbeParams p) {
     }
     __syncthreads();
   }
+}
+
+// Chunk counts -> exclusive offsets in place, many CTAs: each claims a tile
+// of 1024 counts in order, scans it, and gets the tile's offset from the tiles
+// before it by decoupled look-back; the last tile writes the total.
+struct ScanParams {
+  int64_t* counts;
+  int64_t n;
+  int64_t ntiles;
+  int64_t* d_total;
+  uint64_t* lb;
+  uint32_t epoch;
+  unsigned long long* counters;
+  int32_t* status;
+};
+
+__global__ void __launch_bounds__(1024) join_scan_lb_kernel(ScanParams p) {
+  __shared__ int64_t s_tile;
+  __shared__ int64_t s_warp[32];
+  __shared__ uint64_t s_excl;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  while (true) {
+    claim_tile(&p.counters[0], &s_tile);
+    const int64_t tile = s_tile;
+    if (tile >= p.ntiles) break;
+    const int64_t i = tile * 1024 + threadIdx.x;
+    const int64_t v = i < p.n ? p.counts[i] : 0;
+    int64_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const int64_t w = s_warp[lane];
+      int64_t wi = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += t;
+      }
+      s_warp[lane] = wi - w;
+      const int64_t total = __shfl_sync(0xffffffffu, wi, 31);
+      const uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, (uint64_t)total, p.status);
+      if (lane == 0) {
+        s_excl = ex;
+        if (tile == p.ntiles - 1) *p.d_total = (int64_t)(ex + total);
+      }
+    }
+    __syncthreads();
+    if (i < p.n) p.counts[i] = (int64_t)s_excl + s_warp[warp] + incl - v;
+    __syncthreads();
+  }
+  claim_finish(p.counters);
 }
 
 // One CTA: chunk counts -> exclusive offsets in place; the total to d_out_rows.
@@ -825,7 +880,21 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   int grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   count_kernel<<<grid, threads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
-  join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, p.nchunks, d_out_rows);
+  if (p.nchunks <= 4096) {
+    join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, p.nchunks, d_out_rows);
+  } else {
+    ScanParams sp;
+    sp.counts = p.chunk_count;
+    sp.n = p.nchunks;
+    sp.ntiles = (p.nchunks + 1023) / 1024;
+    sp.d_total = d_out_rows;
+    if ((st = lookback_prepare(ctx, sp.ntiles, &sp.epoch, stream))) return st;
+    sp.lb = ctx->lb_status;
+    sp.counters = ctx->d_counters;
+    sp.status = ctx->d_status;
+    const int sgrid = (int)std::min<int64_t>(sp.ntiles, (int64_t)ctx->num_sms);
+    join_scan_lb_kernel<<<sgrid, 1024, 0, stream>>>(sp);
+  }
   GHB_LAUNCH_CHECK(ctx);
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, write_kernel, threads, 0));
   grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));

@@ -554,3 +554,22 @@ def test_join_direct_and_hashed_tables(ctx, dense):
     t.free()
     if dense:  # INT keys
         _check_join(ctx, bkey.astype(np.int32), pkey.astype(np.int32), bpay=pay)
+
+
+def test_join_many_chunks(ctx):
+    """A probe of more than 4096 1024-row chunks: the chunk offsets come from
+    the multi-CTA look-back scan.  Pairs compared as sorted arrays."""
+    g = np.random.default_rng(26)
+    nb, m = 100_000, 6_000_000
+    bkey = g.permutation(np.arange(1, nb + 1, dtype=np.int64))
+    bkey[:1000] = bkey[1000:2000]  # some keys twice
+    pkey = g.integers(0, nb + 5000, m, dtype=np.int64)
+    pr, br = oracle.hash_join(bkey, pkey, abi.INNER_JOIN)
+    t = ctx.join_build(dev(bkey))
+    r = ctx.join_probe(t, dev(pkey), abi.INNER_JOIN)
+    assert r["rows"] == len(pr)
+    gp, gb = host(r["probe_rowid"]).astype(np.int64), host(r["build_rowid"]).astype(np.int64)
+    assert np.all(np.diff(gp) >= 0)
+    o1, o2 = np.lexsort((gb, gp)), np.lexsort((br, pr))
+    assert np.array_equal(gp[o1], pr[o2]) and np.array_equal(gb[o1], br[o2])
+    t.free()
