@@ -75,16 +75,14 @@ struct ghb_join_table {
   ulonglong2* payw = nullptr;          // per slot: first row's inline payload words
   int32_t* chain = nullptr;   // per slot: chain head (row + 1) of the key's 2nd.. rows
   int32_t* next = nullptr;    // per build row: next row + 1 in its key's chain
-  int64_t slots = 0;          // hashed slots (power of two); slot `slots` is the side slot;
-                              // a direct table: one slot per key of [dmin, dmin + slots)
-  int64_t dmin = 0;           // direct table: the smallest build key
-  bool direct = false;        // slot = key - dmin (dense build keys), no key array
+  int64_t slots = 0;          // hashed slots (power of two); slot `slots` is the side slot
+                              // (a direct table uses the first key-range slots of them)
   int64_t build_rows = 0;
   int32_t key_type = GHB_LONG;
   int32_t nbp = 0;            // build payload columns the table serves
   int32_t n_inline = 0;       // of which copied into the slots
   ghb_column pay[8];          // the build payload columns (caller-owned)
-  unsigned long long* d_stats = nullptr;  // [0] rows stored, [1] max duplicates
+  unsigned long long* d_stats = nullptr;  // [0] rows stored, [1] max duplicates, [2..4] key range
   void* alloc = nullptr;      // slots, then chain, next and stats
   size_t alloc_bytes = 0;
   cudaStream_t stream = 0;    // build stream; the table is released in its order

@@ -39,7 +39,6 @@
 //        chunk and writes (probe row, build row, payloads) at its offset, in
 //        probe-row order.
 #include <algorithm>
-#include <climits>
 
 #include "ghb_ctx.hpp"
 
@@ -79,36 +78,63 @@ struct BuildParams {
   int64_t side;          // index of the side bucket
   unsigned long long* stats;  // [0] rows stored, [1] max duplicates
   int32_t* status;
-  int32_t direct;        // slot = key - dmin
-  int64_t dmin;
+  int64_t slots;         // hashed slots allocated (a direct table fits in them)
 };
 
-// Smallest and largest non-NULL build key (signed), for the choice of a
-// direct table.  out: [0] min, [1] max, [2] non-NULL keys.
-__global__ void __launch_bounds__(256) join_key_range_kernel(ghb_column key, long long* out) {
-  long long mn = LLONG_MAX, mx = LLONG_MIN;
-  unsigned long long cnt = 0;
+// The table's layout, decided on the device from the build keys' range
+// (stats[2] non-NULL keys, stats[3] max of the complemented order images,
+// stats[4] max of the order images): dense keys (a range below twice the
+// rows and within the allocated slots, the common surrogate key of a
+// dimension table) get a direct table, slot = key - min, with no key array
+// and no bucket scan on probe; other keys the hashed buckets.  Every thread
+// of the build and probe kernels computes the same answer from the same
+// words, so no host round trip is needed.
+struct JoinLayout {
+  bool direct;
+  int64_t dmin;
+  int64_t drange;
+};
+
+__host__ __device__ inline JoinLayout join_layout(const unsigned long long* stats, int64_t build_rows,
+                                                  int64_t slots) {
+  JoinLayout L{false, 0, 0};
+  if (stats[2] == 0) return L;
+  const unsigned long long umin = ~stats[3], umax = stats[4];
+  const unsigned long long span = umax - umin;   // the images keep the keys' order and distances
+  if (span < 2ull * (unsigned long long)build_rows && span < (unsigned long long)slots && span < (1ull << 30)) {
+    L.direct = true;
+    L.dmin = (int64_t)(umin ^ 0x8000000000000000ull);
+    L.drange = (int64_t)span + 1;
+  }
+  return L;
+}
+
+// The build keys' range into stats[2..4] (zeroed with the table).
+__global__ void __launch_bounds__(256) join_key_range_kernel(ghb_column key, unsigned long long* stats) {
+  unsigned long long cmin = 0, umax = 0, cnt = 0;   // cmin: max of ~image = ~(min image)
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < key.n;
        r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t raw = ld_raw(key, r);
     if (raw_is_null(key, raw, r)) continue;
-    mn = min(mn, (long long)raw);
-    mx = max(mx, (long long)raw);
+    const unsigned long long u = flip_i64(raw);
+    cmin = max(cmin, ~u);
+    umax = max(umax, u);
     cnt++;
   }
   for (int o = 16; o > 0; o >>= 1) {
-    mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
-    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    cmin = max(cmin, __shfl_down_sync(0xffffffffu, cmin, o));
+    umax = max(umax, __shfl_down_sync(0xffffffffu, umax, o));
     cnt += __shfl_down_sync(0xffffffffu, cnt, o);
   }
   if ((threadIdx.x & 31) == 0 && cnt) {
-    atomicMin(&out[0], mn);
-    atomicMax(&out[1], mx);
-    atomicAdd((unsigned long long*)&out[2], cnt);
+    atomicMax(&stats[3], cmin);
+    atomicMax(&stats[4], umax);
+    atomicAdd(&stats[2], cnt);
   }
 }
 
 __global__ void __launch_bounds__(256) join_build_kernel(BuildParams p) {
+  const JoinLayout L = join_layout(p.stats, p.key.n, p.slots);
   unsigned long long stored = 0, maxdup = 0;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < p.key.n;
        r += (int64_t)gridDim.x * blockDim.x) {
@@ -116,8 +142,8 @@ __global__ void __launch_bounds__(256) join_build_kernel(BuildParams p) {
     if (raw_is_null(p.key, raw, r)) continue;   // NULL keys never join
     unsigned long long u = flip_i64(raw);
     int64_t bk, j = -1;
-    if (p.direct) {   // slot = key - dmin: bucket * 4 + j
-      const unsigned long long d = (unsigned long long)raw - (unsigned long long)p.dmin;
+    if (L.direct) {   // slot = key - dmin: bucket * 4 + j
+      const unsigned long long d = (unsigned long long)raw - (unsigned long long)L.dmin;
       bk = (int64_t)(d >> 2);
       j = (int64_t)(d & 3);
     } else if (u == 0) {
@@ -191,8 +217,8 @@ struct ProbeParams {
   int64_t* chunk_count;    // [nchunks] output rows of each chunk, then its offset
   int64_t* d_out_rows;
   int32_t* status;
-  int64_t dmin;            // direct table: slot = key - dmin for keys below dmin + drange
-  int64_t drange;
+  int64_t build_rows;      // with slots: the table's layout (join_layout of stats)
+  int64_t slots;
 };
 
 // Output rows a probe row produces, from its slot's count (0 = no match).
@@ -224,9 +250,8 @@ __device__ __forceinline__ int find_in(const unsigned long long k[4], unsigned l
 }
 
 // TH threads x IT rows per thread = one chunk (kChunk rows) per iteration.
-// DIRECT: the table is direct (slot = key - dmin); else hashed buckets.
 // Four 256-thread CTAs per SM (64 registers): more key and table loads in flight.
-template <int TH, int IT, bool KEY_INT, bool NULLABLE, bool DIRECT>
+template <int TH, int IT, bool KEY_INT, bool NULLABLE>
 __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
@@ -234,6 +259,7 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;   // every key once: a match is one output row
+  const JoinLayout L = join_layout(p.stats, p.build_rows, p.slots);
   const int woff = warp * (32 * kJItems) + lane;
   // The keys of the CTA's next chunk are loaded while this chunk probes the
   // table, so the DRAM latency of the key stream overlaps the table loads.
@@ -269,15 +295,15 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
       u[k] = flip_i64(raw);
     }
     uint64_t m_sum = 0;
-    if constexpr (DIRECT) {
+    if (L.direct) {
       // one load per row: the slot's (first row, count); a key outside
       // [dmin, dmin + drange) has no slot
       int32_t cnt[kJItems];
       unsigned long long d[kJItems];
 #pragma unroll
       for (int k = 0; k < kJItems; k++) {
-        d[k] = (unsigned long long)cur_raw[k] - (unsigned long long)p.dmin;
-        cnt[k] = (valid[k] && d[k] < (unsigned long long)p.drange) ? p.meta[d[k]].y : 0;
+        d[k] = (unsigned long long)cur_raw[k] - (unsigned long long)L.dmin;
+        cnt[k] = (valid[k] && d[k] < (unsigned long long)L.drange) ? p.meta[d[k]].y : 0;
       }
 #pragma unroll
       for (int k = 0; k < kJItems; k++) {
@@ -660,45 +686,8 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
   }
   float lf = (cfg && cfg->load_factor > 0.f && cfg->load_factor < 0.95f) ? cfg->load_factor : 0.5f;
   int64_t nb = next_pow2(std::max<int64_t>(16, (int64_t)((double)build_key->n / (4.0 * lf)) + 1));
-  // Dense build keys (a range at most twice the rows, the common surrogate
-  // key of a dimension table) get a direct table: slot = key - min, no key
-  // array and no bucket scan on probe.  One read of the keys and a host read
-  // of their range decide it.
-  bool direct = false;
-  long long dmin = 0;
-  int64_t drange = 0;
-  if (build_key->n > 0) {
-    long long* d_rng = nullptr;
-    if (cudaMallocAsync((void**)&d_rng, 3 * sizeof(long long), stream) != cudaSuccess) {
-      cudaGetLastError();
-      return set_error(ctx, GHB_ERR_OOM, "cannot allocate the key-range words");
-    }
-    long long init[3] = {LLONG_MAX, LLONG_MIN, 0}, rng[3] = {0, 0, 0};
-    cudaError_t e = cudaMemcpyAsync(d_rng, init, sizeof(init), cudaMemcpyHostToDevice, stream);
-    const int g = (int)std::min<int64_t>((build_key->n + 255) / 256, (int64_t)ctx->num_sms * 8);
-    if (e == cudaSuccess) {
-      join_key_range_kernel<<<g, 256, 0, stream>>>(*build_key, d_rng);
-      ctx->launches++;
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(rng, d_rng, sizeof(rng), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFreeAsync(d_rng, stream);
-    if (e != cudaSuccess) return set_error(ctx, GHB_ERR_CUDA, "join key range: %s", cudaGetErrorString(e));
-    if (rng[2] > 0) {
-      const unsigned long long span = (unsigned long long)rng[1] - (unsigned long long)rng[0];
-      if (span < 2ull * (unsigned long long)build_key->n && span < (1ull << 30)) {
-        direct = true;
-        dmin = rng[0];
-        drange = (int64_t)span + 1;
-      }
-    }
-  }
-  if (direct) nb = (drange + 3) / 4;   // slots grouped by four as the hashed layout's buckets
   ghb_join_table* t = new ghb_join_table();
-  t->slots = direct ? drange : nb * 4;
-  t->direct = direct;
-  t->dmin = dmin;
+  t->slots = nb * 4;
   t->build_rows = build_key->n;
   t->key_type = build_key->type;
   t->nbp = nbp;
@@ -709,8 +698,7 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
     t->n_inline++;
   const size_t slots = (size_t)(nb + 1) * 4;   // hashed buckets + the side bucket
   auto a256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t key_bytes = direct ? 0 : a256(slots * 8), meta_bytes = a256(slots * 8),
-               pay_bytes = a256(slots * 16);
+  const size_t key_bytes = a256(slots * 8), meta_bytes = a256(slots * 8), pay_bytes = a256(slots * 16);
   size_t bucket_bytes = key_bytes + meta_bytes + pay_bytes;
   size_t chain_bytes = a256(slots * 4);
   size_t next_bytes = a256((size_t)std::max<int64_t>(build_key->n, 1) * 4);
@@ -725,7 +713,7 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
     return set_error(ctx, GHB_ERR_OOM, "cannot allocate a %zu-byte join table", bytes);
   }
   t->alloc_bytes = bytes;
-  t->kimg = direct ? nullptr : (unsigned long long*)t->alloc;
+  t->kimg = (unsigned long long*)t->alloc;
   t->meta = (int2*)((char*)t->alloc + key_bytes);
   t->payw = (ulonglong2*)((char*)t->alloc + key_bytes + meta_bytes);
   t->chain = (int32_t*)((char*)t->alloc + bucket_bytes);
@@ -752,10 +740,11 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
   p.side = nb;
   p.stats = t->d_stats;
   p.status = ctx->d_status;
-  p.direct = direct ? 1 : 0;
-  p.dmin = dmin;
+  p.slots = nb * 4;
   if (build_key->n > 0) {
     int grid = (int)std::min<int64_t>((build_key->n + 255) / 256, (int64_t)ctx->num_sms * 8);
+    join_key_range_kernel<<<grid, 256, 0, stream>>>(*build_key, t->d_stats);
+    ctx->launches++;
     join_build_kernel<<<grid, 256, 0, stream>>>(p);
     ctx->launches++;
     cudaError_t e = cudaGetLastError();
@@ -836,8 +825,8 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   p.bmask = t->slots / 4 - 1;
   p.hshift = 64 - __builtin_ctzll((unsigned long long)(t->slots / 4));
   p.side = t->slots / 4;
-  p.dmin = t->dmin;
-  p.drange = t->direct ? t->slots : 0;
+  p.build_rows = t->build_rows;
+  p.slots = t->slots;
   p.pkey = *probe_key;
   p.join_type = join_type;
   p.nbp = t->nbp;
@@ -864,17 +853,14 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   const bool kint = probe_key->type == GHB_INT, knull = probe_key->null_mode != GHB_NULLS_NONE;
   void (*count_kernel)(ProbeParams) = nullptr;
   void (*write_kernel)(ProbeParams) = nullptr;
-#define GHB_COUNT_D(TH, IT, D)                                                              \
-  count_kernel = kint ? (knull ? join_count_kernel<TH, IT, true, true, D> : join_count_kernel<TH, IT, true, false, D>) \
-                      : (knull ? join_count_kernel<TH, IT, false, true, D> : join_count_kernel<TH, IT, false, false, D>)
 #define GHB_COUNT(TH, IT)                                                                   \
-  if (t->direct) { GHB_COUNT_D(TH, IT, true); } else { GHB_COUNT_D(TH, IT, false); }        \
+  count_kernel = kint ? (knull ? join_count_kernel<TH, IT, true, true> : join_count_kernel<TH, IT, true, false>) \
+                      : (knull ? join_count_kernel<TH, IT, false, true> : join_count_kernel<TH, IT, false, false>); \
   write_kernel = join_write_kernel<TH, IT>
   if (threads == 128) { GHB_COUNT(128, 8); }
   else if (threads == 512) { GHB_COUNT(512, 2); }
   else { GHB_COUNT(256, 4); }
 #undef GHB_COUNT
-#undef GHB_COUNT_D
   int per_sm = 0;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, count_kernel, threads, 0));
   int grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
@@ -935,11 +921,13 @@ int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table) {
 int32_t ghb_join_table_info(ghb_ctx* ctx, const ghb_join_table* table, int64_t* rows,
                             int64_t* max_dup, int64_t* slots) {
   if (!ctx || !table) return GHB_ERR_INVALID;
-  unsigned long long st[2] = {0, 0};
+  unsigned long long st[5] = {0, 0, 0, 0, 0};
   GHB_CUDA_TRY(ctx, cudaMemcpy(st, table->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
   if (rows) *rows = (int64_t)st[0];
   if (max_dup) *max_dup = (int64_t)st[1];
-  if (slots) *slots = table->slots;
+  // a direct table reports its key range as its slots
+  const JoinLayout L = join_layout(st, table->build_rows, table->slots);
+  if (slots) *slots = L.direct ? L.drange : table->slots;
   return GHB_OK;
 }
 
