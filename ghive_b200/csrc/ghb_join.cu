@@ -552,10 +552,86 @@ __device__ __forceinline__ void emit_lean(const LeanOut& o, int64_t pos, int64_t
   }
 }
 
+// The write pass of an INNER join on unique build keys whose output is the
+// probe row and at most two inline, non-NULL build payloads (p.lean, no
+// build row ids): a row's output is its slot's two payload words or nothing,
+// so a thread keeps only slots and words and many CTAs fit on an SM.  It runs
+// beside the general write pass; the build's statistics (unique keys) choose
+// which of the two does the work and the other returns at once.
+template <int TH, int IT>
+__global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
+  static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
+  if (!(p.lean && p.out_brow == nullptr && p.stats[1] <= 1)) return;
+  __shared__ uint32_t s_warp_tot[TH / 32];
+  __shared__ uint32_t s_warp_excl[TH / 32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  int32_t next_s[IT];
+#pragma unroll
+  for (int k = 0; k < IT; k++) {
+    const int64_t row = (int64_t)blockIdx.x * kChunk + (int64_t)warp * (32 * IT) + k * 32 + lane;
+    next_s[k] = row < p.n ? __ldcs(p.slot_of_row + row) : -1;
+  }
+  for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
+    const int64_t wbase = c * kChunk + (int64_t)warp * (32 * IT);
+    int32_t s[IT];
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      s[k] = next_s[k];
+      const int64_t nrow = wbase + (int64_t)gridDim.x * kChunk + k * 32 + lane;
+      next_s[k] = nrow < p.n ? __ldcs(p.slot_of_row + nrow) : -1;
+    }
+    ulonglong2 w[IT];
+#pragma unroll
+    for (int k = 0; k < IT; k++) w[k] = s[k] >= 0 && p.nbp > 0 ? p.payw[s[k]] : make_ulonglong2(0, 0);
+    uint32_t excl[IT];
+    uint32_t running = 0;
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      const unsigned bal = __ballot_sync(0xffffffffu, s[k] >= 0);
+      excl[k] = running + __popc(bal & ((1u << lane) - 1u));
+      running += __popc(bal);
+    }
+    if (lane == 0) s_warp_tot[warp] = running;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t v = lane < TH / 32 ? s_warp_tot[lane] : 0;
+      uint32_t incl = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane < TH / 32) s_warp_excl[lane] = incl - v;
+    }
+    __syncthreads();
+    const int64_t wpos = p.chunk_count[c] + s_warp_excl[warp];
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      if (s[k] < 0) continue;
+      const int64_t pos = wpos + excl[k];
+      if (pos >= p.cap) {
+        raise_status(p.status, kDevCapacity);
+        continue;
+      }
+      if (p.out_prow) __stcs(p.out_prow + pos, (int)(wbase + k * 32 + lane));
+#pragma unroll
+      for (int j = 0; j < kInline; j++) {
+        if (j >= p.nbp) break;
+        const unsigned long long x = j == 0 ? w[k].x : w[k].y;
+        if (p.bpay[j].type == GHB_INT) __stcs((int*)p.obp[j].data + pos, (int)x);
+        else __stcs((unsigned long long*)p.obp[j].data + pos, x);
+        if (p.obp[j].is_null) p.obp[j].is_null[pos] = 0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int TH, int IT>
 __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
+  if (p.lean && p.out_brow == nullptr && p.stats[1] <= 1) return;   // join_write_lean_kernel's case
   __shared__ uint32_t s_warp_tot[kJThreads / 32];
   __shared__ uint32_t s_warp_excl[kJThreads / 32];
   const int lane = threadIdx.x & 31;
@@ -853,10 +929,12 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   const bool kint = probe_key->type == GHB_INT, knull = probe_key->null_mode != GHB_NULLS_NONE;
   void (*count_kernel)(ProbeParams) = nullptr;
   void (*write_kernel)(ProbeParams) = nullptr;
+  void (*write_lean)(ProbeParams) = nullptr;
 #define GHB_COUNT(TH, IT)                                                                   \
   count_kernel = kint ? (knull ? join_count_kernel<TH, IT, true, true> : join_count_kernel<TH, IT, true, false>) \
                       : (knull ? join_count_kernel<TH, IT, false, true> : join_count_kernel<TH, IT, false, false>); \
-  write_kernel = join_write_kernel<TH, IT>
+  write_kernel = join_write_kernel<TH, IT>;                                                  \
+  write_lean = join_write_lean_kernel<TH, IT>
   if (threads == 128) { GHB_COUNT(128, 8); }
   else if (threads == 512) { GHB_COUNT(512, 2); }
   else { GHB_COUNT(256, 4); }
@@ -885,6 +963,12 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, write_kernel, threads, 0));
   grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   write_kernel<<<grid, threads, 0, stream>>>(p);
+  GHB_LAUNCH_CHECK(ctx);
+  if (p.lean && !p.out_brow) {   // the lean write pass, when the build's keys turn out unique
+    GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, write_lean, threads, 0));
+    grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
+    write_lean<<<grid, threads, 0, stream>>>(p);
+  }
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;
 }
