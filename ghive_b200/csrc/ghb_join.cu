@@ -249,6 +249,71 @@ __device__ __forceinline__ int find_in(const unsigned long long k[4], unsigned l
   return -2;
 }
 
+// The count pass over a direct table: one load of the slot's row count per
+// probe row, nothing else, so a thread keeps little and many CTAs fit on an
+// SM.  It runs beside the hashed count pass; the build's key range chooses
+// which of the two does the work and the other returns at once.
+template <int TH, int IT, bool KEY_INT, bool NULLABLE>
+__global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
+  static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
+  const JoinLayout L = join_layout(p.stats, p.build_rows, p.slots);
+  if (!L.direct) return;
+  __shared__ uint64_t s_warp[TH / 32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const bool unique = p.stats[1] <= 1;
+  const int woff = warp * (32 * IT) + lane;
+  auto load_chunk_keys = [&](int64_t c, long long* raw) {
+    const int64_t cbase = c * kChunk;
+    const int left = (int)min((int64_t)kChunk, p.n - cbase);
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      const int off = woff + k * 32;
+      raw[k] = 0;
+      if (c < p.nchunks && off < left)
+        raw[k] = KEY_INT ? (long long)__ldcs((const int*)p.pkey.data + cbase + off)
+                         : __ldcs((const long long*)p.pkey.data + cbase + off);
+    }
+  };
+  long long next_raw[IT];
+  load_chunk_keys(blockIdx.x, next_raw);
+  for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
+    const int64_t cbase = c * kChunk;
+    const int left = (int)min((int64_t)kChunk, p.n - cbase);
+    long long raw[IT];
+#pragma unroll
+    for (int k = 0; k < IT; k++) raw[k] = next_raw[k];
+    load_chunk_keys(c + gridDim.x, next_raw);
+    unsigned long long d[IT];
+    int32_t cnt[IT];
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      const int off = woff + k * 32;
+      const bool valid = off < left && !(NULLABLE && raw_is_null(p.pkey, raw[k], cbase + off));
+      d[k] = (unsigned long long)raw[k] - (unsigned long long)L.dmin;
+      cnt[k] = (valid && d[k] < (unsigned long long)L.drange) ? p.meta[d[k]].y : 0;
+    }
+    uint64_t m_sum = 0;
+#pragma unroll
+    for (int k = 0; k < IT; k++) {
+      const int off = woff + k * 32;
+      if (off < left) {
+        p.slot_of_row[cbase + off] = cnt[k] > 0 ? (int32_t)d[k] : -1;
+        m_sum += (uint64_t)out_rows_of(p.join_type, unique ? (cnt[k] > 0 ? 1 : 0) : cnt[k]);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) m_sum += __shfl_down_sync(0xffffffffu, m_sum, o);
+    if (lane == 0) s_warp[warp] = m_sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint64_t t = 0;
+      for (int w = 0; w < TH / 32; w++) t += s_warp[w];
+      p.chunk_count[c] = (int64_t)t;
+    }
+    __syncthreads();
+  }
+}
+
 // TH threads x IT rows per thread = one chunk (kChunk rows) per iteration.
 // Four 256-thread CTAs per SM (64 registers): more key and table loads in flight.
 template <int TH, int IT, bool KEY_INT, bool NULLABLE>
@@ -259,7 +324,7 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;   // every key once: a match is one output row
-  const JoinLayout L = join_layout(p.stats, p.build_rows, p.slots);
+  if (join_layout(p.stats, p.build_rows, p.slots).direct) return;   // join_count_direct_kernel's table
   const int woff = warp * (32 * kJItems) + lane;
   // The keys of the CTA's next chunk are loaded while this chunk probes the
   // table, so the DRAM latency of the key stream overlaps the table loads.
@@ -295,25 +360,6 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
       u[k] = flip_i64(raw);
     }
     uint64_t m_sum = 0;
-    if (L.direct) {
-      // one load per row: the slot's (first row, count); a key outside
-      // [dmin, dmin + drange) has no slot
-      int32_t cnt[kJItems];
-      unsigned long long d[kJItems];
-#pragma unroll
-      for (int k = 0; k < kJItems; k++) {
-        d[k] = (unsigned long long)cur_raw[k] - (unsigned long long)L.dmin;
-        cnt[k] = (valid[k] && d[k] < (unsigned long long)L.drange) ? p.meta[d[k]].y : 0;
-      }
-#pragma unroll
-      for (int k = 0; k < kJItems; k++) {
-        const int off = woff + k * 32;
-        if (off < left) {
-          p.slot_of_row[cbase + off] = cnt[k] > 0 ? (int32_t)d[k] : -1;
-          m_sum += (uint64_t)out_rows_of(p.join_type, unique ? (cnt[k] > 0 ? 1 : 0) : cnt[k]);
-        }
-      }
-    } else {
     int64_t bk[kJItems];
     unsigned long long keys[kJItems][4];
 #pragma unroll
@@ -347,7 +393,6 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
         p.slot_of_row[row] = slot;
         m_sum += (uint64_t)out_rows_of(p.join_type, count);
       }
-    }
     }
     for (int o = 16; o > 0; o >>= 1) m_sum += __shfl_down_sync(0xffffffffu, m_sum, o);
     if (lane == 0) s_warp[warp] = m_sum;
@@ -930,9 +975,12 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   void (*count_kernel)(ProbeParams) = nullptr;
   void (*write_kernel)(ProbeParams) = nullptr;
   void (*write_lean)(ProbeParams) = nullptr;
+  void (*count_direct)(ProbeParams) = nullptr;
 #define GHB_COUNT(TH, IT)                                                                   \
   count_kernel = kint ? (knull ? join_count_kernel<TH, IT, true, true> : join_count_kernel<TH, IT, true, false>) \
                       : (knull ? join_count_kernel<TH, IT, false, true> : join_count_kernel<TH, IT, false, false>); \
+  count_direct = kint ? (knull ? join_count_direct_kernel<TH, IT, true, true> : join_count_direct_kernel<TH, IT, true, false>) \
+                      : (knull ? join_count_direct_kernel<TH, IT, false, true> : join_count_direct_kernel<TH, IT, false, false>); \
   write_kernel = join_write_kernel<TH, IT>;                                                  \
   write_lean = join_write_lean_kernel<TH, IT>
   if (threads == 128) { GHB_COUNT(128, 8); }
@@ -943,6 +991,11 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, count_kernel, threads, 0));
   int grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   count_kernel<<<grid, threads, 0, stream>>>(p);
+  GHB_LAUNCH_CHECK(ctx);
+  // the count pass of a direct table (the build decided on the device which one works)
+  GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, count_direct, threads, 0));
+  grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  count_direct<<<grid, threads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
   if (p.nchunks <= 4096) {
     join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, p.nchunks, d_out_rows);
