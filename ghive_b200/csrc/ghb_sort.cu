@@ -138,9 +138,35 @@ __global__ void __launch_bounds__(256) sort_minmax_kernel(MinMaxParams p) {
 }
 
 // ---------------------------------------------------------------- histogram
+// One sub-field of a packed key with everything its bits need, so a kernel
+// packing keys reads it with constant indices.
+struct SubPlan {
+  ghb_column col;
+  uint64_t umin;
+  int8_t shift;
+  int8_t is_flag;
+  int8_t desc;
+  int8_t nulls_first;
+  int8_t has_null;
+};
+
+__device__ __forceinline__ uint64_t sub_bits_plan(const SubPlan& sp, int64_t raw, int64_t r) {
+  const bool null = sp.has_null && raw_is_null(sp.col, raw, r);
+  uint64_t v;
+  if (sp.is_flag) {
+    v = (null == (bool)sp.nulls_first) ? 0 : 1;   // NULLS FIRST: null 0 / value 1
+  } else {
+    uint64_t u = key_image(sp.col, raw);
+    if (sp.desc) u = ~u;
+    v = null ? 0 : u - sp.umin;
+  }
+  return v << sp.shift;
+}
+
 struct HistParams {
   KeySet K;
   Segment seg;
+  SubPlan sub[kMaxSub];     // the segment's sub-fields, self-contained
   int64_t n;
   int32_t npasses;
   uint32_t* hist;  // [npasses][kBins]
@@ -163,11 +189,20 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
     uint64_t k[U];
 #pragma unroll
     for (int u = 0; u < U; u++) k[u] = 0;
-    for (int i = 0; i < p.seg.n; i++) {
+#pragma unroll
+    for (int i = 0; i < kMaxSub; i++) {
+      if (i >= p.seg.n) break;
+      const SubPlan& sp = p.sub[i];
+      int64_t raw[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        int64_t r = base + u * stride;
-        if (r < p.n) k[u] |= sub_bits(p.K, p.seg.f[i], r);
+        const int64_t r = base + u * stride;
+        raw[u] = r < p.n ? ld_raw(sp.col, r) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t r = base + u * stride;
+        if (r < p.n) k[u] |= sub_bits_plan(sp, raw[u], r);
       }
     }
 #pragma unroll
@@ -684,6 +719,18 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     hp.n = n;
     hp.npasses = np;
     hp.hist = d_hist + s * kMaxPasses * kBins;
+    for (int i = 0; i < segs[s].n; i++) {
+      const SubField& sf = segs[s].f[i];
+      const KeyField& kf = K.k[sf.key];
+      SubPlan& sp = hp.sub[i];
+      sp.col = kf.col;
+      sp.umin = kf.umin;
+      sp.shift = sf.shift;
+      sp.is_flag = sf.is_flag;
+      sp.desc = (int8_t)kf.desc;
+      sp.nulls_first = (int8_t)kf.nulls_first;
+      sp.has_null = (int8_t)kf.has_null;
+    }
     hp.keys_out = multi ? nullptr : kb[0];
     hp.vals_out = vb[0];
     hp.vals_wide = wide ? 1 : 0;
