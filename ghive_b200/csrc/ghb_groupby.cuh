@@ -545,23 +545,37 @@ constexpr int kFinThreads = 256;
 __host__ __device__ inline int64_t fin_units(int64_t C) { return (C + kFinThreads - 1) / kFinThreads; }
 
 // Called by all kFinThreads threads of a CTA for unit `unit` of the table:
-// each warp covers one bitmap word, takes one block of output rows for the
-// word's claimed slots (ballot + one atomic), clears the word, and each lane
-// with a claimed slot emits its group.  `rb` is the CTA's record buffer,
-// [kFinThreads][kMaxAcc + 1] words.
+// each warp covers one bitmap word (ballot), the CTA takes one block of
+// output rows for the unit's claimed slots (one atomic per CTA: per warp,
+// a large table's warps would serialise on the counter), each warp clears its
+// word, and each lane with a claimed slot emits its group.  `rb` is the CTA's
+// record buffer, [kFinThreads][kMaxAcc + 1] words.
 __device__ __forceinline__ void finalize_unit(const FinParams& f, int64_t unit, uint64_t* rb) {
+  __shared__ uint32_t s_cnt[kFinThreads / 32];
+  __shared__ unsigned long long s_base;
   const int64_t s = unit * kFinThreads + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t word = s < f.C ? f.gbits[s >> 5] : 0u;   // the same word for the whole warp
   const bool has = (word >> lane) & 1u;
   const unsigned m = __ballot_sync(0xffffffffu, has);
-  unsigned long long base = 0;
-  if (lane == 0 && m) {
-    base = atomicAdd(f.growc, (unsigned long long)__popc(m));
-    f.gbits[s >> 5] = 0;
+  if (lane == 0) {
+    s_cnt[warp] = __popc(m);
+    if (m) f.gbits[s >> 5] = 0;
   }
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (has) emit_group(f, s, (int64_t)base + __popc(m & ((1u << lane) - 1u)), rb + threadIdx.x * (kMaxAcc + 1));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int w = 0; w < kFinThreads / 32; w++) {
+      const uint32_t c = s_cnt[w];
+      s_cnt[w] = run;
+      run += c;
+    }
+    s_base = run ? atomicAdd(f.growc, (unsigned long long)run) : 0ull;
+  }
+  __syncthreads();
+  const int64_t row = (int64_t)s_base + s_cnt[warp] + __popc(m & ((1u << lane) - 1u));
+  if (has) emit_group(f, s, row, rb + threadIdx.x * (kMaxAcc + 1));
+  __syncthreads();   // s_cnt and s_base are reused by the next unit
 }
 
 // One thread: the two side records (key INT64_MIN, NULL key); a global

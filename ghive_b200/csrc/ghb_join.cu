@@ -126,10 +126,27 @@ __global__ void __launch_bounds__(256) join_key_range_kernel(ghb_column key, uns
     umax = max(umax, __shfl_down_sync(0xffffffffu, umax, o));
     cnt += __shfl_down_sync(0xffffffffu, cnt, o);
   }
-  if ((threadIdx.x & 31) == 0 && cnt) {
-    atomicMax(&stats[3], cmin);
-    atomicMax(&stats[4], umax);
-    atomicAdd(&stats[2], cnt);
+  // one set of atomics per CTA (the same three words from every warp would
+  // serialise at L2)
+  __shared__ unsigned long long s_red[3][8];
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    s_red[0][warp] = cmin;
+    s_red[1][warp] = umax;
+    s_red[2][warp] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+      cmin = max(cmin, s_red[0][w]);
+      umax = max(umax, s_red[1][w]);
+      cnt += s_red[2][w];
+    }
+    if (cnt) {
+      atomicMax(&stats[3], cmin);
+      atomicMax(&stats[4], umax);
+      atomicAdd(&stats[2], cnt);
+    }
   }
 }
 
@@ -180,12 +197,24 @@ __global__ void __launch_bounds__(256) join_build_kernel(BuildParams p) {
     stored++;
     maxdup = max(maxdup, (unsigned long long)(old + 1));
   }
-  // one atomic per warp for the statistics
+  // one atomic per CTA for the statistics (per warp, thousands of warps'
+  // atomics on two words would serialise at L2)
   for (int o = 16; o > 0; o >>= 1) {
     stored += __shfl_down_sync(0xffffffffu, stored, o);
     maxdup = max(maxdup, __shfl_down_sync(0xffffffffu, maxdup, o));
   }
+  __shared__ unsigned long long s_red[2][8];
+  const int warp = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    s_red[0][warp] = stored;
+    s_red[1][warp] = maxdup;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+      stored += s_red[0][w];
+      maxdup = max(maxdup, s_red[1][w]);
+    }
     if (stored) atomicAdd(&p.stats[0], stored);
     if (maxdup) atomicMax(&p.stats[1], maxdup);
   }

@@ -129,11 +129,27 @@ __global__ void __launch_bounds__(256) sort_minmax_kernel(MinMaxParams p) {
       mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
       anynull |= __shfl_down_sync(0xffffffffu, anynull, o);
     }
+    // one set of atomics per CTA: every CTA's warps hitting the same three
+    // words would serialise at L2
+    __shared__ unsigned long long s_red[3][8];
+    const int warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
+      s_red[0][warp] = mn;
+      s_red[1][warp] = mx;
+      s_red[2][warp] = anynull;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+        mn = min(mn, s_red[0][w]);
+        mx = max(mx, s_red[1][w]);
+        anynull |= s_red[2][w];
+      }
       atomicMin(&p.out[3 * j], mn);
       atomicMax(&p.out[3 * j + 1], mx);
       if (anynull) atomicOr(&p.out[3 * j + 2], 1ull);
     }
+    __syncthreads();
   }
 }
 
