@@ -869,7 +869,10 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
   t->chain = (int32_t*)((char*)t->alloc + bucket_bytes);
   t->next = (int32_t*)((char*)t->alloc + bucket_bytes + chain_bytes);
   t->d_stats = (unsigned long long*)((char*)t->alloc + bucket_bytes + chain_bytes + next_bytes);
-  if (cudaMemsetAsync(t->alloc, 0, bucket_bytes + chain_bytes, stream) != cudaSuccess ||
+  // keys, counts and chain heads start at zero; the payload words are read
+  // only in slots a build row filled, so they are not cleared
+  if (cudaMemsetAsync(t->alloc, 0, key_bytes + meta_bytes, stream) != cudaSuccess ||
+      cudaMemsetAsync(t->chain, 0, chain_bytes, stream) != cudaSuccess ||
       cudaMemsetAsync(t->d_stats, 0, 256, stream) != cudaSuccess) {
     cudaFreeAsync(t->alloc, stream);
     delete t;
