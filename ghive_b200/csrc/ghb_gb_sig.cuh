@@ -271,6 +271,16 @@ struct SigFolder {
   }
   static constexpr int kTableWords = off<kN>();   // u32 words per slot
 
+  // A global aggregate keeps each thread's partial aggregates in registers
+  // for the whole launch (sums, counts, extremes in the shared table's
+  // narrow form; a double sum with its compensation word) and merges them
+  // once, in drain, instead of reducing every row slot across the warp.
+  struct Empty {};
+  struct Partials {
+    uint64_t w[kN];
+  };
+  using State = typename TypeIf<KEYED, Empty, Partials>::type;
+
   template <int... I>
   struct Seq {};
   template <int N, int... I>
@@ -303,7 +313,7 @@ struct SigFolder {
   template <int I, class ACC>
   __device__ __forceinline__ static void acc_pass(const GbParams& p, const unsigned char* stage, const int* slot,
                                                   const bool* ins, const unsigned* peers, uint32_t* tab,
-                                                  int sstride, uint64_t* wstage) {
+                                                  int sstride, uint64_t* wstage, State& st) {
     constexpr int kind = ACC::kind;
     if constexpr (kind == A_COMP_F) {
       return;
@@ -312,21 +322,21 @@ struct SigFolder {
       for (int j = 0; j < ROWS; j++) {
         const int r = j * blockDim.x + threadIdx.x;
         if constexpr (!KEYED) {
-          // every live row is in the one group: a warp reduction, one update
-          const int lane = threadIdx.x & 31;
-          uint64_t tot = 0, comp = 0;
-          if constexpr (kind == A_SUM_F) {
-            double sf = ins[j] ? __longlong_as_double(ACC::contrib(p, stage, r)) : 0.0, cf = 0.0;
-            warp_sum_f64(sf, cf);
-            tot = (uint64_t)__double_as_longlong(sf);
-            comp = (uint64_t)__double_as_longlong(cf);
-          } else if constexpr (kind == A_MAX_O || kind == A_MIN_O) {
-            tot = warp_max_u64(ins[j] ? ACC::narrow(p, stage, r) : 0);
-          } else {
-            tot = warp_sum_u64(ins[j] ? ACC::contrib(p, stage, r) : 0);
+          // every live row is in the one group: into this thread's partials
+          if (ins[j]) {
+            if constexpr (kind == A_SUM_F) {
+              const double x = __longlong_as_double(ACC::contrib(p, stage, r));
+              const double s0 = __longlong_as_double(st.w[I]);
+              const double t = __dadd_rn(s0, x);
+              st.w[I + 1] = (uint64_t)__double_as_longlong(
+                  __dadd_rn(__longlong_as_double(st.w[I + 1]), two_sum_err(s0, x, t)));
+              st.w[I] = (uint64_t)__double_as_longlong(t);
+            } else if constexpr (kind == A_MAX_O || kind == A_MIN_O) {
+              st.w[I] = max(st.w[I], ACC::narrow(p, stage, r));
+            } else {
+              st.w[I] += ACC::contrib(p, stage, r);
+            }
           }
-          const unsigned any = __ballot_sync(0xffffffffu, ins[j]);
-          if (any && lane == __ffs(any) - 1) shared_merge<I, ACC>(tab, sstride, slot[j], tot, comp);
         } else if (WAGG == 1 || (WAGG == 2 && p.warp_agg)) {
           // lanes of one shared slot combine first; the lowest applies it
           wstage[threadIdx.x & 31] = ins[j] ? ACC::narrow(p, stage, r) : 0;
@@ -364,8 +374,58 @@ struct SigFolder {
   template <int... I>
   __device__ __forceinline__ static void all_accs(Seq<I...>, const GbParams& p, const unsigned char* stage,
                                                   const int* slot, const bool* ins, const unsigned* peers,
-                                                  uint32_t* tab, int sstride, uint64_t* wstage) {
-    (acc_pass<I, ACCS>(p, stage, slot, ins, peers, tab, sstride, wstage), ...);
+                                                  uint32_t* tab, int sstride, uint64_t* wstage, State& st) {
+    (acc_pass<I, ACCS>(p, stage, slot, ins, peers, tab, sstride, wstage, st), ...);
+  }
+
+  // One accumulator of a global aggregate's partials: reduced across the
+  // warp, merged by lane 0 into the one group's shared slot (or its global
+  // record when there is no shared table), then cleared.
+  template <int I, class ACC>
+  __device__ __forceinline__ static void drain_one(const GbParams& p, uint32_t* tab, int sstride, State& st) {
+    constexpr int kind = ACC::kind;
+    if constexpr (!KEYED && kind != A_COMP_F) {
+      uint64_t tot = 0, comp = 0;
+      if constexpr (kind == A_SUM_F) {
+        double sf = __longlong_as_double(st.w[I]), cf = __longlong_as_double(st.w[I + 1]);
+        warp_sum_f64(sf, cf);
+        tot = (uint64_t)__double_as_longlong(sf);
+        comp = (uint64_t)__double_as_longlong(cf);
+        st.w[I + 1] = 0;
+      } else if constexpr (kind == A_MAX_O || kind == A_MIN_O) {
+        tot = warp_max_u64(st.w[I]);
+      } else {
+        tot = warp_sum_u64(st.w[I]);
+      }
+      st.w[I] = 0;
+      if ((threadIdx.x & 31) == 0) {
+        const int S = p.smem_slots;
+        if (S > 0) {
+          shared_merge<I, ACC>(tab, sstride, S + 1, tot, comp);
+        } else {
+          // global record: extremes in the wide form (an untouched u32 word is
+          // the neutral value, harmless to merge, as in flush)
+          uint64_t w = tot;
+          if constexpr (ACC::rep == R_IMG32) {
+            const uint64_t img = img32_to_64(kind == A_MAX_O ? (uint32_t)tot : ~(uint32_t)tot);
+            w = kind == A_MAX_O ? img : ~img;
+          }
+          acc_merge(kind, p.grec + (p.C + 1) * p.R + 1 + I, 1, w, comp);
+        }
+      }
+    }
+  }
+
+  template <int... I>
+  __device__ __forceinline__ static void drain_all(Seq<I...>, const GbParams& p, uint32_t* tab, int sstride,
+                                                   State& st) {
+    (drain_one<I, ACCS>(p, tab, sstride, st), ...);
+  }
+
+  // Merges this thread's partials (a global aggregate's) into the table; all
+  // threads, before the barrier that precedes the flush.
+  __device__ __forceinline__ static void drain(const GbParams& p, uint64_t* skeys, State& st) {
+    if constexpr (!KEYED) drain_all(Accs{}, p, (uint32_t*)skeys, p.smem_slots + 2, st);
   }
 
   // Every accumulator of row r into global record g.
@@ -386,7 +446,7 @@ struct SigFolder {
   }
 
   __device__ __forceinline__ static void fold(const GbParams& p, const unsigned char* stage, int rows,
-                                              uint64_t* skeys, uint64_t* wstage) {
+                                              uint64_t* skeys, uint64_t* wstage, State& st) {
     const int S = p.smem_slots;
     const int sstride = S + 2;
     uint32_t* tab = (uint32_t*)skeys;
@@ -468,7 +528,7 @@ struct SigFolder {
       if (KEYED && (WAGG == 1 || (WAGG == 2 && p.warp_agg)))
         peers[j] = __match_any_sync(0xffffffffu, ins[j] ? slot[j] : -1);
     }
-    all_accs(Accs{}, p, stage, slot, ins, peers, tab, sstride, wstage);
+    all_accs(Accs{}, p, stage, slot, ins, peers, tab, sstride, wstage, st);
     if (__any_sync(0xffffffffu, glob)) {
 #pragma unroll
       for (int j = 0; j < ROWS; j++)

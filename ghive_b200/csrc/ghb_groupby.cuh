@@ -593,10 +593,12 @@ __device__ __forceinline__ void finalize_sides(const FinParams& f, uint64_t* rb)
 template <bool KEYED, bool NULLABLE>
 struct GenericFolder {
   static constexpr bool kNarrow = false;   // 64-bit shared counters: no flush guard
+  struct State {};                          // nothing kept per thread between tiles
   __device__ __forceinline__ static void fold(const GbParams& p, const unsigned char* stage, int rows,
-                                              uint64_t* skeys, uint64_t* wstage) {
+                                              uint64_t* skeys, uint64_t* wstage, State&) {
     fold_tile<KEYED, NULLABLE>(p, stage, rows, skeys, wstage);
   }
+  __device__ __forceinline__ static void drain(const GbParams&, uint64_t*, State&) {}
   // The shared table of p fits the words the launch reserved.
   __device__ __forceinline__ static bool fits(const GbParams& p) {
     return (int64_t)(p.smem_slots + 2) * (1 + p.acc.n_acc) <= p.table_words;
@@ -638,6 +640,7 @@ __device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
   }
 
   Folder::clear(p, skeys);
+  typename Folder::State st{};   // per-thread partial aggregates of the folder, if it keeps any
   if (threadIdx.x < kGbMaxStages) {
     done[threadIdx.x] = 0;
     issued[threadIdx.x] = 0;
@@ -672,7 +675,7 @@ __device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
       if (lane == 0) atomicExch(gave_up, 1);
       break;
     }
-    Folder::fold(p, stage(s), p.tile_rows, skeys, wstage);
+    Folder::fold(p, stage(s), p.tile_rows, skeys, wstage, st);
     // Every value the warp read from the stage has been consumed by the fold
     // (in-order issue waits for a load's result at its first use), so after
     // __syncwarp the warp's reads are complete.  No memory fence here: one
@@ -699,9 +702,11 @@ __device__ __forceinline__ void fold_kernel_body(const GbParams& p) {
   for (int64_t i = nfull; i < mine; i++) {
     const int64_t tile = tile_of(i);
     load_tile_plain(p, stage(0), tile);
-    Folder::fold(p, stage(0), (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows), skeys, wstage);
+    Folder::fold(p, stage(0), (int)min((int64_t)p.tile_rows, p.n - tile * p.tile_rows), skeys, wstage, st);
     __syncthreads();
   }
+  Folder::drain(p, skeys, st);
+  __syncthreads();
   Folder::flush(p, skeys);
 }
 
@@ -801,6 +806,7 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
   int32_t active = -1;
   bool failed = false;
   uint64_t since = 0;   // rows of `active` folded since its shared table was last cleared
+  typename Folder::State st{};   // per-thread partial aggregates of the folder, if it keeps any
   for (int64_t it = 0;; it++) {
     const int s = (int)(it & 1);
     if (!((valid >> s) & 1u)) break;
@@ -808,6 +814,8 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     const int64_t tile = s ? q_tile[1] : q_tile[0];
     if (inst != active) {
       if (active >= 0) {
+        Folder::drain(*sp, skeys, st);
+        __syncthreads();
         Folder::flush(*sp, skeys);
         __syncthreads();
       }
@@ -831,11 +839,13 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     }
     const unsigned char* stage = smem_raw + s * (size_t)bp.stage_bytes;
     const int rows = (int)min((int64_t)sp->tile_rows, sp->n - tile * sp->tile_rows);
-    Folder::fold(*sp, stage, rows, skeys, wstage);
+    Folder::fold(*sp, stage, rows, skeys, wstage, st);
     __syncthreads();  // every thread is done with this stage
     if constexpr (Folder::kNarrow) {
       since += (uint64_t)rows;
       if (since + (uint64_t)sp->tile_rows > kNarrowRowLimit) {
+        Folder::drain(*sp, skeys, st);
+        __syncthreads();
         Folder::flush(*sp, skeys);
         __syncthreads();
         Folder::clear(*sp, skeys);
@@ -864,7 +874,11 @@ __device__ __forceinline__ void batch_fold_body(const BatchParams& bp) {
     return;
   }
   __syncthreads();
-  if (active >= 0) Folder::flush(*sp, skeys);
+  if (active >= 0) {
+    Folder::drain(*sp, skeys, st);
+    __syncthreads();
+    Folder::flush(*sp, skeys);
+  }
 }
 
 
