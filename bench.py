@@ -310,7 +310,7 @@ def run_ours(args, world, rank, local):
                            "l2": "inputs larger than L2 (probe key column 480 MB)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
-                             "kernel": "join_probe_kernel",
+                             "kernel": "join probe: count + scan + write passes (one ghb_join_probe call)",
                              "bytes_per_launch": probe_bytes, "ms_per_launch": probe_ms,
                              "traffic": profile_traffic("join_probe_60M.md")},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
