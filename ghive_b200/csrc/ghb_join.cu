@@ -7,47 +7,51 @@
 // 4-97).  Hive's CPU map-join probes a power-of-two open-addressing table
 // whose value store holds each build row's retained columns
 // (VectorMapJoinFastLongHashTable.java:99-254, VectorMapJoinFastLongHashMap.
-// java:71-84).  The device table keeps keys and values together, laid out in
-// 128-byte buckets, one L2 line each, of four slots:
+// java:71-84).  The device table keeps, per slot, the key, the (first row,
+// count) of the rows with that key and the first row's payload words, in
+// three arrays (below), under one of two layouts the build chooses on the
+// device from the keys' range (join_layout):
 //
-//   sector 0   uint64 key image[4]      (flip_i64 of the key, 0 = empty)
-//   sector 1   int32  first row + 1 [4], int32 rows with this key [4]
-//   sectors 2-3 uint64 payload[4][2]    (first build row's payload words)
+//   direct  dense keys (a range below twice the rows, the surrogate key of a
+//           dimension table): slot = key - min; the probe loads the slot's
+//           count, no key array, no bucket scan;
+//   hashed  4-slot buckets, Fibonacci-hashed bucket index; slots fill in order
+//           inside a bucket and spill to the next bucket (linear probing by
+//           buckets), so one 32-byte load of the bucket's keys settles almost
+//           every probe.  The key INT64_MIN, whose image is the empty marker,
+//           lives in slot 0 of an extra side bucket.
 //
-// Slots fill in order inside a bucket and spill to the next bucket (linear
-// probing by buckets), so one 32-byte load of sector 0 settles almost every
-// probe: probe chains stay short, the warp does not wait for a long tail.  A
-// key that occurs more than once in the build chains its later rows through
+// A key that occurs more than once in the build chains its later rows through
 // chain[slot] / next[row] (row + 1, 0 ends the chain; pushed with atomicExch)
-// and their payloads are read from the build columns.  The key INT64_MIN,
-// whose image is the empty marker, lives in slot 0 of an extra side bucket.
-// The default load factor is 0.5, below Hive's hive.hashtable.loadfactor
-// (0.75): at 0.75 more full buckets send a probe on to the next bucket, and
-// the 60M-row probe measured 7% slower.  The 1.5M-key table is then 1M
-// buckets: a 32 MB key array (all the count pass reads), 32 MB of (first row,
-// count) and 64 MB of payload words, probed while the keys and results stream
-// with evict-first loads and stores.
+// and their payloads are read from the build columns.  The default load
+// factor is 0.5, below Hive's hive.hashtable.loadfactor (0.75): at 0.75 more
+// full buckets send a probe on to the next bucket, and the 60M-row probe
+// measured 7% slower.  Keys and results stream with evict-first loads and
+// stores.
 //
 // The probe counts, then writes (two passes over fixed chunks of probe rows,
 // no ordering dependency between CTAs):
-//   J2a  count: each CTA takes a chunk, loads its keys, issues the key-sector
+//   J2a  count: each CTA takes a chunk, loads its keys, issues the table
 //        loads of all its rows together, stores each row's slot (-1 = no
-//        match) and the chunk's output-row count;
-//   J2b  scan: one CTA turns the chunk counts into output offsets;
-//   J2c  write: each CTA re-reads its chunk's slots, loads each matching
-//        slot's payload sector, scans the rows' output counts inside the
-//        chunk and writes (probe row, build row, payloads) at its offset, in
-//        probe-row order.
+//        match) and each warp's output-row count (a warp covers consecutive
+//        rows of the chunk);
+//   J2b  scan: the warp counts become output offsets (a multi-CTA look-back
+//        scan);
+//   J2c  write: each warp re-reads its rows' slots, loads each matching
+//        slot's payload words, scans its rows' output counts and writes
+//        (probe row, build row, payloads) at its offset, in probe-row order.
+// Neither pass takes a CTA barrier per chunk.
 #include <algorithm>
 
 #include "ghb_ctx.hpp"
 
 namespace ghb {
 
-// Slot s = bucket * 4 + index.  The slots' fields live in three arrays, so
-// each probe pass reads one dense array: the count pass only keys (4 per
-// bucket = one 32-byte sector; 16 MB for 1.5M keys), the write pass the
-// payload words and, when it needs them, the (first row, count) pairs.
+// Slot s = bucket * 4 + index (a direct table: key - min).  The slots' fields
+// live in three arrays, so each probe pass reads one dense array: the hashed
+// count pass only keys (4 per bucket = one 32-byte sector), the direct one
+// only the counts, the write pass the payload words and, when it needs them,
+// the (first row, count) pairs.
 //   key[s]   uint64 key image (flip_i64 of the key, 0 = empty)
 //   meta[s]  int2 {first build row + 1, build rows with this key}
 //   pay[s]   ulonglong2, the first build row's inline payload words
@@ -243,7 +247,8 @@ struct ProbeParams {
   int32_t* out_brow;
   int64_t n, nchunks, cap;
   int32_t* slot_of_row;    // [n] slot (bucket * 4 + index) of the row's key, -1 = no match
-  int64_t* chunk_count;    // [nchunks] output rows of each chunk, then its offset
+  int64_t* chunk_count;    // [nchunks * warps per CTA] output rows of each warp's rows of a
+                           // chunk (a warp covers 32 * IT consecutive rows), then their offset
   int64_t* d_out_rows;
   int32_t* status;
   int64_t build_rows;      // with slots: the table's layout (join_layout of stats)
@@ -287,7 +292,6 @@ __global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
   const JoinLayout L = join_layout(p.stats, p.build_rows, p.slots);
   if (!L.direct) return;
-  __shared__ uint64_t s_warp[TH / 32];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;
@@ -332,14 +336,7 @@ __global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
       }
     }
     for (int o = 16; o > 0; o >>= 1) m_sum += __shfl_down_sync(0xffffffffu, m_sum, o);
-    if (lane == 0) s_warp[warp] = m_sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint64_t t = 0;
-      for (int w = 0; w < TH / 32; w++) t += s_warp[w];
-      p.chunk_count[c] = (int64_t)t;
-    }
-    __syncthreads();
+    if (lane == 0) p.chunk_count[c * (TH / 32) + warp] = (int64_t)m_sum;
   }
 }
 
@@ -349,7 +346,6 @@ template <int TH, int IT, bool KEY_INT, bool NULLABLE>
 __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
-  __shared__ uint64_t s_warp[kJThreads / 32];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;   // every key once: a match is one output row
@@ -424,14 +420,7 @@ __global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p
       }
     }
     for (int o = 16; o > 0; o >>= 1) m_sum += __shfl_down_sync(0xffffffffu, m_sum, o);
-    if (lane == 0) s_warp[warp] = m_sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint64_t t = 0;
-      for (int w = 0; w < kJThreads / 32; w++) t += s_warp[w];
-      p.chunk_count[c] = (int64_t)t;
-    }
-    __syncthreads();
+    if (lane == 0) p.chunk_count[c * (kJThreads / 32) + warp] = (int64_t)m_sum;
   }
 }
 
@@ -636,8 +625,6 @@ template <int TH, int IT>
 __global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
   if (!(p.lean && p.out_brow == nullptr && p.stats[1] <= 1)) return;
-  __shared__ uint32_t s_warp_tot[TH / 32];
-  __shared__ uint32_t s_warp_excl[TH / 32];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   int32_t next_s[IT];
@@ -666,19 +653,7 @@ __global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
       excl[k] = running + __popc(bal & ((1u << lane) - 1u));
       running += __popc(bal);
     }
-    if (lane == 0) s_warp_tot[warp] = running;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t v = lane < TH / 32 ? s_warp_tot[lane] : 0;
-      uint32_t incl = v;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (lane < TH / 32) s_warp_excl[lane] = incl - v;
-    }
-    __syncthreads();
-    const int64_t wpos = p.chunk_count[c] + s_warp_excl[warp];
+    const int64_t wpos = p.chunk_count[c * (TH / 32) + warp];   // this warp's offset
 #pragma unroll
     for (int k = 0; k < IT; k++) {
       if (s[k] < 0) continue;
@@ -697,7 +672,6 @@ __global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
         if (p.obp[j].is_null) p.obp[j].is_null[pos] = 0;
       }
     }
-    __syncthreads();
   }
 }
 
@@ -706,8 +680,6 @@ __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
   if (p.lean && p.out_brow == nullptr && p.stats[1] <= 1) return;   // join_write_lean_kernel's case
-  __shared__ uint32_t s_warp_tot[kJThreads / 32];
-  __shared__ uint32_t s_warp_excl[kJThreads / 32];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;
@@ -769,19 +741,7 @@ __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
       excl[k] = running + incl - (uint32_t)m;
       running += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (lane == 0) s_warp_tot[warp] = running;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t v = lane < kJThreads / 32 ? s_warp_tot[lane] : 0;
-      uint32_t incl = v;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (lane < kJThreads / 32) s_warp_excl[lane] = incl - v;
-    }
-    __syncthreads();
-    const int64_t wpos = p.chunk_count[c] + s_warp_excl[warp];
+    const int64_t wpos = p.chunk_count[c * (kJThreads / 32) + warp];   // this warp's offset
 #pragma unroll
     for (int k = 0; k < kJItems; k++) {
       if (mult[k] == 0) continue;
@@ -805,7 +765,6 @@ __global__ void __launch_bounds__(TH) join_write_kernel(ProbeParams p) {
         }
       }
     }
-    __syncthreads();
   }
 }
 
@@ -930,8 +889,9 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
 // Scratch one probe of n rows needs (slot per row, count per chunk).
 size_t join_probe_scratch_bytes(int64_t n) {
   int64_t nchunks = (n + kChunk - 1) / kChunk;
+  // a count per warp of each chunk: 16 warps at most (512-thread CTAs)
   return (((size_t)std::max<int64_t>(n, 1) * 4 + 255) & ~(size_t)255) +
-         (((size_t)std::max<int64_t>(nchunks, 1) * 8 + 255) & ~(size_t)255) + 512;
+         (((size_t)std::max<int64_t>(nchunks, 1) * 16 * 8 + 255) & ~(size_t)255) + 512;
 }
 
 int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column* probe_key,
@@ -998,11 +958,12 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
     GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_out_rows, 0, sizeof(int64_t), stream));
     return GHB_OK;
   }
-  if ((st = scratch_alloc(ctx, (size_t)p.n * 4, (void**)&p.slot_of_row, stream))) return st;
-  if ((st = scratch_alloc(ctx, (size_t)p.nchunks * 8, (void**)&p.chunk_count, stream))) return st;
   // CTA shape (threads x rows per thread, one 1024-row chunk either way),
   // chosen by the build's ghb_join_cfg.block_threads
   const int threads = t->probe_threads == 128 || t->probe_threads == 512 ? t->probe_threads : 256;
+  const int64_t nunits = p.nchunks * (threads / 32);   // a count per warp of each chunk
+  if ((st = scratch_alloc(ctx, (size_t)p.n * 4, (void**)&p.slot_of_row, stream))) return st;
+  if ((st = scratch_alloc(ctx, (size_t)nunits * 8, (void**)&p.chunk_count, stream))) return st;
   const bool kint = probe_key->type == GHB_INT, knull = probe_key->null_mode != GHB_NULLS_NONE;
   void (*count_kernel)(ProbeParams) = nullptr;
   void (*write_kernel)(ProbeParams) = nullptr;
@@ -1029,13 +990,13 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   count_direct<<<grid, threads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
-  if (p.nchunks <= 4096) {
-    join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, p.nchunks, d_out_rows);
+  if (nunits <= 4096) {
+    join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, nunits, d_out_rows);
   } else {
     ScanParams sp;
     sp.counts = p.chunk_count;
-    sp.n = p.nchunks;
-    sp.ntiles = (p.nchunks + 1023) / 1024;
+    sp.n = nunits;
+    sp.ntiles = (nunits + 1023) / 1024;
     sp.d_total = d_out_rows;
     if ((st = lookback_prepare(ctx, sp.ntiles, &sp.epoch, stream))) return st;
     sp.lb = ctx->lb_status;
