@@ -77,3 +77,26 @@ def test_literals_are_not_part_of_the_signature():
     assert a == b
     c = _source(abi.Pred.leaf(abi.FILTER_GT, 3, a=10), cols, keys, aggs)
     assert c != a
+
+
+def test_rows_and_warp_combine_are_in_the_signature():
+    """The folder's rows per thread and warp-combine mode are template
+    arguments: a single call fixes warp combining (0 or 1), a batch decides it
+    per instance at run time (2), a global aggregate never uses it."""
+    pred, cols, keys, aggs = CASES["fact"]
+    single = _source(pred, cols, keys, aggs)
+    batch = _source(pred, cols, keys, aggs, batch=True)
+    glob = _source(pred, cols, [], aggs)
+
+    def sig_args(src):
+        head = src.split(b"SigFolder<", 1)[1].split(b",")
+        return int(head[0]), int(head[1]), head[2].strip()
+
+    rows, wagg, keyed = sig_args(single)
+    assert 1 <= rows <= 4 and wagg in (0, 1) and keyed == b"true"
+    _, wagg_b, _ = sig_args(batch)
+    assert wagg_b == 2
+    _, wagg_g, keyed_g = sig_args(glob)
+    assert wagg_g == 0 and keyed_g == b"false"
+    for s in (single, batch, glob):
+        _compile(s)
