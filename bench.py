@@ -7,9 +7,22 @@ Headline workload (one GPU's worth, weak-scaled over N ranks): the inner hash
 equi-join of a 1.5M-row build side (unique int64 keys, int64 + double
 payloads) with a 60M-row probe side (int64 foreign key, 5% misses, int32
 payload), emitting every (probe row id, build int64 payload, build double
-payload) match.  One step = build the table + probe all 60M rows.  The fused
-filter + group-by (6M-row fact table) and the 60M-row (d, k) sort are timed
-too and reported under "ops".
+payload) match.  One step = build the table + probe all 60M rows.
+
+Before the headline line (the last line, the only one with "metric"), one
+JSON line per further operator workload (single GPU, N = 1 only), each with
+its device-timed rows/s, its HBM roofline, a CPU baseline (the C++
+restatement of Hive's vectorized operator at T = 1 and T = all host threads)
+and an end-to-end figure through the host-buffer entry point:
+  - "filter_groupby": filter d < 1263 + GROUP BY k over the 6M-row fact table,
+    with the error of each DOUBLE SUM/AVG against an FP64 compensated sum;
+  - "join_hashed": the headline join with the keys spread over the int64
+    range (the hashed table instead of the direct one);
+  - "sort": ORDER BY (d, k) of 60M rows, uniform and Zipf(0.99) k;
+  - "batched_groupby": 512 filter + group-by instances in one launch against
+    one call per instance;
+  - "served_mix": the served mixed operator stream against serial per-call
+    execution with the same resident tables and output sets.
 
 Timing: CUDA events on the launching stream, W untimed warm-up steps, then K
 timed steps between a barrier + device synchronise on both sides; the
@@ -20,7 +33,8 @@ synthetic data of the workload shapes.
 
 `--impl reference` times the CPU restatement of Hive's vectorized map-join
 (the oracle port: HashCodeUtil hash, triangular probing, load factor 0.75)
-on all host threads over a bounded sample of the same workload.
+on all host threads over the same workload: one build + all 60M probe rows
+per step.
 """
 import argparse
 import json
@@ -41,6 +55,17 @@ N_PROBE = 60_000_000
 N_FACT = 6_000_000
 N_SORT = 60_000_000
 METRIC = "GPU rows/s (inner hash join: probe rows per second, build + probe per step)"
+JOIN_OUTPUT_ROWS = 56_999_683   # matches of the rank-0 probe (seeded), for the shared config
+
+
+def join_config(world):
+    """The workload both arms time (identical dicts, so the arms compare)."""
+    return {"workload": "inner hash join, build 1.5M unique int64 keys + int64/double payloads, "
+                        "probe 60M int64 keys (5% miss), output (probe row, int64 payload, double "
+                        "payload) per match",
+            "build_rows": N_BUILD, "probe_rows": N_PROBE, "output_rows": JOIN_OUTPUT_ROWS,
+            "parallelism": "dp%d (replicated build, sharded probe, no collective)" % world,
+            "l2": "inputs larger than L2 (probe key column 480 MB)"}
 
 
 def load_peaks():
@@ -62,6 +87,14 @@ def profile_traffic(name):
             if line.startswith("dram_bytes_per_launch:"):
                 return float(line.split(":")[1])
     return None
+
+
+def roofline(nbytes, ms, peak, peak_kind, **extra):
+    ach = nbytes / (ms / 1e3) / 1e9
+    d = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+         "peak_kind": peak_kind, "bytes_per_launch": int(nbytes), "ms_per_launch": ms}
+    d.update(extra)
+    return d
 
 
 class ClockSampler:
@@ -109,11 +142,11 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def dist_init(gpus):
+def dist_init(gpus, impl):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and impl == "ours":   # the CPU arm needs no collective
         import datetime
 
         import torch.distributed as dist
@@ -137,46 +170,91 @@ def max_over_ranks(world, v, device):
     return float(t.item())
 
 
-# ----------------------------------------------------------------- CPU arm
-def cpu_join_sample(threads, probe_rows, seed_idx=1):
-    """Oracle port of Hive's map-join on a sample: full build, probe_rows rows."""
-    from ghive_b200 import workloads
-    from oracle import oracle
-    (bkey, bpay), (fk, _) = workloads.join_tables(N_BUILD, probe_rows, seed_idx=seed_idx)
+def timed_cpu(fn):
     t0 = time.perf_counter()
-    prow, outs = oracle.hash_join_mt(threads, bkey, fk, bpay)
-    dt = time.perf_counter() - t0
-    return probe_rows / dt, dt, len(prow)
+    r = fn()
+    return time.perf_counter() - t0, r
 
 
+def host_threads():
+    return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------- CPU arm
 def run_reference(args, world, rank):
+    """The C++ restatement of Hive's map-join (build + probe of all 60M rows
+    per step) on every host thread; rank 0 alone runs it."""
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    sample = 6_000_000
-    vals = []
+    from ghive_b200 import workloads
+    from oracle import oracle
+    threads = host_threads()
+    (bkey, bpay), (fk, _) = workloads.join_tables(N_BUILD, N_PROBE, seed_idx=1)
+    secs, rows = [], None
     for i in range(args.warmup + args.steps):
-        v, dt, rows = cpu_join_sample(threads, sample)
+        dt, (prow, _) = timed_cpu(lambda: oracle.hash_join_mt(threads, bkey, fk, bpay, cap=N_PROBE))
+        rows = len(prow)
         if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+            secs.append(dt)
+    step_s = statistics.median(secs)
+    dt1, _ = timed_cpu(lambda: oracle.hash_join_mt(1, bkey, fk, bpay, cap=N_PROBE))
+    value = N_PROBE / step_s
+    sample = ("each step: build 1.5M rows + probe all 60M probe rows (Hive "
+              "VectorMapJoinFastLongHashTable + VectorMapJoinInnerLongOperator restated in C++), "
+              "%d matches; T=1: %.3g rows/s (one step, %.1f s)" % (rows, N_PROBE / dt1, dt1))
+    if world > 1:
+        sample += "; one rank's 60M-row probe shard per step (every shard has this shape)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": sample / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded PCG64)",
-            "config": {"workload": "inner hash join, build 1.5M unique int64 keys + int64/double "
-                                   "payloads, probe 60M int64 keys (5% miss)",
-                       "build_rows": N_BUILD, "probe_rows": N_PROBE,
-                       "parallelism": "host threads"},
+            "config": join_config(world),
             "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": "build 1.5M rows + probe %d of the 60M probe rows per step "
-                                       "(Hive VectorMapJoinFastLongHashTable restated, C++)" % sample},
-            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": sample, "t1_value": N_PROBE / dt1},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ----------------------------------------------------------------- GPU arm
+def pinned(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+
+def pinned_outs(types, cap, with_nulls=True):
+    """Host output columns in pinned memory (the D2H copies run at DMA speed)."""
+    import torch
+
+    from ghive_b200 import abi
+    from ghive_b200.ops import _Outs
+    o = _Outs(types, cap, None, with_nulls=with_nulls)
+    keep = []
+    for j, t in enumerate(types):
+        buf = torch.empty(max(1, cap), dtype={abi.LONG: torch.int64, abi.DOUBLE: torch.float64,
+                                              abi.INT: torch.int32}[t]).pin_memory()
+        nb = torch.empty(max(1, cap), dtype=torch.uint8).pin_memory() if with_nulls else None
+        o.cols[j] = (buf.numpy(), None if nb is None else nb.numpy())
+        o.arr[j].data = buf.data_ptr()
+        o.arr[j].is_null = None if nb is None else nb.data_ptr()
+        keep += [buf, nb]
+    o._pinned = keep
+    return o
+
+
+def probe_outs(types, cap, dev):
+    """Device outputs of a probe emitting (probe row id, build payloads)."""
+    import torch
+
+    from ghive_b200.ops import _Outs
+    ob = _Outs(types, cap, dev, with_nulls=False)
+    op = _Outs([], cap, dev)
+    prow = torch.empty(cap, dtype=torch.int32, device=dev)
+    d_rows = torch.zeros(1, dtype=torch.int64, device=dev)
+    return (ob, op, prow, None, d_rows)
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -195,27 +273,17 @@ def run_ours(args, world, rank, local):
     d_bpay = [torch.from_numpy(c).to(dev) for c in bpay]
     d_fk = torch.from_numpy(fk).to(dev)
     cap = N_PROBE
-    outs = None
+    outs = probe_outs([abi.LONG, abi.DOUBLE], cap, dev)
+    d_rows = outs[4]
 
     def join_step(ev=None):
-        nonlocal outs
         t = ctx.join_build(d_bkey, build_payload=d_bpay)
         if ev:
             ev[0].record(stream)
-        outs = ctx.join_probe(t, d_fk, abi.INNER_JOIN, capacity=cap, rowids=False, sync=False,
-                              outs=outs)
+        ctx.join_probe(t, d_fk, abi.INNER_JOIN, capacity=cap, rowids=False, sync=False, outs=outs)
         if ev:
             ev[1].record(stream)
         t.free()
-        return outs
-
-    # probe output: probe row id (int32) is written through the rowid slot
-    from ghive_b200.ops import _Outs
-    ob = _Outs([abi.LONG, abi.DOUBLE], cap, dev, with_nulls=False)
-    op = _Outs([], cap, dev)
-    prow = torch.empty(cap, dtype=torch.int32, device=dev)
-    d_rows = torch.zeros(1, dtype=torch.int64, device=dev)
-    outs = (ob, op, prow, None, d_rows)
 
     for _ in range(args.warmup):
         join_step()
@@ -241,80 +309,70 @@ def run_ours(args, world, rank, local):
     probe_ms = statistics.mean(a.elapsed_time(b) for a, b in probe_ev)
     value = world * N_PROBE / (step_ms / 1e3)
     probe_bytes = N_PROBE * 8 + rows_out * 20 + N_BUILD * 16
-    achieved = probe_bytes / (probe_ms / 1e3) / 1e9
 
     # ---------------- e2e: host buffers through the C ABI entry point
-    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
-    h_bkey, h_bpay, h_fk = pin(bkey), [pin(c) for c in bpay], pin(fk)
-    from ghive_b200.ops import _Outs as HOuts
-    hob = HOuts([abi.LONG, abi.DOUBLE], cap, None, with_nulls=False)
+    h_bkey, h_bpay, h_fk = pinned(bkey), [pinned(c) for c in bpay], pinned(fk)
+    hob = pinned_outs([abi.LONG, abi.DOUBLE], cap, with_nulls=False)
+    hop = pinned_outs([], cap)
     hprow = torch.empty(cap, dtype=torch.int32).pin_memory().numpy()
-    hob_pinned = []  # pinned output columns: the D2H copies run at DMA speed
-    for j, t in enumerate((abi.LONG, abi.DOUBLE)):
-        buf = torch.empty(cap, dtype=torch.int64 if t == abi.LONG else torch.float64).pin_memory()
-        hob.cols[j] = (buf.numpy(), None)
-        hob.arr[j].data = buf.data_ptr()
-        hob_pinned.append(buf)
-    hop = HOuts([], cap, None)
     e2e_steps = max(1, min(args.steps, 5))
-    for _ in range(1):
+    for _ in range(2):
         ctx.hash_join_host(h_bkey, h_fk, abi.INNER_JOIN, build_payload=h_bpay, capacity=cap,
                            outs=(hob, hop, hprow, None))
-    dstream = torch.cuda.default_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
     torch.cuda.synchronize()
-    e0.record(dstream)
+    t0 = time.perf_counter()
     for _ in range(e2e_steps):
         r = ctx.hash_join_host(h_bkey, h_fk, abi.INNER_JOIN, build_payload=h_bpay, capacity=cap,
                                outs=(hob, hop, hprow, None))
-    e1.record(dstream)
     torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
     barrier(world)
-    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / e2e_steps, dev)
+    e2e_ms = max_over_ranks(world, e2e_ms, dev)
     assert r["rows"] == rows_out
     e2e = {"value": world * N_PROBE / (e2e_ms / 1e3), "unit": "rows/s",
            "h2d_bytes_per_step": int(bkey.nbytes + sum(c.nbytes for c in bpay) + fk.nbytes),
            "d2h_bytes_per_step": int(rows_out * 20 + 8), "ms_per_step": e2e_ms,
-           "api": "ghb_hash_join_host (pinned host columns)"}
-    del d_fk, outs, ob, prow
+           "api": "ghb_hash_join_host (pinned host columns; host clock, returns with the "
+                  "results in host memory)"}
+    del d_fk, outs
     torch.cuda.empty_cache()
 
-    ops = {}
-    if not args.headline_only:
-        ops["filter_groupby"] = bench_groupby(ctx, args, dev, stream, peak)
-        ops["sort"] = bench_sort(ctx, args, dev, stream, peak)
+    lines = []
+    if world == 1 and not args.headline_only:
+        lines.append(bench_groupby(ctx, args, dev, stream, peak, peak_kind))
+        lines.append(bench_join_hashed(ctx, args, dev, stream, peak, peak_kind))
+        lines.append(bench_sort(ctx, args, dev, stream, peak, peak_kind))
         if not args.skip_batched:
-            ops["batched_groupby"] = bench_batched(ctx, args, dev, stream, peak)
+            lines.append(bench_batched(ctx, args, dev, stream, peak, peak_kind))
         if not args.skip_served:
-            ops["served_mix"] = bench_served(ctx, args, dev)
+            lines.append(bench_served(ctx, args, dev))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        v, dt, _ = cpu_join_sample(threads, 12_000_000)
-        cpu = {"value": v, "unit": "rows/s", "cores": threads, "kind": "port",
-               "sample": "build 1.5M rows + probe 12M of the 60M probe rows "
-                         "(Hive VectorMapJoinFastLongHashTable restated, C++), %.1f s" % dt}
+        from oracle import oracle
+        threads = host_threads()
+        dt, _ = timed_cpu(lambda: oracle.hash_join_mt(threads, bkey, fk, bpay, cap=N_PROBE))
+        cpu = {"value": N_PROBE / dt, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": "one full step: build 1.5M rows + probe all 60M probe rows (Hive "
+                         "VectorMapJoinFastLongHashTable restated, C++), %.2f s" % dt}
 
     if rank == 0:
+        for ln in lines:
+            print(json.dumps(ln), flush=True)
+        cfg = join_config(world)
+        cfg["output_rows"] = rows_out if world == 1 else cfg["output_rows"]
         line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-                "data": "synthetic (seeded PCG64)",
-                "config": {"workload": "inner hash join, build 1.5M unique int64 keys + int64/double "
-                                       "payloads, probe 60M int64 keys (5% miss), output (probe row, "
-                                       "int64 payload, double payload) per match",
-                           "build_rows": N_BUILD, "probe_rows": N_PROBE, "output_rows": rows_out,
-                           "parallelism": "dp%d (replicated build, sharded probe, no collective)" % world,
-                           "l2": "inputs larger than L2 (probe key column 480 MB)"},
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "peak_kind": peak_kind,
-                             "kernel": "join probe: count + scan + write passes (one ghb_join_probe call)",
-                             "bytes_per_launch": probe_bytes, "ms_per_launch": probe_ms,
-                             "traffic": profile_traffic("join_probe_60M.md")},
+                "data": "synthetic (seeded PCG64)", "config": cfg,
+                "roofline": roofline(probe_bytes, probe_ms, peak, peak_kind,
+                                     kernel="join probe: count + scan + write passes (one "
+                                            "ghb_join_probe call)",
+                                     traffic=profile_traffic("join_probe_60M.md")),
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary(), "ops": ops}
+                "clocks": clk.summary(),
+                "ops": [ln["op"] for ln in lines]}
         print(json.dumps(line), flush=True)
     ctx.close()
     return 0
@@ -324,18 +382,38 @@ def flush_l2(buf):
     buf.add_(1)
 
 
-def bench_groupby(ctx, args, dev, stream, peak):
+def _double_errors(gpu_keys, gpu_aggs, ok, comp, out_types):
+    """Relative error of each DOUBLE SUM/AVG result against the oracle's FP64
+    Neumaier compensated sum (groups matched by key)."""
+    gk = gpu_keys[0][0].cpu().numpy()
+    okk = ok[0][0]
+    go, oo = np.argsort(gk, kind="stable"), np.argsort(okk, kind="stable")
+    errs = []
+    from ghive_b200 import abi
+    for j, t in enumerate(out_types):
+        if t != abi.DOUBLE or not np.any(comp[j] != 0):
+            continue
+        g = gpu_aggs[j][0].cpu().numpy()[go]
+        c = comp[j][oo]
+        errs.append(np.abs(g - c) / np.maximum(np.abs(c), 1e-300))
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    return {"results": int(e.size), "max_rel": float(e.max()) if e.size else None,
+            "median_rel": float(np.median(e)) if e.size else None,
+            "reference": "FP64 Neumaier compensated sum per group (CPU oracle)"}
+
+
+def bench_groupby(ctx, args, dev, stream, peak, peak_kind):
     import torch
 
-    from ghive_b200 import workloads
+    from ghive_b200 import abi, workloads
     cols = workloads.fact_table(N_FACT, seed_idx=0)
     dcols = [torch.from_numpy(c).to(dev) for c in cols]
-    pred = workloads.fact_predicate()
+    pred, aggs = workloads.fact_predicate(), workloads.AGGS_FACT
+    out_types = [abi.LONG, abi.LONG, abi.DOUBLE, abi.DOUBLE, abi.INT, abi.INT]
     flush = torch.zeros(64 << 20, dtype=torch.float32, device=dev)  # 256 MB
     res = None
     for _ in range(args.warmup):
-        res = ctx.filter_groupby(pred, dcols, [0], workloads.AGGS_FACT, capacity=1000,
-                                 max_groups=1000, sync=False)
+        res = ctx.filter_groupby(pred, dcols, [0], aggs, capacity=1000, max_groups=1000, sync=False)
     ctx.sync()
     times = []
     for _ in range(max(args.steps, 10)):
@@ -345,34 +423,123 @@ def bench_groupby(ctx, args, dev, stream, peak):
         torch.cuda._sleep(300_000)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        res = ctx.filter_groupby(pred, dcols, [0], workloads.AGGS_FACT, capacity=1000,
-                                 max_groups=1000, sync=False)
+        res = ctx.filter_groupby(pred, dcols, [0], aggs, capacity=1000, max_groups=1000, sync=False)
         b.record(stream)
         times.append((a, b))
     ctx.sync()
     groups = int(res[1].item())
     ms = statistics.median(x.elapsed_time(y) for x, y in times)
-    nbytes = N_FACT * 24 + groups * 48
-    ach = nbytes / (ms / 1e3) / 1e9
-    return {"workload": "filter d<1263 + GROUP BY k (1000 groups): COUNT(*), SUM(qty), SUM(price), "
-                        "AVG(price), MIN(d), MAX(d) over 6M rows",
-            "rows_per_s": N_FACT / (ms / 1e3), "ms": ms, "groups": groups,
-            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "bytes": nbytes, "l2": "flushed before each launch",
-                         "traffic": profile_traffic("groupby_fold_fact6M.md")}}
+    # the whole call from the host: argument checks, signature lookup, launches
+    ctx.sync()
+    t0 = time.perf_counter()
+    reps = 20
+    for _ in range(reps):
+        res = ctx.filter_groupby(pred, dcols, [0], aggs, capacity=1000, max_groups=1000, sync=False)
+    ctx.sync()
+    call_ms = (time.perf_counter() - t0) / reps * 1e3
+    gk, ga, _ = ctx.filter_groupby(pred, dcols, [0], aggs, capacity=1000, max_groups=1000)
+
+    # e2e: pinned host columns through ghb_filter_groupby_host
+    hcols = [pinned(c) for c in cols]
+    houts = pinned_outs([abi.INT] + out_types, 1000)   # key k (int32), then the aggregates
+    ctx.filter_groupby_host(pred, hcols, [0], aggs, 1000, max_groups=1000, outs=houts)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        ctx.filter_groupby_host(pred, hcols, [0], aggs, 1000, max_groups=1000, outs=houts)
+    e2e_ms = (time.perf_counter() - t0) / 5 * 1e3
+
+    out = {"op": "filter_groupby",
+           "workload": "filter d<1263 + GROUP BY k (1000 groups): COUNT(*), SUM(qty), SUM(price), "
+                       "AVG(price), MIN(d), MAX(d) over 6M rows",
+           "value": N_FACT / (ms / 1e3), "unit": "rows/s", "ms": ms, "groups": groups,
+           "host_call_ms": call_ms,
+           "roofline": roofline(N_FACT * 24 + groups * 48, ms, peak, peak_kind,
+                                kernel="fold + finalize (one ghb_filter_groupby call)",
+                                l2="flushed before each launch",
+                                traffic=profile_traffic("groupby_fold_fact6M.md")),
+           "e2e": {"value": N_FACT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+                   "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)),
+                   "d2h_bytes_per_step": int(groups * 44 + 8),
+                   "api": "ghb_filter_groupby_host (pinned host columns)"}}
+    if not args.no_cpu:
+        from oracle import oracle
+        threads = host_threads()
+        t1, _ = timed_cpu(lambda: oracle.filter_groupby(pred, cols, [0], aggs, cap=1000))
+        tn, _ = timed_cpu(lambda: oracle.filter_groupby(pred, cols, [0], aggs, cap=1000,
+                                                        threads=threads))
+        out["cpu_baseline"] = {"value": N_FACT / tn, "unit": "rows/s", "cores": threads,
+                               "kind": "port", "t1_value": N_FACT / t1,
+                               "sample": "the whole 6M-row workload (Hive VectorFilterOperator + "
+                                         "VectorGroupByOperator hash mode restated in C++, 1024-row "
+                                         "batches); T=all: row ranges with private hash maps, merged"}
+        # the checker: the oracle's compensated sums beside the GPU's results
+        ok, oa, comp = oracle.filter_groupby(pred, cols, [0], aggs, cap=1000, with_comp=True)
+        out["double_error_vs_compensated_sum"] = _double_errors(gk, ga, ok, comp, out_types)
+    del dcols, flush
+    torch.cuda.empty_cache()
+    return out
 
 
-def bench_sort(ctx, args, dev, stream, peak):
+def bench_join_hashed(ctx, args, dev, stream, peak, peak_kind):
+    """The headline join with keys spread over the int64 range: the hashed
+    table layout (bucketized open addressing) instead of the direct one."""
     import torch
 
-    from ghive_b200 import workloads
-    out = {}
+    from ghive_b200 import abi, workloads
+    (bkey, bpay), (fk, _) = workloads.join_tables(N_BUILD, N_PROBE, seed_idx=1, sparse=True)
+    d_bkey = torch.from_numpy(bkey).to(dev)
+    d_bpay = [torch.from_numpy(c).to(dev) for c in bpay]
+    d_fk = torch.from_numpy(fk).to(dev)
+    outs = probe_outs([abi.LONG, abi.DOUBLE], N_PROBE, dev)
+    t = ctx.join_build(d_bkey, build_payload=d_bpay)
+    for _ in range(args.warmup):
+        ctx.join_probe(t, d_fk, abi.INNER_JOIN, capacity=N_PROBE, rowids=False, sync=False,
+                       outs=outs)
+    ctx.sync()
+    ev = []
+    for _ in range(max(3, min(args.steps, 10))):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.join_probe(t, d_fk, abi.INNER_JOIN, capacity=N_PROBE, rowids=False, sync=False,
+                       outs=outs)
+        b.record(stream)
+        ev.append((a, b))
+    ctx.sync()
+    rows_out = int(outs[4].item())
+    _, _, slots = t.info()
+    t.free()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    nbytes = N_PROBE * 8 + rows_out * 20 + N_BUILD * 16
+    del d_fk, outs
+    torch.cuda.empty_cache()
+    return {"op": "join_hashed",
+            "workload": "the headline join (1.5M x 60M) with every key passed through a 64-bit "
+                        "bijection (keys spread over the int64 range): hashed table, %d slots"
+                        % slots,
+            "value": N_PROBE / (ms / 1e3), "unit": "rows/s", "ms": ms, "output_rows": rows_out,
+            "roofline": roofline(nbytes, ms, peak, peak_kind,
+                                 kernel="join probe on the hashed table (count + scan + write)",
+                                 traffic=profile_traffic("join_probe_hashed_60M.md"))}
+
+
+def bench_sort(ctx, args, dev, stream, peak, peak_kind):
+    import torch
+
+    from ghive_b200 import abi, workloads
+    out = {"op": "sort",
+           "workload": "ORDER BY (d int32, k int64) ASC, stable, int32 row-id payload, 60M rows"}
     for zipf in (False, True):
         d, k, rowid = workloads.sort_table(N_SORT, zipf=zipf, seed_idx=2)
         dd, dk, dr = (torch.from_numpy(x).to(dev) for x in (d, k, rowid))
         for _ in range(max(1, args.warmup)):
             ctx.sort([dd, dk], payload=[dr], sync=False)
         ctx.sync()
+        l0 = ctx.launches
+        ctx.sort([dd, dk], payload=[dr], sync=False)
+        ctx.sync()
+        # the sort launches a min/max and a histogram kernel, then one kernel
+        # per executed radix pass
+        passes = ctx.launches - l0 - 2
         times = []
         for _ in range(max(3, min(args.steps, 10))):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -382,18 +549,47 @@ def bench_sort(ctx, args, dev, stream, peak):
             times.append((a, b))
         ctx.sync()
         ms = statistics.median(x.elapsed_time(y) for x, y in times)
-        nbytes = N_SORT * 32
-        ach = nbytes / (ms / 1e3) / 1e9
-        out["zipf" if zipf else "uniform"] = {
-            "rows_per_s": N_SORT / (ms / 1e3), "ms": ms,
-            "roofline_lower_bound_32B_per_row": {"achieved": ach, "peak": peak, "frac": ach / peak}}
+        per_pass_bytes = N_SORT * 12 + passes * N_SORT * 24 + N_SORT * 16
+        # e2e: pinned host columns through ghb_sort_host
+        hd, hk, hr = pinned(d), pinned(k), pinned(rowid)
+        hok = pinned_outs([abi.INT, abi.LONG], N_SORT, with_nulls=False)
+        hop = pinned_outs([abi.INT], N_SORT, with_nulls=False)
+        ctx.sort_host([hd, hk], payload=[hr], outs=(hok, hop, None))
+        t0 = time.perf_counter()
+        for _ in range(3):
+            ctx.sort_host([hd, hk], payload=[hr], outs=(hok, hop, None))
+        e2e_ms = (time.perf_counter() - t0) / 3 * 1e3
+        entry = {"value": N_SORT / (ms / 1e3), "unit": "rows/s", "ms": ms, "passes": passes,
+                 "roofline": roofline(N_SORT * 32, ms, peak, peak_kind,
+                                      kernel="whole sort against the 32 B/row lower bound "
+                                             "(read d 4 + k 8 + rowid 4, write 16)"),
+                 "roofline_per_pass_formula": roofline(
+                     per_pass_bytes, ms, peak, peak_kind,
+                     kernel="whole sort against N*12 + P*N*24 + N*16 bytes, P = %d executed "
+                            "radix passes" % passes),
+                 "e2e": {"value": N_SORT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+                         "h2d_bytes_per_step": N_SORT * 16, "d2h_bytes_per_step": N_SORT * 16,
+                         "api": "ghb_sort_host (pinned host columns)"}}
+        if not args.no_cpu:
+            from oracle import oracle
+            threads = host_threads()
+            tn, _ = timed_cpu(lambda: oracle.sort_perm([d, k], threads=threads))
+            s1 = 6_000_000
+            t1, _ = timed_cpu(lambda: oracle.sort_perm([d[:s1], k[:s1]]))
+            entry["cpu_baseline"] = {"value": N_SORT / tn, "unit": "rows/s", "cores": threads,
+                                     "kind": "port", "t1_value": s1 / t1,
+                                     "sample": "T=all: the whole 60M rows (std::stable_sort per "
+                                               "thread chunk + stable merges, BinarySortable "
+                                               "order); T=1: the first 6M rows"}
+        out["zipf" if zipf else "uniform"] = entry
         del dd, dk, dr
         torch.cuda.empty_cache()
-    out["workload"] = "ORDER BY (d int32, k int64) ASC, stable, int32 row-id payload, 60M rows"
+    out["value"] = min(out["uniform"]["value"], out["zipf"]["value"])
+    out["unit"] = "rows/s"
     return out
 
 
-def bench_batched(ctx, args, dev, stream, peak, count=512):
+def bench_batched(ctx, args, dev, stream, peak, peak_kind, count=512):
     """512 filter + group-by instances of uneven size: one captured batch vs
     one ghb_filter_groupby call per instance on the same GPU."""
     import ctypes as C
@@ -472,19 +668,21 @@ def bench_batched(ctx, args, dev, stream, peak, count=512):
     ctx.sync()
     single_counts = np.array([int(k[-1].item()) for _, k in calls])
     parity = bool(np.array_equal(counts, single_counts))
+    b.launch()
+    ctx.sync()
 
     groups = int(counts.sum())
     nbytes = rows * 28 + groups * 52
-    ach = nbytes / (batched_ms / 1e3) / 1e9
-    out = {"workload": "%d filter + GROUP BY instances, rows log-U[1e3,1e7] (%d in all), groups "
+    out = {"op": "batched_groupby",
+           "workload": "%d filter + GROUP BY instances, rows log-U[1e3,1e7] (%d in all), groups "
                        "log-U[10,1e6], Zipf keys, selectivity U[0.01,0.9]; fact-table aggregates"
                        % (count, rows),
+           "value": rows / (batched_ms / 1e3), "unit": "rows/s",
            "instances": count, "rows": rows, "groups": groups,
            "batched": {"ms": batched_ms, "rows_per_s": rows / (batched_ms / 1e3),
                        "launches_per_run": batch_launches,
-                       "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                                    "frac": ach / peak, "bytes": nbytes,
-                                    "l2": "inputs (%.1f GB) larger than L2" % (rows * 28 / 1e9)}},
+                       "roofline": roofline(nbytes, batched_ms, peak, peak_kind,
+                                            l2="inputs (%.1f GB) larger than L2" % (rows * 28 / 1e9))},
            "per_call_sync": {"ms": sync_ms, "rows_per_s": rows / (sync_ms / 1e3)},
            "per_call_async": {"ms": async_ms, "rows_per_s": rows / (async_ms / 1e3),
                               "launches_per_run": call_launches},
@@ -492,6 +690,43 @@ def bench_batched(ctx, args, dev, stream, peak, count=512):
            "speedup_vs_per_call_async": async_ms / batched_ms,
            "group_counts_equal_per_call": parity,
            "create_s": create_s, "plan": b.describe()}
+    if not args.no_cpu:
+        # CPU baseline and the double-error check on a bounded sample: the
+        # first 64 instances, each run by the sequential oracle (Hive order),
+        # the instances spread over every host thread
+        from concurrent.futures import ThreadPoolExecutor
+
+        from oracle import oracle
+        threads = host_threads()
+        sample = list(range(64))
+        hcols = [[c.cpu().numpy() for c in inst[i]["cols"]] for i in sample]
+        srows = sum(specs[i]["rows"] for i in sample)
+
+        def one(j):
+            i = sample[j]
+            return oracle.filter_groupby(workloads.batched_predicate(specs[i]["cut"]), hcols[j], [0],
+                                         aggs, cap=entries[i][2], with_comp=True)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            res = list(ex.map(one, range(len(sample))))
+        dt = time.perf_counter() - t0
+        errs = []
+        types = [abi.LONG, abi.LONG, abi.DOUBLE, abi.DOUBLE, abi.INT, abi.INT]
+        for j, i in enumerate(sample):
+            gk, ga, _ = b.results(i, counts)
+            e = _double_errors(gk, ga, res[j][0], res[j][2], types)
+            if e["results"]:
+                errs.append((e["max_rel"], e["results"]))
+        out["cpu_baseline"] = {"value": srows / dt, "unit": "rows/s", "cores": threads,
+                               "kind": "port",
+                               "sample": "instances 0-63 (%d rows), one sequential Hive group-by "
+                                         "restatement per instance over a %d-thread pool"
+                                         % (srows, threads)}
+        out["double_error_vs_compensated_sum"] = {
+            "results": int(sum(n for _, n in errs)),
+            "max_rel": max(m for m, _ in errs) if errs else None,
+            "sample": "instances 0-63"}
     b.free()
     del inst, entries, calls
     torch.cuda.empty_cache()
@@ -499,7 +734,8 @@ def bench_batched(ctx, args, dev, stream, peak, count=512):
 
 
 def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.8, 0.95)):
-    """Served mixed operator stream against serial per-call execution."""
+    """Served mixed operator stream against serial per-call execution with the
+    same resident tables and the same output sets."""
     import itertools
     from concurrent.futures import ThreadPoolExecutor
 
@@ -536,6 +772,12 @@ def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.
     def sl(cols, s):
         return [c[s["offset"]:s["offset"] + s["rows"]] for c in cols]
 
+    # serial per-call execution with what the server has: the 8 build tables
+    # resident (built once, outside the timing) and each probe emitting (probe
+    # row id, build payloads) without build row ids, as a served probe does
+    tables = [ctx.join_build(k, build_payload=p) for k, p in builds]
+    pouts = probe_outs([abi.LONG, abi.DOUBLE], max_rows, dev)
+
     def run_plain(s):
         pred = workloads.fact_predicate(s["cut"])
         if s["op"] == "groupby":
@@ -545,14 +787,11 @@ def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.
         elif s["op"] == "sort":
             ctx.sort(sl(sortc[:2], s), payload=sl(sortc[2:], s))
         else:
-            key, pay = builds[s["table"]]
-            t = ctx.join_build(key, build_payload=pay)
-            ctx.join_probe(t, sl([probes[s["table"]]], s)[0], abi.INNER_JOIN, capacity=s["rows"],
-                           rowids=True)
-            t.free()
+            ctx.join_probe(tables[s["table"]], sl([probes[s["table"]]], s)[0], abi.INNER_JOIN,
+                           capacity=s["rows"], rowids=False, outs=pouts, sync=False)
+            ctx.sync()
 
-    # serial per-call execution: one request at a time, each returning its
-    # result; a full untimed pass first so the allocators hold their sizes
+    # a full untimed pass first so the allocators hold their sizes
     for s in specs:
         run_plain(s)
     torch.cuda.synchronize()
@@ -564,37 +803,9 @@ def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.
         service.append(time.perf_counter() - a)
     serial_s = time.perf_counter() - t0
     serial_rate = len(specs) / serial_s
-
-    # per call through the host-buffer entry points, the way a Hive task calls
-    # GHive's JNI path: pageable host inputs in, results copied back into host
-    # arrays made per call; a bounded sample of the requests
-    hfact = [c.cpu().numpy() for c in fact]
-    hsort = [c.cpu().numpy() for c in sortc]
-    hprobe = [p.cpu().numpy() for p in probes]
-    hbuild = [(k.cpu().numpy(), [x.cpu().numpy() for x in p]) for k, p in builds]
-
-    def run_host(s):
-        pred = workloads.fact_predicate(s["cut"])
-        if s["op"] == "groupby":
-            ctx.filter_groupby_host(pred, sl(hfact, s), [0], aggs, 1000, max_groups=1000)
-        elif s["op"] == "filter":
-            ctx.filter_host(pred, sl(hfact, s), proj=[0, 1, 2])
-        elif s["op"] == "sort":
-            ctx.sort_host(sl(hsort[:2], s), payload=sl(hsort[2:], s))
-        else:
-            key, pay = hbuild[s["table"]]
-            ctx.hash_join_host(key, sl([hprobe[s["table"]]], s)[0], abi.INNER_JOIN,
-                               build_payload=pay, capacity=s["rows"])
-
-    host_sample = specs[:100]
-    for s in host_sample[:5]:
-        run_host(s)
-    t0 = time.perf_counter()
-    for s in host_sample:
-        run_host(s)
-    host_s = time.perf_counter() - t0
-    host_rows = sum(s["rows"] for s in host_sample)
-    del hfact, hsort, hprobe, hbuild
+    for t in tables:
+        t.free()
+    del pouts
 
     srv = Server(dev.index, slots=8)
     try:
@@ -684,26 +895,23 @@ def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.
                 fin = max(at, fin) + sv
                 slat.append((fin - at) * 1e3)
             name = "%d%%" % round(frac * 100)
-            load[name if name not in load else name + "_again"] = {
+            load[name] = {
                 "offered_requests_per_s": rate,
                 "served": dict(rows_per_s=rows_total / span, queue_wait_p50_ms=float(np.median(qwait)),
                                queue_wait_p99_ms=float(np.percentile(qwait, 99)), **pct(lat)),
                 "serial": dict(rows_per_s=rows_total / max(fin, 1e-9), **pct(slat))}
     finally:
         srv.close()
-    out = {"workload": "%d requests: 40%% filter+group-by, 30%% join probe against 8 resident build "
+    out = {"op": "served_mix",
+           "workload": "%d requests: 40%% filter+group-by, 30%% join probe against 8 resident build "
                        "tables (1e5-1e7 keys), 20%% sort, 10%% filter; rows log-U[1e4,1e8] "
                        "(%d in all), device-resident inputs" % (n_req, rows_total),
+           "value": best, "unit": "rows/s",
            "requests": n_req, "rows": rows_total, "slots": 8,
            "serial": {"rows_per_s": rows_total / serial_s, "ms": serial_s * 1e3,
-                      "note": "one plain operator call at a time, each synchronised; a probe "
-                              "builds its table first"},
-           "serial_host_buffers": {"rows_per_s": host_rows / host_s, "ms": host_s * 1e3,
-                                   "sample": "first %d requests (%d rows)" % (len(host_sample), host_rows),
-                                   "note": "ghb_*_host per call: pageable host inputs, results "
-                                           "copied back, a probe builds its table first"},
+                      "note": "one plain operator call at a time, each synchronised; the same "
+                              "resident build tables and probe output set as the server"},
            "served_saturation": sat, "speedup_vs_serial": best / (rows_total / serial_s),
-           "speedup_vs_serial_host_buffers": best / (host_rows / host_s),
            "latency_under_load": load}
     del fact, sortc, builds, probes
     torch.cuda.empty_cache()
@@ -723,13 +931,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    world, rank, local = dist_init(args.gpus)
+    world, rank, local = dist_init(args.gpus, args.impl)
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)
         return run_ours(args, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 and args.impl == "ours":
             import torch.distributed as dist
             dist.destroy_process_group()
 

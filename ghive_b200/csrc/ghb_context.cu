@@ -263,6 +263,11 @@ int32_t ghb_ctx_destroy(ghb_ctx* ctx) {
   if (ctx->lb_status) cudaFree(ctx->lb_status);
   if (ctx->gb_table) cudaFree(ctx->gb_table);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (cudaStream_t& hs : ctx->hstream)
+    if (hs) cudaStreamDestroy(hs);
+  for (auto& row : ctx->hev)
+    for (cudaEvent_t& e : row)
+      if (e) cudaEventDestroy(e);
   delete ctx;
   return GHB_OK;
 }
@@ -272,6 +277,12 @@ const char* ghb_last_error(const ghb_ctx* ctx) {
 }
 
 int64_t ghb_kernel_launches(const ghb_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int32_t ghb_ctx_set_spin_limit(ghb_ctx* ctx, int32_t polls) {
+  if (!ctx) return GHB_ERR_INVALID;
+  ctx->spin_limit = polls > 0 ? polls : ghb::kSpinLimit;
+  return GHB_OK;
+}
 
 int32_t ghb_sync(ghb_ctx* ctx, void* stream) {
   if (!ctx) return GHB_ERR_INVALID;

@@ -36,6 +36,10 @@ struct ghb_ctx {
   int64_t lb_tiles = 0;
   uint32_t epoch = 0;
 
+  // polls of a not-ready earlier tile before a look-back gives up
+  // (ghb_ctx_set_spin_limit)
+  int32_t spin_limit = ghb::kSpinLimit;
+
   // self-resetting counters: [0] tile claim, [1] finished CTAs, ...
   unsigned long long* d_counters = nullptr;
 
@@ -47,6 +51,11 @@ struct ghb_ctx {
   // pinned staging for the host-buffer entry points
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
+
+  // the host-buffer join's copy-in, compute and copy-out streams and its
+  // per-chunk events (created on first use)
+  cudaStream_t hstream[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t hev[4][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
 
   // Every call of this context runs on one stream (a server slot): its
   // device buffers grow with stream-ordered frees and allocations instead of
@@ -87,6 +96,7 @@ struct ghb_join_table {
   size_t alloc_bytes = 0;
   cudaStream_t stream = 0;    // build stream; the table is released in its order
   bool l2_window = false;
+  int device = 0;             // device of the L2 window
   int32_t probe_threads = 256; // probe CTA size (ghb_join_cfg.block_threads)
 };
 
@@ -125,5 +135,29 @@ int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, in
 int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, PredProg* prog);
 
 inline size_t type_width(int32_t t) { return t == GHB_INT ? 4 : 8; }
+
+// ---- several GROUP BY keys packed into one int64 key (ghb_keypack.cu)
+constexpr int kMaxPackKeys = 8;
+struct KeyOuts {
+  ghb_out_column o[kMaxPackKeys];
+};
+struct KeyPackPlan {
+  int32_t nkeys;
+  ghb_column col[kMaxPackKeys];
+  uint64_t umin[kMaxPackKeys];     // min order image of the key's non-NULL values
+  int8_t vbits[kMaxPackKeys];      // value field width
+  int8_t vshift[kMaxPackKeys];     // value field position
+  int8_t fshift[kMaxPackKeys];     // NULL flag position, -1 when the key has no NULLs
+};
+// Scratch bytes the packing needs beside the group-by itself.
+inline size_t keypack_scratch_bytes(int64_t n, int64_t cap) {
+  return 3 * 8 * kMaxPackKeys + 256 + (((size_t)n * 8 + 255) & ~(size_t)255) +
+         (((size_t)cap * 8 + 255) & ~(size_t)255) + 512;
+}
+int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys,
+                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream);
+int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* packed,
+                       const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
+                       cudaStream_t stream);
 
 }  // namespace ghb

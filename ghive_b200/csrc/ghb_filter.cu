@@ -37,6 +37,7 @@ struct FilterParams {
   uint32_t epoch;
   unsigned long long* counters;  // [0] next tile, [1] finished CTAs
   int32_t* status;
+  int32_t spin_limit;            // look-back polls before GHB_ERR_TIMEOUT
 };
 
 __device__ __forceinline__ void copy_value(const ghb_column& c, const ghb_out_column& o, int64_t row,
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kFiltThreads) filter_kernel(FilterParams p) {
       ((uint32_t*)s_warp_off)[2 * lane + 1] = excl + a;
       uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
       static_assert(kSlots == 64, "scan assumes 64 (item, warp) slots");
-      uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, total, p.status);
+      uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, total, p.status, p.spin_limit);
       if (lane == 0) {
         s_tile_excl = ex;
         if (tile == p.ntiles - 1) *p.d_out_rows = (int64_t)(ex + total);
@@ -150,6 +151,7 @@ int32_t filter_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* c
   p.d_out_rows = d_out_rows;
   p.status = ctx->d_status;
   p.counters = ctx->d_counters;
+  p.spin_limit = ctx->spin_limit;
   if (p.ntiles == 0) {
     GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_out_rows, 0, sizeof(int64_t), stream));
     return GHB_OK;

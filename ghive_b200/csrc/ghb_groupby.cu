@@ -154,7 +154,7 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   int32_t st = validate_columns(ctx, cols, ncols, &n);
   if (st) return st;
   if (nkeys < 0 || nkeys > 1)
-    return set_error(ctx, GHB_ERR_UNSUPPORTED, "nkeys=%d: the device group-by takes 0 or 1 key column", nkeys);
+    return set_error(ctx, GHB_ERR_INVALID, "nkeys=%d: this kernel takes 0 or 1 key column", nkeys);
   if (nkeys == 1 && (!key_cols || key_cols[0] < 0 || key_cols[0] >= ncols))
     return set_error(ctx, GHB_ERR_INVALID, "key column out of range");
   if (naggs > 0 && !aggs) return set_error(ctx, GHB_ERR_INVALID, "aggs is NULL");
@@ -315,6 +315,46 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
                             const ghb_groupby_cfg* cfg, cudaStream_t stream,
                             void* fixed_table, size_t fixed_table_bytes) {
   if (!ctx) return GHB_ERR_INVALID;
+  if (nkeys > 1) {
+    // several key columns: group by their packed int64 value, then unpack
+    if (fixed_table)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d key columns: the allocation-free entry point takes "
+                       "at most one", nkeys);
+    int64_t n = 0;
+    int32_t st = validate_columns(ctx, cols, ncols, &n);
+    if (st) return st;
+    if (!key_cols) return set_error(ctx, GHB_ERR_INVALID, "key_cols is NULL");
+    if (!out) return set_error(ctx, GHB_ERR_INVALID, "out is NULL");
+    if (ncols + 1 > kMaxCols)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d columns and a packed key exceed %d", ncols, kMaxCols);
+    for (int j = 0; j < nkeys; j++) {
+      if (key_cols[j] < 0 || key_cols[j] >= ncols)
+        return set_error(ctx, GHB_ERR_INVALID, "key %d: column %d out of range", j, key_cols[j]);
+      if (out[j].type != cols[key_cols[j]].type || !out[j].data)
+        return set_error(ctx, GHB_ERR_INVALID, "key output %d: type %d (expected %d) or no data", j,
+                         out[j].type, cols[key_cols[j]].type);
+    }
+    if (out_capacity < 1) return set_error(ctx, GHB_ERR_INVALID, "out_capacity must be >= 1");
+    if (ctx->scratch_used == 0 &&
+        (st = scratch_reserve(ctx, keypack_scratch_bytes(n, out_capacity), stream)))
+      return st;
+    int64_t *packed = nullptr, *kout = nullptr;
+    if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 8, (void**)&packed, stream))) return st;
+    if ((st = scratch_alloc(ctx, (size_t)out_capacity * 8, (void**)&kout, stream))) return st;
+    KeyPackPlan plan;
+    if ((st = keypack_prepare(ctx, cols, key_cols, nkeys, n, packed, &plan, stream))) return st;
+    ghb_column pc[kMaxCols];
+    for (int c = 0; c < ncols; c++) pc[c] = cols[c];
+    pc[ncols] = ghb_column{GHB_LONG, GHB_NULLS_NONE, packed, nullptr, nullptr, n};
+    ghb_out_column po[kMaxCols + kMaxAggs + 1];
+    po[0] = ghb_out_column{GHB_LONG, 0, kout, nullptr};
+    for (int i = 0; i < naggs && i < kMaxAggs; i++) po[1 + i] = out[nkeys + i];
+    const int32_t pk = ncols;
+    st = filter_groupby_impl(ctx, pred, pc, ncols + 1, &pk, 1, aggs, naggs, po, out_capacity, d_out_groups,
+                             cfg, stream, nullptr, 0);
+    if (st) return st;
+    return keypack_unpack(ctx, plan, kout, d_out_groups, out_capacity, out, stream);
+  }
   GbSetup su{};
   su.max_groups = (cfg && cfg->max_groups > 0) ? cfg->max_groups : 0;
   su.smem_slots = cfg ? cfg->smem_slots : 0;
@@ -390,6 +430,20 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
   const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>(fin_units(p.C), (int64_t)ctx->num_sms * 8));
   gb_finalize_kernel<<<fgrid, kFinThreads, 0, stream>>>(f);
   GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+// Loads every kernel the fixed-table path can launch (the generic folds and
+// the finalize) and sets their shared-memory attributes, so that a later call
+// of that path loads no code.  CUDA loads kernels lazily, on first launch or
+// first attribute query, and loading one may allocate device memory.
+int32_t preload_fixed_table_kernels(ghb_ctx* ctx) {
+  const void* folds[] = {(const void*)gb_fold_kernel<true, true>, (const void*)gb_fold_kernel<true, false>,
+                         (const void*)gb_fold_kernel<false, true>, (const void*)gb_fold_kernel<false, false>};
+  for (const void* fn : folds)
+    if (int32_t st = ensure_dyn_smem(ctx, fn, 0)) return st;
+  cudaFuncAttributes fa;
+  GHB_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, (const void*)gb_finalize_kernel));
   return GHB_OK;
 }
 

@@ -24,7 +24,7 @@ int32_t join_build_impl(ghb_ctx*, const ghb_column*, const ghb_column*, int32_t,
                         const ghb_join_cfg*, ghb_join_table**, cudaStream_t);
 int32_t join_probe_impl(ghb_ctx*, const ghb_join_table*, const ghb_column*, int32_t,
                         ghb_out_column*, const ghb_column*, int32_t, ghb_out_column*, int32_t*,
-                        int32_t*, int64_t, int64_t*, cudaStream_t);
+                        int32_t*, int64_t, int64_t*, cudaStream_t, int32_t);
 int32_t sort_impl(ghb_ctx*, const ghb_column*, const int32_t*, const int32_t*, int32_t,
                   const ghb_column*, int32_t, ghb_out_column*, ghb_out_column*, int32_t*,
                   const ghb_sort_cfg*, cudaStream_t);
@@ -165,6 +165,7 @@ int32_t ghb_filter_groupby_host(ghb_ctx* ctx, const ghb_predicate* pred, const g
   size_t need = 4096;
   for (int i = 0; i < ncols; i++) need += in_bytes(cols[i]) + 256;
   for (int j = 0; j < nkeys + naggs; j++) need += out_bytes(out[j], out_capacity) + 512;
+  if (nkeys > 1) need += keypack_scratch_bytes(n, out_capacity);
   st = scratch_reserve(ctx, need, s);
   if (st) return st;
   std::vector<ghb_column> dc;
@@ -193,49 +194,235 @@ int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_
                            const ghb_join_cfg* cfg) {
   if (!ctx || !out_rows || !build_key || !probe_key) return GHB_ERR_INVALID;
   if (nbp < 0 || nbp > 8 || npp < 0 || npp > 8) return set_error(ctx, GHB_ERR_INVALID, "payload counts");
-  cudaStream_t s = 0;
+  if ((nbp > 0 && (!build_payload || !out_build)) || (npp > 0 && (!probe_payload || !out_probe)))
+    return set_error(ctx, GHB_ERR_INVALID, "payload columns or their outputs are NULL");
+  if (out_capacity < 0) return set_error(ctx, GHB_ERR_INVALID, "negative out_capacity");
+  *out_rows = 0;
   scratch_reset(ctx);
-  size_t need = 8192 + in_bytes(*build_key) + in_bytes(*probe_key);
-  for (int j = 0; j < nbp; j++) need += in_bytes(build_payload[j]) + out_bytes(out_build[j], out_capacity) + 1024;
-  for (int j = 0; j < npp; j++) need += in_bytes(probe_payload[j]) + out_bytes(out_probe[j], out_capacity) + 1024;
-  if (out_probe_rowid) need += align256((size_t)out_capacity * 4) + 256;
-  if (out_build_rowid) need += align256((size_t)out_capacity * 4) + 256;
-  need += join_probe_scratch_bytes(probe_key->n);
-  int32_t st = scratch_reserve(ctx, need, s);
-  if (st) return st;
-  std::vector<ghb_column> dbk, dpk, dbp, dpp;
-  std::vector<ghb_out_column> dob, dop;
-  int64_t* d_rows = nullptr;
-  int32_t *d_prow = nullptr, *d_brow = nullptr;
-  if ((st = scratch_alloc(ctx, 8, (void**)&d_rows, s))) return st;
-  if ((st = stage_in(ctx, build_key, 1, dbk, s))) return st;
-  if ((st = stage_in(ctx, probe_key, 1, dpk, s))) return st;
-  if ((st = stage_in(ctx, build_payload, nbp, dbp, s))) return st;
-  if ((st = stage_in(ctx, probe_payload, npp, dpp, s))) return st;
-  if ((st = stage_out(ctx, out_build, nbp, out_capacity, dob, s))) return st;
-  if ((st = stage_out(ctx, out_probe, npp, out_capacity, dop, s))) return st;
-  if (out_probe_rowid && (st = scratch_alloc(ctx, (size_t)out_capacity * 4 + 16, (void**)&d_prow, s))) return st;
-  if (out_build_rowid && (st = scratch_alloc(ctx, (size_t)out_capacity * 4 + 16, (void**)&d_brow, s))) return st;
+  const int64_t n = probe_key->n;
+  for (int j = 0; j < npp; j++)
+    if (probe_payload[j].n != n)
+      return set_error(ctx, GHB_ERR_INVALID, "probe payload %d row count differs from the key", j);
+  if (n >= (int64_t)INT32_MAX) return set_error(ctx, GHB_ERR_UNSUPPORTED, "probe of 2^31 rows or more");
+  int32_t st;
+  for (int i = 0; i < 3; i++)
+    if (!ctx->hstream[i]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[i], cudaStreamNonBlocking));
+  for (auto& row : ctx->hev)
+    for (cudaEvent_t& e : row)
+      if (!e) GHB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaStream_t s_in = ctx->hstream[0], s_k = ctx->hstream[1], s_out = ctx->hstream[2];
+  // the calling thread's legacy default stream may hold work on these
+  // buffers: start after it
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(0));
+
+  // The probe runs in chunks of rows, each through three streams: its key
+  // (and payload) chunk is copied in while the previous chunk is probed and
+  // the one before is copied out, so the copies in both directions overlap
+  // each other and the kernels.  A chunk's output goes to one of two device
+  // buffers; its row count comes back before its copy-out is issued.
+  const int64_t kChunkRows = 8 << 20;
+  const int64_t chunk = std::min<int64_t>(std::max<int64_t>(n, 1), kChunkRows);
+  const int64_t nchunks = n == 0 ? 0 : (n + chunk - 1) / chunk;
+
+  size_t need = 8192 + in_bytes(*build_key) + join_probe_scratch_bytes(n) + (size_t)nchunks * 256 * 2;
+  for (int j = 0; j < nbp; j++) need += in_bytes(build_payload[j]) + 256;
+  auto chunk_in = [&](int64_t rows) {
+    size_t b = align256((size_t)rows * type_width(probe_key->type)) + 256;
+    if (probe_key->null_mode == GHB_NULLS_BYTEMAP) b += align256((size_t)rows) + 256;
+    for (int j = 0; j < npp; j++) {
+      b += align256((size_t)rows * type_width(probe_payload[j].type)) + 256;
+      if (probe_payload[j].null_mode == GHB_NULLS_BYTEMAP) b += align256((size_t)rows) + 256;
+    }
+    return b;
+  };
+  auto chunk_out = [&](int64_t rows) {
+    size_t b = 0;
+    for (int j = 0; j < nbp; j++) b += out_bytes(out_build[j], rows) + 256;
+    for (int j = 0; j < npp; j++) b += out_bytes(out_probe[j], rows) + 256;
+    if (out_probe_rowid) b += align256((size_t)rows * 4) + 256;
+    if (out_build_rowid) b += align256((size_t)rows * 4) + 256;
+    return b;
+  };
+  std::vector<ghb_column> dbk, dbp;
+  if ((st = scratch_reserve(ctx, need + 2 * chunk_in(chunk), s_in))) return st;
+  if ((st = stage_in(ctx, build_key, 1, dbk, s_in))) return st;
+  if ((st = stage_in(ctx, build_payload, nbp, dbp, s_in))) return st;
+  GHB_CUDA_TRY(ctx, cudaEventRecord(ctx->hev[0][0], s_in));
+  GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, ctx->hev[0][0], 0));
   ghb_join_table* t = nullptr;
-  st = join_build_impl(ctx, dbk.data(), dbp.data(), nbp, cfg, &t, s);
-  if (st) return st;
-  st = join_probe_impl(ctx, t, dpk.data(), join_type, dob.data(), dpp.data(), npp, dop.data(),
-                       d_prow, d_brow, out_capacity, d_rows, s);
-  int64_t rows = 0;
-  if (!st) st = read_count(ctx, d_rows, &rows, s);
-  *out_rows = rows;
-  if (!st) {
-    int64_t r = std::min(rows, out_capacity);
-    st = copy_back(ctx, out_build, dob, r, s);
-    if (!st) st = copy_back(ctx, out_probe, dop, r, s);
-    if (!st && d_prow && r > 0)
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_probe_rowid, d_prow, r * 4, cudaMemcpyDeviceToHost, s));
-    if (!st && d_brow && r > 0)
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_build_rowid, d_brow, r * 4, cudaMemcpyDeviceToHost, s));
-    if (!st) GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  if ((st = join_build_impl(ctx, dbk.data(), dbp.data(), nbp, cfg, &t, s_k))) return st;
+  // the output rows a chunk can make: its rows times the most build rows of
+  // one key (one for a semi join, at least one for an outer join)
+  int64_t max_dup = 1;
+  {
+    unsigned long long stats[2] = {0, 0};
+    st = GHB_OK;
+    if (cudaMemcpyAsync(stats, t->d_stats, sizeof(stats), cudaMemcpyDeviceToHost, s_k) != cudaSuccess ||
+        cudaStreamSynchronize(s_k) != cudaSuccess)
+      st = set_error(ctx, GHB_ERR_CUDA, "reading the join table's statistics failed");
+    max_dup = std::max<int64_t>(1, (int64_t)stats[1]);
+    if (join_type == GHB_LEFT_SEMI_JOIN) max_dup = 1;
+    if (st) {
+      ghb_join_table_free(ctx, t);
+      return st;
+    }
   }
+  const int64_t out_chunk = std::min<int64_t>(chunk * max_dup, std::max<int64_t>(out_capacity, 1));
+  struct Slot {
+    std::vector<ghb_column> pk, pp;
+    std::vector<ghb_out_column> ob, op;
+    int32_t *prow = nullptr, *brow = nullptr;
+    int64_t* d_rows = nullptr;
+  } slot[2];
+  int64_t* h_rows = nullptr;   // pinned: each chunk's row count
+  size_t hneed = (size_t)std::max<int64_t>(nchunks, 1) * 8;
+  if (ctx->pinned_bytes < hneed) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    if (cudaMallocHost(&ctx->pinned, std::max<size_t>(hneed, 4096)) != cudaSuccess) {
+      cudaGetLastError();
+      ghb_join_table_free(ctx, t);
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned host memory");
+    }
+    ctx->pinned_bytes = std::max<size_t>(hneed, 4096);
+  }
+  h_rows = (int64_t*)ctx->pinned;
+  auto fail = [&](int32_t code) {
+    cudaStreamSynchronize(s_in);
+    cudaStreamSynchronize(s_k);
+    cudaStreamSynchronize(s_out);
+    ghb_join_table_free(ctx, t);
+    return code;
+  };
+  // room for the chunk buffers beside what is already in the arena: the
+  // arena cannot grow inside a call, so a short arena is an error here
+  {
+    size_t more = 2 * chunk_out(out_chunk) + 4096;
+    if (ctx->scratch_used + more + join_probe_scratch_bytes(n) + (size_t)nchunks * 1024 > ctx->scratch_bytes) {
+      // grow once more: nothing of this call's arena content is in flight
+      // except the build, so wait for it and start the arena over
+      cudaStreamSynchronize(s_k);
+      ghb_join_table_free(ctx, t);
+      size_t want = need + 2 * chunk_in(chunk) + more + (size_t)nchunks * 1024;
+      if ((st = scratch_reserve(ctx, want, s_in))) return st;
+      return ghb_hash_join_host(ctx, build_key, probe_key, join_type, build_payload, nbp, out_build,
+                                probe_payload, npp, out_probe, out_probe_rowid, out_build_rowid,
+                                out_capacity, out_rows, cfg);
+    }
+  }
+  for (int b = 0; b < 2; b++) {
+    Slot& sl = slot[b];
+    sl.pk.assign(probe_key, probe_key + 1);
+    sl.pp.assign(probe_payload, probe_payload + npp);
+    auto dev_col = [&](ghb_column& c) {
+      void* q = nullptr;
+      int32_t r = scratch_alloc(ctx, std::max<size_t>((size_t)chunk * type_width(c.type), 16), &q, s_in);
+      if (r) return r;
+      c.data = q;
+      if (c.null_mode == GHB_NULLS_BYTEMAP) {
+        if ((r = scratch_alloc(ctx, std::max<size_t>((size_t)chunk, 16), &q, s_in))) return r;
+        c.is_null = (const uint8_t*)q;
+      }
+      return (int32_t)GHB_OK;
+    };
+    if ((st = dev_col(sl.pk[0]))) return fail(st);
+    for (int j = 0; j < npp; j++)
+      if ((st = dev_col(sl.pp[j]))) return fail(st);
+    if ((st = stage_out(ctx, out_build, nbp, out_chunk, sl.ob, s_in))) return fail(st);
+    if ((st = stage_out(ctx, out_probe, npp, out_chunk, sl.op, s_in))) return fail(st);
+    if (out_probe_rowid && (st = scratch_alloc(ctx, (size_t)out_chunk * 4 + 16, (void**)&sl.prow, s_in)))
+      return fail(st);
+    if (out_build_rowid && (st = scratch_alloc(ctx, (size_t)out_chunk * 4 + 16, (void**)&sl.brow, s_in)))
+      return fail(st);
+    if ((st = scratch_alloc(ctx, 8, (void**)&sl.d_rows, s_in))) return fail(st);
+  }
+  cudaEvent_t* ev_in = ctx->hev[0];     // chunk copied in (per buffer)
+  cudaEvent_t* ev_probe = ctx->hev[1];  // chunk probed: its input buffer is free
+  cudaEvent_t* ev_rows = ctx->hev[2];   // chunk's row count on the host side
+  cudaEvent_t* ev_out = ctx->hev[3];    // chunk copied out: its output buffer is free
+  int64_t total = 0, written = 0;
+  auto copy_out = [&](int64_t c) -> int32_t {
+    const int b = (int)(c & 1);
+    Slot& sl = slot[b];
+    GHB_CUDA_TRY(ctx, cudaEventSynchronize(ev_rows[b]));
+    const int64_t rows = h_rows[c];
+    total += rows;
+    const int64_t r = std::max<int64_t>(0, std::min<int64_t>(rows, out_capacity - written));
+    GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_out, ev_rows[b], 0));
+    if (r > 0) {
+      for (int j = 0; j < nbp; j++) {
+        const size_t w = type_width(out_build[j].type);
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync((char*)out_build[j].data + written * w, sl.ob[j].data, r * w,
+                                          cudaMemcpyDeviceToHost, s_out));
+        if (out_build[j].is_null)
+          GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_build[j].is_null + written, sl.ob[j].is_null, r,
+                                            cudaMemcpyDeviceToHost, s_out));
+      }
+      for (int j = 0; j < npp; j++) {
+        const size_t w = type_width(out_probe[j].type);
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync((char*)out_probe[j].data + written * w, sl.op[j].data, r * w,
+                                          cudaMemcpyDeviceToHost, s_out));
+        if (out_probe[j].is_null)
+          GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_probe[j].is_null + written, sl.op[j].is_null, r,
+                                            cudaMemcpyDeviceToHost, s_out));
+      }
+      if (sl.prow)
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_probe_rowid + written, sl.prow, r * 4, cudaMemcpyDeviceToHost,
+                                          s_out));
+      if (sl.brow)
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_build_rowid + written, sl.brow, r * 4, cudaMemcpyDeviceToHost,
+                                          s_out));
+    }
+    written += r;
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_out[b], s_out));
+    return GHB_OK;
+  };
+  for (int64_t c = 0; c < nchunks; c++) {
+    const int b = (int)(c & 1);
+    Slot& sl = slot[b];
+    const int64_t r0 = c * chunk, rows = std::min<int64_t>(chunk, n - r0);
+    // copy in, once the probe of chunk c - 2 has read this buffer
+    if (c >= 2) GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_in, ev_probe[b], 0));
+    auto copy_in = [&](const ghb_column& h, ghb_column& d) -> int32_t {
+      const size_t w = type_width(h.type);
+      d.n = rows;
+      if (rows > 0 && !h.data) return set_error(ctx, GHB_ERR_INVALID, "probe column data is NULL");
+      GHB_CUDA_TRY(ctx, cudaMemcpyAsync((void*)d.data, (const char*)h.data + r0 * w, rows * w,
+                                        cudaMemcpyHostToDevice, s_in));
+      if (h.null_mode == GHB_NULLS_BYTEMAP) {
+        if (!h.is_null) return set_error(ctx, GHB_ERR_INVALID, "probe column is_null is NULL");
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync((void*)d.is_null, h.is_null + r0, rows, cudaMemcpyHostToDevice, s_in));
+      }
+      return (int32_t)GHB_OK;
+    };
+    if ((st = copy_in(*probe_key, sl.pk[0]))) return fail(st);
+    for (int j = 0; j < npp; j++)
+      if ((st = copy_in(probe_payload[j], sl.pp[j]))) return fail(st);
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_in[b], s_in));
+    // probe, once the chunk is in and chunk c - 2's output has been copied out
+    GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, ev_in[b], 0));
+    if (c >= 2) GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, ev_out[b], 0));
+    st = join_probe_impl(ctx, t, sl.pk.data(), join_type, sl.ob.data(), sl.pp.data(), npp, sl.op.data(),
+                         sl.prow, sl.brow, out_chunk, sl.d_rows, s_k, (int32_t)r0);
+    if (st) return fail(st);
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_probe[b], s_k));
+    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(&h_rows[c], sl.d_rows, 8, cudaMemcpyDeviceToHost, s_k));
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_rows[b], s_k));
+    // the previous chunk's output goes out while this one is probed
+    if (c >= 1 && (st = copy_out(c - 1))) return fail(st);
+  }
+  if (nchunks >= 1 && (st = copy_out(nchunks - 1))) return fail(st);
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s_out));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s_in));
+  st = ghb_sync(ctx, s_k);   // device status of every chunk's kernels
   ghb_join_table_free(ctx, t);
-  return st;
+  *out_rows = total;
+  if (st) return st;
+  if (total > out_capacity)
+    return set_error(ctx, GHB_ERR_CAPACITY, "join output of %lld rows exceeds out_capacity %lld",
+                     (long long)total, (long long)out_capacity);
+  return GHB_OK;
 }
 
 int32_t ghb_sort_host(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,

@@ -270,11 +270,13 @@ __device__ __forceinline__ uint64_t lb_load(const uint64_t* p) {
 // tiles 32 at a time, then publishes the inclusive prefix.  The words carry
 // only counts (no tile reads another tile's output), so relaxed stores and
 // loads suffice and no fence is needed.  Every wait is bounded: after
-// kSpinLimit polls it raises GHB_ERR_TIMEOUT and returns 0 (the results of
-// that launch are then invalid and the host is told).
+// `spin_limit` polls that find an earlier tile not ready it raises
+// GHB_ERR_TIMEOUT and returns 0 (the results of that launch are then invalid
+// and the host is told; every output position stays below the true one, so
+// no write leaves its buffer).
 __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status_arr, uint32_t epoch,
                                                        int64_t tile, uint64_t count,
-                                                       int32_t* dev_status) {
+                                                       int32_t* dev_status, int spin_limit) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) lb_store(&status_arr[0], lb_pack(epoch, kFlagPrefix, count));
@@ -305,7 +307,7 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status_arr, uin
       int first_nr = __ffs(not_ready) - 1;
       unsigned below = (first_nr == 0) ? 0u : ((1u << first_nr) - 1u);
       if (!(pref & below)) {
-        if (++spins > kSpinLimit) {
+        if (++spins >= spin_limit) {
           if (lane == 0) raise_status(dev_status, kDevTimeout);
           return 0;
         }

@@ -42,6 +42,8 @@
 //        (probe row, build row, payloads) at its offset, in probe-row order.
 // Neither pass takes a CTA barrier per chunk.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "ghb_ctx.hpp"
 
@@ -245,6 +247,7 @@ struct ProbeParams {
   ghb_out_column opp[kMaxPay];
   int32_t* out_prow;
   int32_t* out_brow;
+  int32_t prow_base;       // added to every probe row id written (a chunk of a longer probe)
   int64_t n, nchunks, cap;
   int32_t* slot_of_row;    // [n] slot (bucket * 4 + index) of the row's key, -1 = no match
   int64_t* chunk_count;    // [nchunks * warps per CTA] output rows of each warp's rows of a
@@ -436,6 +439,7 @@ struct ScanParams {
   uint32_t epoch;
   unsigned long long* counters;
   int32_t* status;
+  int32_t spin_limit;   // look-back polls before GHB_ERR_TIMEOUT
 };
 
 __global__ void __launch_bounds__(1024) join_scan_lb_kernel(ScanParams p) {
@@ -465,7 +469,8 @@ __global__ void __launch_bounds__(1024) join_scan_lb_kernel(ScanParams p) {
       }
       s_warp[lane] = wi - w;
       const int64_t total = __shfl_sync(0xffffffffu, wi, 31);
-      const uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, (uint64_t)total, p.status);
+      const uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, (uint64_t)total, p.status,
+                                                    p.spin_limit);
       if (lane == 0) {
         s_excl = ex;
         if (tile == p.ntiles - 1) *p.d_total = (int64_t)(ex + total);
@@ -526,6 +531,7 @@ struct EmitDesc {
   ghb_out_column opp[kMaxPay];
   int32_t* out_prow;
   int32_t* out_brow;
+  int32_t prow_base;
   int32_t nbp, npp, n_inline;
 };
 
@@ -540,6 +546,7 @@ __device__ __forceinline__ void load_emit_desc(const ProbeParams& p, EmitDesc* d
   if (threadIdx.x == 0) {
     d->out_prow = p.out_prow;
     d->out_brow = p.out_brow;
+    d->prow_base = p.prow_base;
     d->nbp = p.nbp;
     d->npp = p.npp;
     d->n_inline = p.n_inline;
@@ -554,7 +561,7 @@ __device__ __forceinline__ void load_emit_desc(const ProbeParams& p, EmitDesc* d
 // registers.
 __device__ __noinline__ void emit_row(const EmitDesc* d, int64_t pos, int64_t prow, int32_t brow, bool inl,
                                       unsigned long long w0, unsigned long long w1) {
-  if (d->out_prow) __stcs(d->out_prow + pos, (int)prow);
+  if (d->out_prow) __stcs(d->out_prow + pos, (int)prow + d->prow_base);
   if (d->out_brow) __stcs(d->out_brow + pos, brow);
   for (int j = 0; j < d->nbp; j++) {
     const ghb_column& c = d->bpay[j];
@@ -581,6 +588,7 @@ __device__ __noinline__ void emit_row(const EmitDesc* d, int64_t pos, int64_t pr
 struct LeanOut {
   int32_t* prow;
   int32_t* brow;
+  int32_t prow_base;
   void* data[kInline];
   uint8_t* nul[kInline];
   bool is_int[kInline];
@@ -591,6 +599,7 @@ __device__ __forceinline__ LeanOut lean_out(const ProbeParams& p) {
   LeanOut o;
   o.prow = p.out_prow;
   o.brow = p.out_brow;
+  o.prow_base = p.prow_base;
   o.nbp = p.nbp;
 #pragma unroll
   for (int j = 0; j < kInline; j++) {
@@ -603,7 +612,7 @@ __device__ __forceinline__ LeanOut lean_out(const ProbeParams& p) {
 
 __device__ __forceinline__ void emit_lean(const LeanOut& o, int64_t pos, int64_t prow, int32_t brow,
                                           unsigned long long w0, unsigned long long w1) {
-  if (o.prow) __stcs(o.prow + pos, (int)prow);
+  if (o.prow) __stcs(o.prow + pos, (int)prow + o.prow_base);
   if (o.brow) __stcs(o.brow + pos, brow);
 #pragma unroll
   for (int j = 0; j < kInline; j++) {
@@ -662,7 +671,7 @@ __global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
         raise_status(p.status, kDevCapacity);
         continue;
       }
-      if (p.out_prow) __stcs(p.out_prow + pos, (int)(wbase + k * 32 + lane));
+      if (p.out_prow) __stcs(p.out_prow + pos, (int)(wbase + k * 32 + lane) + p.prow_base);
 #pragma unroll
       for (int j = 0; j < kInline; j++) {
         if (j >= p.nbp) break;
@@ -774,6 +783,15 @@ static int64_t next_pow2(int64_t v) {
   return p;
 }
 
+// Tables holding an L2 persistence window, per device (`delta` added under a
+// lock; returns the new count).
+static int l2_window_count(int device, int delta) {
+  static std::mutex mu;
+  static std::map<int, int> count;
+  std::lock_guard<std::mutex> lock(mu);
+  return count[device] += delta;
+}
+
 int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* build_payload,
                         int32_t nbp, const ghb_join_cfg* cfg, ghb_join_table** out,
                         cudaStream_t stream) {
@@ -880,6 +898,8 @@ int32_t join_build_impl(ghb_ctx* ctx, const ghb_column* build_key, const ghb_col
       attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
       cudaStreamSetAttribute(stream, cudaStreamAttributeAccessPolicyWindow, &attr);
       t->l2_window = true;
+      t->device = ctx->device;
+      l2_window_count(ctx->device, +1);
     }
   }
   *out = t;
@@ -898,7 +918,7 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
                         int32_t join_type, ghb_out_column* out_build, const ghb_column* probe_payload,
                         int32_t npp, ghb_out_column* out_probe, int32_t* out_probe_rowid,
                         int32_t* out_build_rowid, int64_t out_capacity, int64_t* d_out_rows,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int32_t prow_base) {
   if (!t) return set_error(ctx, GHB_ERR_INVALID, "table is NULL");
   int32_t st = validate_columns(ctx, probe_key, 1, nullptr);
   if (st) return st;
@@ -949,6 +969,7 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   for (int j = 0; j < t->n_inline && p.lean; j++) p.lean = t->pay[j].null_mode == GHB_NULLS_NONE;
   p.out_prow = out_probe_rowid;
   p.out_brow = out_build_rowid;
+  p.prow_base = prow_base;
   p.n = probe_key->n;
   p.nchunks = (p.n + kChunk - 1) / kChunk;
   p.cap = out_capacity;
@@ -1002,6 +1023,7 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
     sp.lb = ctx->lb_status;
     sp.counters = ctx->d_counters;
     sp.status = ctx->d_status;
+    sp.spin_limit = ctx->spin_limit;
     const int sgrid = (int)std::min<int64_t>(sp.ntiles, (int64_t)ctx->num_sms);
     join_scan_lb_kernel<<<sgrid, 1024, 0, stream>>>(sp);
   }
@@ -1037,8 +1059,21 @@ int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table) {
   if (!ctx || !table) return GHB_ERR_INVALID;
   if (table->l2_window) {
     cudaStreamSynchronize(table->stream);
-    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
-    cudaCtxResetPersistingL2Cache();
+    // the build stream's window, if it still points at this table, goes
+    cudaStreamAttrValue attr;
+    std::memset(&attr, 0, sizeof(attr));
+    if (cudaStreamGetAttribute(table->stream, cudaStreamAttributeAccessPolicyWindow, &attr) == cudaSuccess &&
+        attr.accessPolicyWindow.base_ptr == table->alloc) {
+      std::memset(&attr, 0, sizeof(attr));
+      cudaStreamSetAttribute(table->stream, cudaStreamAttributeAccessPolicyWindow, &attr);
+    }
+    cudaGetLastError();
+    // the persisting carve-out is shared by every resident table of the
+    // device: it is released with the last table that holds a window
+    if (l2_window_count(table->device, -1) == 0) {
+      cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+      cudaCtxResetPersistingL2Cache();
+    }
   }
   // released in the order of the build stream: probes issued on that stream
   // before this call finish first; probes on other streams must be ordered
@@ -1073,7 +1108,7 @@ int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table, const ghb_colu
   if (st) return st;
   return join_probe_impl(ctx, table, probe_key, join_type, out_build, probe_payload, n_probe_payload,
                          out_probe, out_probe_rowid, out_build_rowid, out_capacity, d_out_rows,
-                         (cudaStream_t)stream);
+                         (cudaStream_t)stream, 0);
 }
 
 }  // extern "C"

@@ -1,0 +1,201 @@
+// ghb_keypack.cu — GROUP BY over several key columns, by packing the keys of
+// a row into one 64-bit key.
+//
+// GHive groups by any number of key columns of mixed types: it sorts row
+// indices with a comparator over all `key_num` key columns
+// (gpu_impl/src/Operator/GroupByPredicate.cu:24-105, comparator
+// gpu_impl/inc/Operator/GroupByPredicate.hpp:22-101) and reduces runs of
+// equal keys.  Here the keys of a row become one int64 value, and the
+// single-key hash group-by (ghb_groupby.cu) runs on that value:
+//
+//   1. one read of the key columns: per key the min/max of its order image
+//      (BinarySortable order: sign-flipped integers, IEEE total order for
+//      doubles) and whether it holds NULLs;
+//   2. plan (host): key j becomes a field [null flag][image - min] of just the
+//      width its range needs; the fields are concatenated into at most 63
+//      bits (the packed value is a non-negative int64).  Equal key tuples
+//      pack to equal values and different ones to different values, so the
+//      groups are exactly Hive's (a NULL key component is its own value);
+//   3. one pass writes the packed keys as an int64 column;
+//   4. after the group-by, the packed key of each output group is unpacked
+//      into the caller's key output columns (NULL components as NULL).
+//
+// Key tuples that need more than 63 bits are refused (GHB_ERR_UNSUPPORTED).
+#include <algorithm>
+
+#include "ghb_ctx.hpp"
+
+namespace ghb {
+
+__device__ __forceinline__ uint64_t kp_image(const ghb_column& c, int64_t raw) {
+  return c.type == GHB_DOUBLE ? flip_f64_bits((uint64_t)raw) : flip_i64(raw);
+}
+
+struct KpMinMaxParams {
+  int32_t nkeys;
+  ghb_column col[kMaxPackKeys];
+  int64_t n;
+  unsigned long long* out;   // per key: [0] min image, [1] max image, [2] any NULL
+};
+
+__global__ void __launch_bounds__(256) keypack_minmax_kernel(KpMinMaxParams p) {
+  __shared__ unsigned long long s_red[3][8];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int warp = threadIdx.x >> 5;
+  for (int j = 0; j < p.nkeys; j++) {
+    const ghb_column c = p.col[j];
+    unsigned long long mn = ~0ull, mx = 0, anynull = 0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < p.n; r += stride) {
+      const int64_t raw = ld_raw_cs(c, r);
+      if (c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, r)) {
+        anynull = 1;
+        continue;
+      }
+      const unsigned long long img = kp_image(c, raw);
+      mn = min(mn, img);
+      mx = max(mx, img);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
+      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+      anynull |= __shfl_down_sync(0xffffffffu, anynull, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      s_red[0][warp] = mn;
+      s_red[1][warp] = mx;
+      s_red[2][warp] = anynull;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // one set of atomics per CTA
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+        mn = min(mn, s_red[0][w]);
+        mx = max(mx, s_red[1][w]);
+        anynull |= s_red[2][w];
+      }
+      atomicMin(&p.out[3 * j], mn);
+      atomicMax(&p.out[3 * j + 1], mx);
+      if (anynull) atomicOr(&p.out[3 * j + 2], 1ull);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) keypack_pack_kernel(KeyPackPlan p, int64_t n, int64_t* out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t v = 0;
+#pragma unroll
+    for (int j = 0; j < kMaxPackKeys; j++) {
+      if (j >= p.nkeys) break;
+      const ghb_column& c = p.col[j];
+      const int64_t raw = ld_raw_cs(c, r);
+      const bool null = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, r);
+      if (p.fshift[j] >= 0 && !null) v |= 1ull << p.fshift[j];
+      if (!null && p.vbits[j] > 0) v |= (kp_image(c, raw) - p.umin[j]) << p.vshift[j];
+    }
+    __stcs((unsigned long long*)out + r, (unsigned long long)v);
+  }
+}
+
+// Unpacks the packed key of each of the first min(*d_groups, cap) output
+// rows into the key output columns.
+__global__ void __launch_bounds__(256) keypack_unpack_kernel(KeyPackPlan p, const int64_t* packed,
+                                                              const int64_t* d_groups, int64_t cap,
+                                                              KeyOuts outs) {
+  const int64_t g = min(*d_groups, cap);
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < g;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = (uint64_t)packed[r];
+#pragma unroll
+    for (int j = 0; j < kMaxPackKeys; j++) {
+      if (j >= p.nkeys) break;
+      const ghb_out_column& o = outs.o[j];
+      const bool null = p.fshift[j] >= 0 && ((v >> p.fshift[j]) & 1ull) == 0;
+      const int vb = p.vbits[j];
+      const uint64_t field = vb == 0 ? 0 : (v >> p.vshift[j]) & ((1ull << vb) - 1);
+      const uint64_t img = field + p.umin[j];
+      const int64_t raw = o.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(img)
+                                               : (int64_t)(img ^ 0x8000000000000000ull);
+      if (o.is_null) o.is_null[r] = null ? 1 : 0;
+      switch (o.type) {
+        case GHB_LONG: ((int64_t*)o.data)[r] = null ? INT64_MAX : raw; break;
+        case GHB_INT: ((int32_t*)o.data)[r] = null ? INT32_MAX : (int32_t)raw; break;
+        case GHB_DOUBLE: ((int64_t*)o.data)[r] = null ? 0x7ff8000000000000ll : raw; break;
+      }
+    }
+  }
+}
+
+// Plans the packing of the key columns and writes the packed keys (n int64
+// values) to `packed`.  Reads the keys' ranges back to the host (one
+// stream synchronisation).
+int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys,
+                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream) {
+  if (nkeys < 1 || nkeys > kMaxPackKeys)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d key columns: at most %d", nkeys, kMaxPackKeys);
+  KeyPackPlan& P = *plan;
+  std::memset(&P, 0, sizeof(P));
+  P.nkeys = nkeys;
+  KpMinMaxParams mp;
+  std::memset(&mp, 0, sizeof(mp));
+  mp.nkeys = nkeys;
+  mp.n = n;
+  for (int j = 0; j < nkeys; j++) {
+    const ghb_column& c = cols[key_cols[j]];
+    if (c.type == GHB_STRING)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "key %d: STRING keys are not on the device path", j);
+    P.col[j] = c;
+    mp.col[j] = c;
+  }
+  unsigned long long* d_mm = nullptr;
+  int32_t st = scratch_alloc(ctx, 3 * 8 * kMaxPackKeys, (void**)&d_mm, stream);
+  if (st) return st;
+  unsigned long long init[3 * kMaxPackKeys];
+  for (int j = 0; j < kMaxPackKeys; j++) {
+    init[3 * j] = ~0ull;
+    init[3 * j + 1] = 0;
+    init[3 * j + 2] = 0;
+  }
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(d_mm, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  mp.out = d_mm;
+  keypack_minmax_kernel<<<grid, 256, 0, stream>>>(mp);
+  GHB_LAUNCH_CHECK(ctx);
+  unsigned long long mm[3 * kMaxPackKeys];
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost, stream));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+  int bits = 0;
+  for (int j = 0; j < nkeys; j++) {
+    const bool anyval = mm[3 * j] <= mm[3 * j + 1];
+    P.umin[j] = anyval ? mm[3 * j] : 0;
+    const uint64_t range = anyval ? mm[3 * j + 1] - mm[3 * j] : 0;
+    P.vbits[j] = (int8_t)(range == 0 ? 0 : 64 - __builtin_clzll(range));
+    P.vshift[j] = (int8_t)bits;
+    bits += P.vbits[j];
+    P.fshift[j] = -1;
+    if (mm[3 * j + 2]) {
+      P.fshift[j] = (int8_t)bits;
+      bits++;
+    }
+    if (bits > 63)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED,
+                       "the %d key columns' value ranges need more than 63 bits together", nkeys);
+  }
+  keypack_pack_kernel<<<grid, 256, 0, stream>>>(P, n, packed);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* packed,
+                       const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
+                       cudaStream_t stream) {
+  KeyOuts outs;
+  std::memset(&outs, 0, sizeof(outs));
+  for (int j = 0; j < plan.nkeys; j++) outs.o[j] = key_out[j];
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->num_sms * 4));
+  keypack_unpack_kernel<<<grid, 256, 0, stream>>>(plan, packed, d_groups, cap, outs);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+}  // namespace ghb

@@ -13,8 +13,12 @@
 // The array is GHB_NOALLOC_SCRATCH_BYTES (8 MiB) and every GPU that loads the
 // library holds it until the process exits.  Its device address is looked up
 // once per device with cudaGetSymbolAddress (in host code the array's name is
-// only a host-side stand-in, not a device address); the first call on a
-// device does that lookup.
+// only a host-side stand-in, not a device address).  The first call on a
+// device does that set-up, and with it loads this file's module (which
+// creates the array) and every kernel the call can launch: CUDA loads code
+// lazily, and loading may allocate device memory.  After that first call no
+// call loads code or allocates.  The cached address assumes the device's
+// primary context lives as long as the process (no cudaDeviceReset).
 #include <mutex>
 
 #include "ghb_ctx.hpp"
@@ -24,6 +28,7 @@ namespace ghb {
 int32_t filter_groupby_impl(ghb_ctx*, const ghb_predicate*, const ghb_column*, int32_t,
                             const int32_t*, int32_t, const ghb_agg_desc*, int32_t, ghb_out_column*,
                             int64_t, int64_t*, const ghb_groupby_cfg*, cudaStream_t, void*, size_t);
+int32_t preload_fixed_table_kernels(ghb_ctx* ctx);
 
 namespace {
 
@@ -37,8 +42,9 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 std::mutex g_setup_mutex;
 void* g_scratch_ptr[kMaxDevices] = {nullptr};
 
-// Device address of the scratch on the current device (looked up once).
-int32_t scratch_address(int device, void** out) {
+// Device address of the scratch on the current device (looked up once, with
+// the kernels the call launches loaded at the same time).
+int32_t scratch_address(ghb_ctx* local, int device, void** out) {
   if (device < 0 || device >= kMaxDevices) return GHB_ERR_INVALID;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_ptr[device]) {
@@ -48,6 +54,7 @@ int32_t scratch_address(int device, void** out) {
       cudaGetLastError();
       return GHB_ERR_CUDA;
     }
+    if (int32_t st = preload_fixed_table_kernels(local)) return st;
     g_scratch_ptr[device] = ptr;
   }
   *out = g_scratch_ptr[device];
@@ -70,15 +77,15 @@ extern "C" int32_t ghb_filter_groupby_noalloc(const ghb_predicate* pred, const g
     cudaGetLastError();
     return GHB_ERR_CUDA;
   }
-  void* base = nullptr;
-  int32_t st = scratch_address(device, &base);
-  if (st) return st;
   cudaStream_t s = (cudaStream_t)stream;
   // a host-side context object only: its device pointers stay empty except
   // the status word, which lives in the scratch
   ghb_ctx local;
   local.device = device;
   cudaDeviceGetAttribute(&local.num_sms, cudaDevAttrMultiProcessorCount, device);
+  void* base = nullptr;
+  int32_t st = scratch_address(&local, device, &base);
+  if (st) return st;
   local.d_status = (int32_t*)base;
   if (cudaMemsetAsync(base, 0, kStatusBytes, s) != cudaSuccess) {
     cudaGetLastError();

@@ -152,7 +152,7 @@ int32_t plan_outputs(ghb_server* s, Req* q, std::string* err) {
       break;
     }
     case GHB_OP_GROUPBY: {
-      if (q->idx.size() > 1) return *err = "group-by takes 0 or 1 key column", GHB_ERR_UNSUPPORTED;
+      if (q->idx.size() > (size_t)kMaxPackKeys) return *err = "too many group-by key columns", GHB_ERR_UNSUPPORTED;
       for (int32_t k : q->idx) {
         if (k < 0 || k >= (int)q->cols.size()) return *err = "key column out of range", GHB_ERR_INVALID;
         q->out_types.push_back(q->cols[k].type);
@@ -167,6 +167,7 @@ int32_t plan_outputs(ghb_server* s, Req* q, std::string* err) {
       q->out_rows = g;
       int64_t C = next_pow2_i64(std::max<int64_t>(2 * std::min<int64_t>(g, std::max<int64_t>(n, 1)) + 1, 64));
       q->work_bytes = gb_table_bytes(C, 1 + 2 * (int32_t)q->aggs.size() + 1);
+      if (q->idx.size() > 1) q->work_bytes += keypack_scratch_bytes(n, g);   // the packed keys
       break;
     }
     case GHB_OP_JOIN_PROBE: {

@@ -225,6 +225,10 @@ class Context:
     def sync(self, stream=None):
         self._check(lib().ghb_sync(self.h, _stream(stream)))
 
+    def set_spin_limit(self, polls):
+        """Bound of this context's look-back waits (polls <= 0: the default)."""
+        self._check(lib().ghb_ctx_set_spin_limit(self.h, int(polls)))
+
     # ------------------------------------------------------------ device ops
     def filter(self, pred, cols, proj=None, capacity=None, stream=None, sync=True):
         """FilterPredicate::process + FilterOperator::clean_data on device columns.

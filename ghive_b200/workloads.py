@@ -33,11 +33,13 @@ def fact_predicate(cut=1263):
     return abi.Pred.leaf(abi.FILTER_LT, 3, a=cut)
 
 
-def join_tables(n_build=1_500_000, n_probe=60_000_000, miss=0.05, seed_idx=1):
+def join_tables(n_build=1_500_000, n_probe=60_000_000, miss=0.05, seed_idx=1, sparse=False):
     """Build: unique int64 keys = a permutation of [1, n_build], payload int64
     U[0,2^62), payload double U[0,1).  Probe: int64 foreign key uniform over the
     build keys, a `miss` fraction replaced by keys in (n_build, 2*n_build] that
-    match nothing, plus an int32 payload."""
+    match nothing, plus an int32 payload.  sparse=True passes every key (build
+    and probe) through mix64_np, a bijection: the same matches, but keys spread
+    over the whole int64 range (a natural key instead of a surrogate one)."""
     g = rng(seed_idx)
     bkey = g.permutation(np.arange(1, n_build + 1, dtype=np.int64))
     bpay_l = g.integers(0, 1 << 62, n_build, dtype=np.int64)
@@ -46,6 +48,8 @@ def join_tables(n_build=1_500_000, n_probe=60_000_000, miss=0.05, seed_idx=1):
     m = g.random(n_probe) < miss
     fk[m] = g.integers(n_build + 1, 2 * n_build + 1, int(m.sum()), dtype=np.int64)
     ppay = g.integers(0, 1 << 31, n_probe, dtype=np.int64).astype(np.int32)
+    if sparse:
+        bkey, fk = mix64_np(bkey), mix64_np(fk)
     return (bkey, [bpay_l, bpay_d]), (fk, ppay)
 
 

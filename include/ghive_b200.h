@@ -204,6 +204,15 @@ int32_t ghb_abi_version(void);
 int32_t ghb_sync(ghb_ctx* ctx, void* stream);
 /* Number of kernels the context launched since creation. */
 int64_t ghb_kernel_launches(const ghb_ctx* ctx);
+/* Bound of the decoupled look-back waits (filter, join probe offsets, sort
+ * passes) of this context's later launches: a CTA that polls an earlier,
+ * not yet published tile `polls` times gives up, raises GHB_ERR_TIMEOUT
+ * (reported by ghb_sync) and returns; its results are then invalid, but
+ * every write stays inside the caller's buffers.  polls <= 0 restores the
+ * default (2^21 polls, about a second).  No counterpart in the reference,
+ * whose waits are inside Thrust; a small bound lets a test reach the
+ * timeout path on purpose. */
+int32_t ghb_ctx_set_spin_limit(ghb_ctx* ctx, int32_t polls);
 
 /* ---- filter (F1) -------------------------------------------------------
  * Replaces FilterPredicate::process (FilterPredicate.cu:434-571) followed by
@@ -306,8 +315,13 @@ int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
  * plus COUNT(*)), R rounded up to 2, 4, 8, 16 or 24 when C > 2^17; a call
  * that would need more than the array holds returns GHB_ERR_CAPACITY before
  * launching.  About 60,000 groups fit with the fact-table aggregates.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Each call clears the part of the
+ * The first call on a device is its set-up: it looks up the array's device
+ * address and loads the array and every kernel the call launches (CUDA
+ * loads code lazily, and loading may allocate device memory).  Make that
+ * first call before handing the device's memory to another allocator and
+ * before any stream capture; later calls load and allocate nothing.  The
+ * looked-up address is kept for the life of the process (it assumes no
+ * cudaDeviceReset).  Each call clears the part of the
  * array it uses, runs on `stream`, waits for it and returns the device
  * status (GHB_ERR_CAPACITY for a short output).  Calls share the one array:
  * calls that overlap on the GPU (other streams, other host threads) race and

@@ -573,3 +573,110 @@ def test_join_many_chunks(ctx):
     o1, o2 = np.lexsort((gb, gp)), np.lexsort((br, pr))
     assert np.array_equal(gp[o1], pr[o2]) and np.array_equal(gb[o1], br[o2])
     t.free()
+
+
+# --------------------------------------------------- several GROUP BY keys
+@pytest.mark.parametrize("nkeys", [2, 3])
+def test_groupby_several_keys_fact_shape(ctx, nkeys):
+    """GROUP BY (k, d % 7[, qty]) over the fact table: the keys of a row are
+    packed into one int64 value on the device and unpacked into the key
+    output columns; results equal the oracle's Hive group-by."""
+    k, qty, price, d = workloads.fact_table(600_000, seed_idx=60, groups=200)
+    dow = (d % 7).astype(np.int32)
+    cols = [k, qty, price, d, dow]
+    keys = [0, 4] if nkeys == 2 else [0, 4, 1]
+    g = 200 * 7 * (50 if nkeys == 3 else 1)
+    got = _check_groupby(ctx, workloads.fact_predicate(), cols, keys, workloads.AGGS_FACT, max_groups=g)
+    assert got > 1000
+
+
+def test_groupby_several_keys_nulls_types_and_extremes(ctx):
+    g = np.random.default_rng(61)
+    n = 120_000
+    i32, i64 = np.iinfo(np.int32), np.iinfo(np.int64)
+    a = g.choice(np.array([i32.min, -1, 0, 7, i32.max - 1], dtype=np.int32), n)   # INT, full range
+    an = g.random(n) < 0.1
+    b = g.integers(-3, 3, n, dtype=np.int64)                                       # LONG, small
+    bn = g.random(n) < 0.1
+    c = np.round(g.integers(0, 5, n) * 0.25 - 0.5, 2)                              # DOUBLE, few values
+    v = g.integers(-1000, 1000, n, dtype=np.int64)
+    aggs = [(abi.CNT, -1), (abi.SUM, 3), (abi.MIN, 3), (abi.MAX, 3), (abi.AVG, 3)]
+    cols = [(a, an), (b, bn), c, v]
+    _check_groupby(ctx, None, cols, [0, 1, 2], aggs, max_groups=5 * 7 * 5)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_GT, 3, a=0), cols, [2, 0], aggs, max_groups=64)
+    # a key column that is all NULL, and one constant column
+    allnull = np.ones(n, dtype=bool)
+    _check_groupby(ctx, None, [(b, allnull), np.full(n, 5, dtype=np.int64), v], [0, 1],
+                   [(abi.SUM, 2)], max_groups=4)
+    # empty input
+    _check_groupby(ctx, None, [b[:0], c[:0], v[:0]], [0, 1], [(abi.SUM, 2)], max_groups=4)
+
+
+def test_groupby_several_keys_too_wide_is_refused(ctx):
+    from ghive_b200._lib import GhbError
+    g = np.random.default_rng(62)
+    n = 10_000
+    i64 = np.iinfo(np.int64)
+    a = g.integers(i64.min, i64.max, n, dtype=np.int64)
+    b = g.integers(i64.min, i64.max, n, dtype=np.int64)
+    with pytest.raises(GhbError) as e:
+        ctx.filter_groupby(None, [dev(a), dev(b)], [0, 1], [(abi.CNT, -1)], capacity=n, max_groups=n)
+    assert e.value.code == abi.ERR_UNSUPPORTED
+    # the context stays usable
+    _check_groupby(ctx, None, [a % 10, b % 10], [0, 1], [(abi.CNT, -1)], max_groups=400)
+
+
+def test_groupby_several_keys_host_entry_point(ctx):
+    k, qty, price, d = workloads.fact_table(200_000, seed_idx=63, groups=50)
+    cols = [k, qty, price, d, (d % 3).astype(np.int32)]
+    gk, ga, g = ctx.filter_groupby_host(workloads.fact_predicate(), cols, [0, 4], workloads.AGGS_FACT,
+                                        capacity=256, max_groups=150)
+    ok, oa = oracle.filter_groupby(workloads.fact_predicate(), cols, [0, 4], workloads.AGGS_FACT)
+    assert g == len(ok[0][0]) == 150
+    got, exp = _norm_rows(gk, ga), _norm_rows(ok, oa)
+    for a_, b_ in zip(got, exp):
+        assert a_[:4] == b_[:4] and a_[6:] == b_[6:]
+        assert abs(a_[4] - b_[4]) <= REL_TOL * abs(b_[4])
+        assert abs(a_[5] - b_[5]) <= REL_TOL * abs(b_[5])
+
+
+# --------------------------------------- host-buffer join in pipelined chunks
+@pytest.mark.parametrize("jt", [abi.INNER_JOIN, abi.LEFT_OUTER_JOIN])
+def test_host_join_in_chunks(ctx, jt):
+    """ghb_hash_join_host probes in 8M-row chunks whose copies in and out
+    overlap the kernels: a 17M-row probe (three chunks, the last partial)
+    with duplicated build keys, a probe payload and both row-id outputs
+    equals the oracle's pairs, in probe-row order."""
+    g = np.random.default_rng(80 + jt)
+    nb, m = 100_000, 17_000_000
+    bkey = g.permutation(np.arange(1, nb + 1, dtype=np.int64))
+    bkey[:500] = bkey[500:1000]                       # keys twice in the build
+    pkey = g.integers(0, nb + 20_000, m, dtype=np.int64)
+    bpay = [g.integers(0, 1 << 40, nb, dtype=np.int64), g.random(nb)]
+    ppay = g.integers(-1000, 1000, m, dtype=np.int64).astype(np.int32)
+    r = ctx.hash_join_host(bkey, pkey, jt, build_payload=bpay, probe_payload=[ppay],
+                           capacity=m + m // 50)
+    pr, br = oracle.hash_join(bkey, pkey, jt)
+    assert r["rows"] == len(pr)
+    gp, gb = r["probe_rowid"].astype(np.int64), r["build_rowid"].astype(np.int64)
+    assert np.all(np.diff(gp) >= 0)
+    o1, o2 = np.lexsort((gb, gp)), np.lexsort((br, pr))
+    gp, gb, pr, br = gp[o1], gb[o1], pr[o2].astype(np.int64), br[o2].astype(np.int64)
+    assert np.array_equal(gp, pr) and np.array_equal(gb, br)
+    hit = gb >= 0
+    (v0, n0), (v1, n1) = r["build"]
+    assert np.array_equal(v0[o1][hit], bpay[0][gb[hit]]) and np.all(n0[o1][~hit])
+    assert np.array_equal(v1[o1][hit].view(np.uint64), bpay[1][gb[hit]].view(np.uint64))
+    assert np.array_equal(r["probe"][0][0][o1], ppay[gp])
+
+
+def test_host_join_in_chunks_short_output(ctx):
+    from ghive_b200._lib import GhbError
+    (bkey, bpay), (fk, _) = workloads.join_tables(50_000, 9_000_000, seed_idx=81)
+    with pytest.raises(GhbError) as e:
+        ctx.hash_join_host(bkey, fk, build_payload=bpay, capacity=1_000_000)
+    assert e.value.code == abi.ERR_CAPACITY
+    r = ctx.hash_join_host(bkey, fk, build_payload=bpay, capacity=9_000_000)
+    pr, br = oracle.hash_join(bkey, fk)
+    assert r["rows"] == len(pr) and np.array_equal(r["probe_rowid"], pr)
+    assert np.array_equal(r["build"][0][0], bpay[0][br])
