@@ -918,8 +918,69 @@ def bench_served(ctx, args, dev, n_req=300, max_rows=100_000_000, loads=(0.5, 0.
     return out
 
 
+def run_profile_case(case, reps):
+    """A small fixed case of one operator's kernels (inputs built on cuda:0,
+    the operator run `reps` times so a capture can skip the first, cold
+    launch), for ncu captures:
+
+      groupby  filter d < 1263 + GROUP BY k over the 6M-row fact table
+      gbcnt    the same table, COUNT(*) only
+      join     1.5M-key build, 20M-row probe, int64 + double build payloads
+      joinhash the same with the keys spread over the int64 range (hashed table)
+      sort     ORDER BY (d int32, k int64) with an int32 row id, 20M rows
+      batch    64 batched filter + group-by instances (rows log-U[1e3, 2e6])
+    """
+    import torch
+
+    from ghive_b200 import abi, workloads
+    from ghive_b200.ops import Context
+    ctx = Context(0)
+    dev = torch.device("cuda", 0)
+    if case in ("join", "joinhash"):
+        (bkey, bpay), (fk, _) = workloads.join_tables(N_BUILD, 20_000_000, seed_idx=1,
+                                                      sparse=case == "joinhash")
+        db = torch.from_numpy(bkey).to(dev)
+        dp = [torch.from_numpy(c).to(dev) for c in bpay]
+        df = torch.from_numpy(fk).to(dev)
+        outs = probe_outs([abi.LONG, abi.DOUBLE], 20_000_000, dev)
+        t = ctx.join_build(db, build_payload=dp)
+        for _ in range(reps):
+            ctx.join_probe(t, df, abi.INNER_JOIN, capacity=20_000_000, rowids=False, outs=outs)
+        print("rows", int(outs[4].item()))
+    elif case in ("groupby", "gbcnt"):
+        cols = [torch.from_numpy(c).to(dev) for c in workloads.fact_table(N_FACT, seed_idx=0)]
+        aggs = workloads.AGGS_FACT if case == "groupby" else [(abi.CNT, -1)]
+        for _ in range(reps):
+            _, _, g = ctx.filter_groupby(workloads.fact_predicate(), cols, [0], aggs, capacity=1000,
+                                         max_groups=1000)
+        print("groups", g)
+    elif case == "sort":
+        d, k, r = workloads.sort_table(20_000_000, seed_idx=2)
+        dd, dk, dr = (torch.from_numpy(x).to(dev) for x in (d, k, r))
+        for _ in range(reps):
+            ctx.sort([dd, dk], payload=[dr])
+        print("sorted")
+    elif case == "batch":
+        specs = workloads.batched_specs(64, seed_idx=3, max_rows=2_000_000)
+        inst = workloads.batched_instances_device(specs, dev)
+        entries = [(workloads.batched_predicate(s["cut"]), it["cols"],
+                    max(1, min(s["groups"], s["rows"])) + 8, s["groups"]) for s, it in zip(specs, inst)]
+        b = ctx.batch_groupby(entries, [0], workloads.AGGS_FACT, autotune=False, use_graph=False)
+        for _ in range(reps):
+            b.launch()
+        ctx.sync()
+        print("rows", sum(s["rows"] for s in specs))
+    else:
+        raise SystemExit("unknown profile case %r" % case)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small fixed operator case for an ncu capture and exit")
+    ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -929,6 +990,8 @@ def main():
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-served", action="store_true")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args.profile_case, args.reps)
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_init(args.gpus, args.impl)

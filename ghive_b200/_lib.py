@@ -51,6 +51,9 @@ _PROTOS = {
     "ghb_hash_join_host": (I32, [P, P, P, I32, P, I32, P, P, I32, P, P, P, I64,
                                  C.POINTER(I64), P]),
     "ghb_sort_host": (I32, [P, P, P, P, I32, P, I32, P, P, P, P]),
+    "ghb_gtables_table": (I32, [P, I32, P, I32, C.POINTER(I32), C.POINTER(I64)]),
+    "ghb_run_plan": (I32, [P, P, I32, P, I32, P]),
+    "ghb_plan_result_free": (I32, [P]),
 }
 
 

@@ -58,7 +58,8 @@ class OutColumn(C.Structure):
 class PredNode(C.Structure):
     _fields_ = [("mode", C.c_int32), ("col", C.c_int32), ("col2", C.c_int32),
                 ("lit_is_double", C.c_int32), ("child", C.c_int32 * 2),
-                ("lit_i", C.c_int64 * 2), ("lit_d", C.c_double * 2)]
+                ("lit_i", C.c_int64 * 2), ("lit_d", C.c_double * 2),
+                ("lit_s", C.c_void_p * 2), ("lit_s_len", C.c_int32 * 2)]
 
 
 class Predicate(C.Structure):
@@ -115,6 +116,33 @@ class Result(C.Structure):
                 ("slot", C.c_int32), ("reserved", C.c_int32)]
 
 
+class GTables(C.Structure):
+    """GHive's GTables with its fields read out (ghb_gtables)."""
+    _fields_ = [("ntables", C.c_int32), ("ncols", C.c_void_p), ("types", C.c_void_p),
+                ("row_cnt", C.c_void_p), ("key_cnt", C.c_void_p), ("vertex_name", C.c_void_p),
+                ("nlong", C.c_int32), ("long_cols", C.c_void_p),
+                ("ndouble", C.c_int32), ("double_cols", C.c_void_p),
+                ("nint", C.c_int32), ("int_cols", C.c_void_p),
+                ("nstring", C.c_int32), ("string_cols", C.c_void_p),
+                ("string_idx_cols", C.c_void_p)]
+
+
+class PlanOp(C.Structure):
+    _fields_ = [("op", C.c_int32), ("join_type", C.c_int32), ("pred", C.c_void_p),
+                ("idx", C.c_void_p), ("nidx", C.c_int32), ("naggs", C.c_int32),
+                ("aggs", C.c_void_p), ("max_groups", C.c_int64), ("orders", C.c_void_p),
+                ("null_orders", C.c_void_p), ("build_table", C.c_int32),
+                ("nbuild_keep", C.c_int32), ("build_keep", C.c_void_p)]
+
+
+class PlanResult(C.Structure):
+    _fields_ = [("ncols", C.c_int32), ("types", C.c_int32 * MAX_RESULT_COLS),
+                ("data", C.c_void_p * MAX_RESULT_COLS), ("is_null", C.c_void_p * MAX_RESULT_COLS),
+                ("sequence", C.c_int32 * MAX_RESULT_COLS), ("rows", C.c_int64),
+                ("n_long", C.c_int32), ("n_double", C.c_int32), ("n_int", C.c_int32),
+                ("n_string", C.c_int32)]
+
+
 class BatchCfg(C.Structure):
     _fields_ = [("autotune", C.c_int32), ("block_threads", C.c_int32),
                 ("smem_slots", C.c_int32), ("load_factor", C.c_float),
@@ -158,19 +186,28 @@ class Pred:
 
     def flatten(self):
         """Returns (nodes array, root index) in post-order."""
-        nodes = []
+        nodes, strs = [], []
 
         def rec(p):
             kids = [rec(c) for c in p.children]
             nd = PredNode()
             nd.mode, nd.col, nd.col2 = p.mode, p.col, p.col2
-            is_d = isinstance(p.a, float) or isinstance(p.b, float)
-            nd.lit_is_double = 1 if is_d else 0
-            for j, v in enumerate((p.a, p.b)):
-                if is_d:
-                    nd.lit_d[j] = float(v)
-                else:
-                    nd.lit_i[j] = int(v)
+            if isinstance(p.a, (str, bytes)) or isinstance(p.b, (str, bytes)):
+                # literals of a STRING column: their bytes, kept alive here
+                for j, v in enumerate((p.a, p.b)):
+                    b = v.encode() if isinstance(v, str) else (v if isinstance(v, bytes) else b"")
+                    buf = C.create_string_buffer(b, max(1, len(b)))
+                    strs.append(buf)
+                    nd.lit_s[j] = C.addressof(buf)
+                    nd.lit_s_len[j] = len(b)
+            else:
+                is_d = isinstance(p.a, float) or isinstance(p.b, float)
+                nd.lit_is_double = 1 if is_d else 0
+                for j, v in enumerate((p.a, p.b)):
+                    if is_d:
+                        nd.lit_d[j] = float(v)
+                    else:
+                        nd.lit_i[j] = int(v)
             nd.child[0] = kids[0] if kids else -1
             nd.child[1] = kids[1] if len(kids) > 1 else -1
             nodes.append(nd)
@@ -180,6 +217,7 @@ class Pred:
         if len(nodes) > MAX_PRED_NODES:
             raise ValueError("predicate tree has more than %d nodes" % MAX_PRED_NODES)
         arr = (PredNode * len(nodes))(*nodes)
+        arr._strs = strs   # the string literals live as long as the nodes
         return arr, root
 
     def as_struct(self):

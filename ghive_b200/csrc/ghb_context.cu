@@ -122,15 +122,23 @@ int32_t lookback_prepare(ghb_ctx* ctx, int64_t tiles, uint32_t* epoch, cudaStrea
   return GHB_OK;
 }
 
-int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, int64_t* n) {
+int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, int64_t* n, bool allow_string) {
   if (ncols < 0 || ncols > kMaxCols)
     return set_error(ctx, GHB_ERR_INVALID, "ncols=%d outside [0,%d]", ncols, kMaxCols);
   if (ncols > 0 && !cols) return set_error(ctx, GHB_ERR_INVALID, "cols is NULL");
   int64_t rows = -1;
   for (int i = 0; i < ncols; i++) {
     const ghb_column& c = cols[i];
-    if (c.type == GHB_STRING)
-      return set_error(ctx, GHB_ERR_UNSUPPORTED, "column %d: STRING columns are not on the device path", i);
+    if (c.type == GHB_STRING) {
+      if (!allow_string)
+        return set_error(ctx, GHB_ERR_UNSUPPORTED, "column %d: STRING columns are not supported here", i);
+      if (c.n > 0 && !c.aux) return set_error(ctx, GHB_ERR_INVALID, "column %d: STRING without its index", i);
+      if (rows >= 0 && c.n != rows)
+        return set_error(ctx, GHB_ERR_INVALID, "column %d has %lld rows, column 0 has %lld", i,
+                         (long long)c.n, (long long)rows);
+      rows = c.n;
+      continue;
+    }
     if (c.type != GHB_LONG && c.type != GHB_DOUBLE && c.type != GHB_INT)
       return set_error(ctx, GHB_ERR_INVALID, "column %d: unknown type %d", i, c.type);
     if (c.null_mode < GHB_NULLS_NONE || c.null_mode > GHB_NULLS_BYTEMAP)
@@ -151,7 +159,8 @@ int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, in
 // Copies the tree into a post-order program (children before parents), as
 // the device evaluator sweeps it forward.  Rejects cycles, bad indices and
 // leaves whose mode needs a literal pair that is absent.
-int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, PredProg* prog) {
+int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,
+                        PredProg* prog) {
   std::memset(prog, 0, sizeof(*prog));
   if (!pred || pred->n_nodes == 0) return GHB_OK;
   if (pred->n_nodes < 0 || pred->n_nodes > GHB_MAX_PRED_NODES || !pred->nodes)
@@ -160,6 +169,7 @@ int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, 
   if (pred->root < 0 || pred->root >= pred->n_nodes)
     return set_error(ctx, GHB_ERR_INVALID, "predicate root %d out of range", pred->root);
   std::vector<int> order, state(pred->n_nodes, 0), remap(pred->n_nodes, -1);
+  int32_t strbytes = 0;
   // iterative post-order DFS from the root
   std::vector<std::pair<int, int>> stack{{pred->root, 0}};
   while (!stack.empty()) {
@@ -201,6 +211,30 @@ int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, 
                      nd.mode == GHB_FILTER_NOT_RANGE || nd.mode == GHB_FILTER_NOT_EQ_RANGE;
       if (two_lit && nd.col2 >= 0)
         return set_error(ctx, GHB_ERR_INVALID, "node %d: range modes compare with literals only", order[k]);
+      const bool str = cols && cols[nd.col].type == GHB_STRING;
+      if (cols && nd.col2 >= 0 && (cols[nd.col2].type == GHB_STRING) != str)
+        return set_error(ctx, GHB_ERR_INVALID, "node %d: a STRING column compares with a STRING only",
+                         order[k]);
+      if (str) {
+        if (!cols[nd.col].aux || (nd.col2 >= 0 && !cols[nd.col2].aux))
+          return set_error(ctx, GHB_ERR_INVALID, "node %d: STRING column without its index", order[k]);
+        prog->has_str = 1;
+        // the literals' bytes go into the program (kernel parameter space)
+        const int nlit = nd.col2 >= 0 || nd.mode == GHB_FILTER_NOT_NULL ? 0 : (two_lit ? 2 : 1);
+        for (int j = 0; j < 2; j++) {
+          const int32_t len = j < nlit ? nd.lit_s_len[j] : 0;
+          if (len < 0 || (len > 0 && !nd.lit_s[j]))
+            return set_error(ctx, GHB_ERR_INVALID, "node %d: string literal %d without bytes", order[k], j);
+          if (strbytes + len > GHB_MAX_PRED_STR_BYTES)
+            return set_error(ctx, GHB_ERR_UNSUPPORTED, "string literals of more than %d bytes",
+                             GHB_MAX_PRED_STR_BYTES);
+          if (len) std::memcpy(prog->sbytes + strbytes, nd.lit_s[j], len);
+          nd.lit_i[j] = strbytes;
+          nd.lit_s_len[j] = len;
+          strbytes += len;
+        }
+      }
+      nd.lit_s[0] = nd.lit_s[1] = nullptr;   // host pointers never reach a kernel
     }
     prog->nodes[k] = nd;
   }

@@ -131,8 +131,14 @@ int32_t scratch_reserve(ghb_ctx* ctx, size_t total, cudaStream_t stream);
 // Look-back status array with room for `tiles` tiles, and a fresh epoch.
 int32_t lookback_prepare(ghb_ctx* ctx, int64_t tiles, uint32_t* epoch, cudaStream_t stream);
 
-int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, int64_t* n);
-int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, int32_t ncols, PredProg* prog);
+// Checks column descriptors and their common row count; STRING columns (bytes
+// + int32 [start,end) index) only where the operator takes them.
+int32_t validate_columns(ghb_ctx* ctx, const ghb_column* cols, int32_t ncols, int64_t* n,
+                         bool allow_string = false);
+// The predicate tree as a post-order program (literals of STRING leaves
+// copied into it); `cols` (nullable) gives the column types to check.
+int32_t build_pred_prog(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,
+                        PredProg* prog);
 
 inline size_t type_width(int32_t t) { return t == GHB_INT ? 4 : 8; }
 
@@ -143,6 +149,8 @@ struct KeyOuts {
 };
 struct KeyPackPlan {
   int32_t nkeys;
+  const int2* str_aux[kMaxPackKeys];   // a STRING key: its [start,end) index (the packed
+                                       // column holds the row of its value's first occurrence)
   ghb_column col[kMaxPackKeys];
   uint64_t umin[kMaxPackKeys];     // min order image of the key's non-NULL values
   int8_t vbits[kMaxPackKeys];      // value field width
@@ -159,5 +167,14 @@ int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key
 int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* packed,
                        const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
                        cudaStream_t stream);
+// A STRING column as an int64 column: each row holds the row of its value's
+// first occurrence (INT64_MAX for NULL, and for rows whose pass flag is 0);
+// `slots` (a power of two, >= twice the distinct values) of hash table in
+// `table` (cleared here).  A full table raises GHB_ERR_CAPACITY on the device.
+int32_t string_rep_rows(ghb_ctx* ctx, const ghb_column& c, const int32_t* pass, int64_t* rep,
+                        unsigned long long* table, int64_t slots, cudaStream_t stream);
+// pass[r] = 1 when row r passes the predicate program, else 0.
+int32_t predicate_pass(ghb_ctx* ctx, const PredProg& prog, const ghb_column* cols, int32_t ncols, int64_t n,
+                       int32_t* pass, cudaStream_t stream);
 
 }  // namespace ghb

@@ -42,6 +42,13 @@ struct FilterParams {
 
 __device__ __forceinline__ void copy_value(const ghb_column& c, const ghb_out_column& o, int64_t row,
                                            int64_t pos) {
+  if (c.type == GHB_STRING) {
+    // a STRING output row is the input row's [start,end) into the same bytes
+    const int2 ix = __ldg((const int2*)c.aux + row);
+    ((int2*)o.data)[pos] = ix;
+    if (o.is_null) o.is_null[pos] = ix.x < 0 ? 1 : 0;
+    return;
+  }
   if (c.type == GHB_INT) ((int32_t*)o.data)[pos] = __ldg((const int32_t*)c.data + row);
   else ((long long*)o.data)[pos] = __ldg((const long long*)c.data + row);
   if (o.is_null) {
@@ -121,7 +128,7 @@ int32_t filter_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* c
                     const int32_t* proj, int32_t nproj, ghb_out_column* out, int64_t out_capacity,
                     int64_t* d_out_rows, cudaStream_t stream) {
   int64_t n = 0;
-  int32_t st = validate_columns(ctx, cols, ncols, &n);
+  int32_t st = validate_columns(ctx, cols, ncols, &n, true);
   if (st) return st;
   if (nproj < 0 || nproj > kMaxProj) return set_error(ctx, GHB_ERR_INVALID, "nproj=%d", nproj);
   if (nproj > 0 && (!proj || !out)) return set_error(ctx, GHB_ERR_INVALID, "proj/out is NULL");
@@ -129,7 +136,7 @@ int32_t filter_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* c
   if (out_capacity < 0) return set_error(ctx, GHB_ERR_INVALID, "negative out_capacity");
   FilterParams p;
   std::memset(&p, 0, sizeof(p));
-  st = build_pred_prog(ctx, pred, ncols, &p.pred);
+  st = build_pred_prog(ctx, pred, cols, ncols, &p.pred);
   if (st) return st;
   for (int j = 0; j < nproj; j++) {
     if (proj[j] < 0 || proj[j] >= ncols)

@@ -151,7 +151,7 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
                  const ghb_out_column* out, int64_t out_capacity, int64_t* d_out_groups,
                  const GbSetup& su, GbParams* pp, FinParams* ff, size_t* table_bytes, size_t* smem) {
   int64_t n = 0;
-  int32_t st = validate_columns(ctx, cols, ncols, &n);
+  int32_t st = validate_columns(ctx, cols, ncols, &n, true);   // STRING columns only if unused
   if (st) return st;
   if (nkeys < 0 || nkeys > 1)
     return set_error(ctx, GHB_ERR_INVALID, "nkeys=%d: this kernel takes 0 or 1 key column", nkeys);
@@ -168,7 +168,7 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   std::memset(&f, 0, sizeof(f));
   st = plan_aggs(ctx, cols, ncols, aggs, naggs, out, nkeys, &p.acc, &f);
   if (st) return st;
-  st = build_pred_prog(ctx, pred, ncols, &p.pred);
+  st = build_pred_prog(ctx, pred, cols, ncols, &p.pred);
   if (st) return st;
   for (int i = 0; i < ncols; i++) p.cols.c[i] = cols[i];
   p.cols.n = ncols;
@@ -192,6 +192,10 @@ int32_t gb_setup(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols
   if (nkeys) used[key_cols[0]] = true;
   for (int a = 0; a < p.acc.n_acc; a++)
     if (p.acc.col[a] >= 0) used[p.acc.col[a]] = true;
+  for (int c = 0; c < ncols; c++)
+    if (used[c] && cols[c].type == GHB_STRING)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "column %d: a STRING column as a key, predicate or "
+                       "aggregate input of this kernel", c);
 
   int64_t max_groups = su.max_groups > 0 ? su.max_groups : out_capacity;
   if (nkeys == 0) max_groups = 1;
@@ -315,43 +319,113 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
                             const ghb_groupby_cfg* cfg, cudaStream_t stream,
                             void* fixed_table, size_t fixed_table_bytes) {
   if (!ctx) return GHB_ERR_INVALID;
-  if (nkeys > 1) {
-    // several key columns: group by their packed int64 value, then unpack
+  // STRING keys or predicate leaves, or several keys: the fold itself reads
+  // one fixed-width key and fixed-width predicate columns, so first
+  //  - a predicate with STRING leaves (or any predicate beside STRING keys)
+  //    becomes a pass flag column the fold tests for 1;
+  //  - each STRING key becomes the row of its value's first occurrence;
+  //  - several keys are packed into one int64 per row (unpacked afterwards).
+  bool str_key = false, str_pred = false;
+  if (cols && ncols > 0 && ncols <= kMaxCols) {
+    for (int j = 0; key_cols && j < nkeys; j++)
+      str_key |= key_cols[j] >= 0 && key_cols[j] < ncols && cols[key_cols[j]].type == GHB_STRING;
+    for (int k = 0; pred && pred->nodes && k < pred->n_nodes && k < GHB_MAX_PRED_NODES; k++) {
+      const ghb_pred_node& nd = pred->nodes[k];
+      if (nd.mode != GHB_FILTER_AND && nd.mode != GHB_FILTER_OR && nd.col >= 0 && nd.col < ncols)
+        str_pred |= cols[nd.col].type == GHB_STRING;
+    }
+  }
+  if (nkeys > 1 || str_key || str_pred) {
     if (fixed_table)
-      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d key columns: the allocation-free entry point takes "
-                       "at most one", nkeys);
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "the allocation-free entry point takes one fixed-width key "
+                       "and no STRING predicate");
     int64_t n = 0;
-    int32_t st = validate_columns(ctx, cols, ncols, &n);
+    int32_t st = validate_columns(ctx, cols, ncols, &n, true);
     if (st) return st;
-    if (!key_cols) return set_error(ctx, GHB_ERR_INVALID, "key_cols is NULL");
+    if (nkeys > 0 && !key_cols) return set_error(ctx, GHB_ERR_INVALID, "key_cols is NULL");
     if (!out) return set_error(ctx, GHB_ERR_INVALID, "out is NULL");
-    if (ncols + 1 > kMaxCols)
-      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d columns and a packed key exceed %d", ncols, kMaxCols);
+    if (nkeys > kMaxPackKeys)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d key columns: at most %d", nkeys, kMaxPackKeys);
+    int nstr = 0;
     for (int j = 0; j < nkeys; j++) {
       if (key_cols[j] < 0 || key_cols[j] >= ncols)
         return set_error(ctx, GHB_ERR_INVALID, "key %d: column %d out of range", j, key_cols[j]);
       if (out[j].type != cols[key_cols[j]].type || !out[j].data)
         return set_error(ctx, GHB_ERR_INVALID, "key output %d: type %d (expected %d) or no data", j,
                          out[j].type, cols[key_cols[j]].type);
+      nstr += cols[key_cols[j]].type == GHB_STRING;
     }
+    for (int a = 0; a < naggs; a++)
+      if (aggs && aggs[a].col >= 0 && aggs[a].col < ncols && cols[aggs[a].col].type == GHB_STRING)
+        return set_error(ctx, GHB_ERR_UNSUPPORTED, "aggregate %d: STRING input", a);
     if (out_capacity < 1) return set_error(ctx, GHB_ERR_INVALID, "out_capacity must be >= 1");
-    if (ctx->scratch_used == 0 &&
-        (st = scratch_reserve(ctx, keypack_scratch_bytes(n, out_capacity), stream)))
-      return st;
+    const bool use_pass = pred && pred->n_nodes > 0 && (str_pred || str_key);
+    const bool packed_key = nkeys > 1 || str_key;
+    if (ncols + (use_pass ? 1 : 0) + nstr + (packed_key ? 1 : 0) > kMaxCols)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d columns and the derived ones exceed %d", ncols, kMaxCols);
+    const int64_t hint = std::max<int64_t>(1, std::min<int64_t>(n, cfg && cfg->max_groups > 0 ? cfg->max_groups
+                                                                                            : out_capacity));
+    const int64_t slots = next_pow2_i64(std::max<int64_t>(64, 2 * hint));
+    if (ctx->scratch_used == 0) {
+      size_t need = keypack_scratch_bytes(n, out_capacity) + (size_t)n * 4 + 512 +
+                    (size_t)nstr * (((size_t)n * 8 + 255) + (size_t)slots * 8 + 512);
+      if ((st = scratch_reserve(ctx, need, stream))) return st;
+    }
+    ghb_column pc[kMaxCols];
+    for (int c = 0; c < ncols; c++) pc[c] = cols[c];
+    int32_t pn = ncols;
+    // the predicate as a pass flag column
+    ghb_pred_node pass_node;
+    ghb_predicate pass_pred{1, 0, &pass_node};
+    const ghb_predicate* fpred = pred;
+    int32_t* pass = nullptr;
+    if (use_pass) {
+      PredProg prog;
+      if ((st = build_pred_prog(ctx, pred, cols, ncols, &prog))) return st;
+      if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 4, (void**)&pass, stream))) return st;
+      if ((st = predicate_pass(ctx, prog, cols, ncols, n, pass, stream))) return st;
+      pc[pn] = ghb_column{GHB_INT, GHB_NULLS_NONE, pass, nullptr, nullptr, n};
+      std::memset(&pass_node, 0, sizeof(pass_node));
+      pass_node.mode = GHB_FILTER_EQ;
+      pass_node.col = pn;
+      pass_node.col2 = -1;
+      pass_node.lit_i[0] = 1;
+      pass_node.child[0] = pass_node.child[1] = -1;
+      fpred = &pass_pred;
+      pn++;
+    }
+    // STRING keys as the rows of their values' first occurrences
+    int32_t kc[kMaxPackKeys];
+    const int2* str_aux[kMaxPackKeys] = {nullptr};
+    for (int j = 0; j < nkeys; j++) {
+      kc[j] = key_cols[j];
+      const ghb_column& c = cols[key_cols[j]];
+      if (c.type != GHB_STRING) continue;
+      int64_t* rep = nullptr;
+      unsigned long long* table = nullptr;
+      if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 8, (void**)&rep, stream))) return st;
+      if ((st = scratch_alloc(ctx, (size_t)slots * 8, (void**)&table, stream))) return st;
+      if ((st = string_rep_rows(ctx, c, pass, rep, table, slots, stream))) return st;
+      pc[pn] = ghb_column{GHB_LONG, GHB_NULLS_SENTINEL, rep, nullptr, nullptr, n};
+      kc[j] = pn++;
+      str_aux[j] = (const int2*)c.aux;
+    }
+    if (!packed_key)   // a STRING predicate over one fixed-width key, or none
+      return filter_groupby_impl(ctx, fpred, pc, pn, kc, nkeys, aggs, naggs, out, out_capacity, d_out_groups,
+                                 cfg, stream, nullptr, 0);
     int64_t *packed = nullptr, *kout = nullptr;
     if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 8, (void**)&packed, stream))) return st;
     if ((st = scratch_alloc(ctx, (size_t)out_capacity * 8, (void**)&kout, stream))) return st;
     KeyPackPlan plan;
-    if ((st = keypack_prepare(ctx, cols, key_cols, nkeys, n, packed, &plan, stream))) return st;
-    ghb_column pc[kMaxCols];
-    for (int c = 0; c < ncols; c++) pc[c] = cols[c];
-    pc[ncols] = ghb_column{GHB_LONG, GHB_NULLS_NONE, packed, nullptr, nullptr, n};
-    ghb_out_column po[kMaxCols + kMaxAggs + 1];
+    if ((st = keypack_prepare(ctx, pc, kc, nkeys, n, packed, &plan, stream))) return st;
+    for (int j = 0; j < nkeys; j++) plan.str_aux[j] = str_aux[j];
+    pc[pn] = ghb_column{GHB_LONG, GHB_NULLS_NONE, packed, nullptr, nullptr, n};
+    ghb_out_column po[kMaxAggs + 1];
     po[0] = ghb_out_column{GHB_LONG, 0, kout, nullptr};
     for (int i = 0; i < naggs && i < kMaxAggs; i++) po[1 + i] = out[nkeys + i];
-    const int32_t pk = ncols;
-    st = filter_groupby_impl(ctx, pred, pc, ncols + 1, &pk, 1, aggs, naggs, po, out_capacity, d_out_groups,
-                             cfg, stream, nullptr, 0);
+    const int32_t pk = pn++;
+    st = filter_groupby_impl(ctx, fpred, pc, pn, &pk, 1, aggs, naggs, po, out_capacity, d_out_groups, cfg, stream,
+                             nullptr, 0);
     if (st) return st;
     return keypack_unpack(ctx, plan, kout, d_out_groups, out_capacity, out, stream);
   }

@@ -38,8 +38,11 @@ struct ColSet {
 // Predicate program: nodes in post-order (children before parents), so one
 // forward sweep evaluates the tree with a bit per node.
 struct PredProg {
-  ghb_pred_node nodes[GHB_MAX_PRED_NODES];
+  ghb_pred_node nodes[GHB_MAX_PRED_NODES];   // a STRING leaf's literal k is
+                                             // sbytes[lit_i[k]], lit_s_len[k] bytes
   int32_t n_nodes;   // 0 = no predicate (all rows pass)
+  int32_t has_str;   // some leaf reads a STRING column
+  uint8_t sbytes[GHB_MAX_PRED_STR_BYTES];
 };
 
 // ----------------------------------------------------------- status
@@ -96,10 +99,54 @@ __device__ __forceinline__ bool cmp_mode(int mode, T x, T a, T b) {
   return false;
 }
 
+// Hive's StringExpr.compare: unsigned bytes, then length.
+__device__ __forceinline__ int str_compare(const uint8_t* a, int la, const uint8_t* b, int lb) {
+  const int m = la < lb ? la : lb;
+  for (int k = 0; k < m; k++)
+    if (a[k] != b[k]) return (int)a[k] - (int)b[k];
+  return la - lb;
+}
+
+// A leaf on a STRING column (data: bytes, aux: int32 [start,end) per row,
+// start < 0 = NULL), against the program's literals or another STRING column.
+static __device__ __noinline__ bool eval_str_leaf(const PredProg& p, const ghb_pred_node& nd, const ColSet& cs,
+                                           int64_t i) {
+  const ghb_column& c = cs.c[nd.col];
+  const int2 ix = ((const int2*)c.aux)[i];
+  if (ix.x < 0) return false;
+  if (nd.mode == GHB_FILTER_NOT_NULL) return true;
+  const uint8_t* x = (const uint8_t*)c.data + ix.x;
+  int ca, cb = 0;
+  if (nd.col2 >= 0) {
+    const ghb_column& c2 = cs.c[nd.col2];
+    const int2 iy = ((const int2*)c2.aux)[i];
+    if (iy.x < 0) return false;
+    ca = str_compare(x, ix.y - ix.x, (const uint8_t*)c2.data + iy.x, iy.y - iy.x);
+  } else {
+    ca = str_compare(x, ix.y - ix.x, p.sbytes + nd.lit_i[0], nd.lit_s_len[0]);
+    cb = str_compare(x, ix.y - ix.x, p.sbytes + nd.lit_i[1], nd.lit_s_len[1]);
+  }
+  switch (nd.mode) {
+    case GHB_FILTER_EQ: return ca == 0;
+    case GHB_FILTER_LE: return ca <= 0;
+    case GHB_FILTER_GE: return ca >= 0;
+    case GHB_FILTER_LT: return ca < 0;
+    case GHB_FILTER_GT: return ca > 0;
+    case GHB_FILTER_RANGE: return ca > 0 && cb < 0;
+    case GHB_FILTER_EQ_RANGE: return ca >= 0 && cb <= 0;
+    case GHB_FILTER_NOT_EQ: return ca != 0;
+    case GHB_FILTER_NOT_RANGE: return ca < 0 || cb > 0;
+    case GHB_FILTER_NOT_EQ_RANGE: return ca <= 0 || cb >= 0;
+  }
+  return false;
+}
+
 // One leaf of FilterPredicate (FilterPredicate.hpp:119-385 functors, with
 // Hive's NULL rule: a NULL operand never passes).
-__device__ __forceinline__ bool eval_leaf(const ghb_pred_node& nd, const ColSet& cs, int64_t i) {
+__device__ __forceinline__ bool eval_leaf(const PredProg& p, const ghb_pred_node& nd, const ColSet& cs,
+                                          int64_t i) {
   const ghb_column& c = cs.c[nd.col];
+  if (p.has_str && c.type == GHB_STRING) return eval_str_leaf(p, nd, cs, i);
   int64_t x = ld_raw(c, i);
   if (raw_is_null(c, x, i)) return false;
   if (nd.mode == GHB_FILTER_NOT_NULL) return true;
@@ -123,7 +170,7 @@ __device__ __forceinline__ bool eval_leaf(const ghb_pred_node& nd, const ColSet&
 // AND/OR reads its children's bits that were set earlier in the sweep.
 __device__ __forceinline__ bool eval_pred(const PredProg& p, const ColSet& cs, int64_t i) {
   if (p.n_nodes == 0) return true;
-  if (p.n_nodes == 1) return eval_leaf(p.nodes[0], cs, i);
+  if (p.n_nodes == 1) return eval_leaf(p, p.nodes[0], cs, i);
   uint32_t bits = 0;
   for (int k = 0; k < p.n_nodes; k++) {
     const ghb_pred_node& nd = p.nodes[k];
@@ -133,7 +180,7 @@ __device__ __forceinline__ bool eval_pred(const PredProg& p, const ColSet& cs, i
     else if (nd.mode == GHB_FILTER_OR)
       r = (((bits >> nd.child[0]) | (bits >> nd.child[1])) & 1u) != 0;
     else
-      r = eval_leaf(nd, cs, i);
+      r = eval_leaf(p, nd, cs, i);
     bits |= (uint32_t)r << k;
   }
   return (bits >> (p.n_nodes - 1)) & 1u;

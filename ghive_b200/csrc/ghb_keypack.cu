@@ -114,6 +114,12 @@ __global__ void __launch_bounds__(256) keypack_unpack_kernel(KeyPackPlan p, cons
       const int vb = p.vbits[j];
       const uint64_t field = vb == 0 ? 0 : (v >> p.vshift[j]) & ((1ull << vb) - 1);
       const uint64_t img = field + p.umin[j];
+      if (p.str_aux[j]) {   // the row of the value's first occurrence -> its bytes
+        const int2 ix = null ? make_int2(-1, -1) : p.str_aux[j][(int64_t)(img ^ 0x8000000000000000ull)];
+        ((int2*)o.data)[r] = ix;
+        if (o.is_null) o.is_null[r] = null ? 1 : 0;
+        continue;
+      }
       const int64_t raw = o.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(img)
                                                : (int64_t)(img ^ 0x8000000000000000ull);
       if (o.is_null) o.is_null[r] = null ? 1 : 0;
@@ -124,6 +130,90 @@ __global__ void __launch_bounds__(256) keypack_unpack_kernel(KeyPackPlan p, cons
       }
     }
   }
+}
+
+// FNV-1a, 64-bit (Fowler, Noll and Vo's published hash), then a 64-bit mixer.
+__device__ __forceinline__ uint64_t string_hash(const uint8_t* b, int len) {
+  uint64_t h = 1469598103934665603ull;
+  for (int k = 0; k < len; k++) {
+    h ^= b[k];
+    h *= 1099511628211ull;
+  }
+  return mix64(h);
+}
+
+// Row of each row's value's first occurrence, through a lock-free table of
+// (hash tag << 32 | row + 1) words: the first row of a value claims a slot by
+// CAS; the bytes a slot stands for are that row's own, so a later row with
+// the same tag compares bytes with it directly.
+__global__ void __launch_bounds__(256) string_rep_kernel(ghb_column c, const int32_t* pass, int64_t* rep,
+                                                          unsigned long long* table, int64_t mask,
+                                                          int32_t* status) {
+  const int2* aux = (const int2*)c.aux;
+  const uint8_t* bytes = (const uint8_t*)c.data;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < c.n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int2 ix = aux[r];
+    if (ix.x < 0 || (pass && pass[r] == 0)) {
+      rep[r] = INT64_MAX;
+      continue;
+    }
+    const uint8_t* b = bytes + ix.x;
+    const int len = ix.y - ix.x;
+    const uint64_t h = string_hash(b, len);
+    const uint32_t tag = (uint32_t)(h >> 32) | 1u;
+    const unsigned long long mine = ((unsigned long long)tag << 32) | (unsigned long long)(r + 1);
+    int64_t s = (int64_t)(h & (uint64_t)mask), found = -1;
+    for (int64_t probe = 0; probe <= mask; probe++) {
+      unsigned long long w = *(volatile unsigned long long*)&table[s];
+      if (w == 0) {
+        const unsigned long long old = atomicCAS(&table[s], 0ull, mine);
+        if (old == 0) {
+          found = r;
+          break;
+        }
+        w = old;
+      }
+      if ((uint32_t)(w >> 32) == tag) {
+        const int64_t o = (int64_t)(w & 0xffffffffull) - 1;
+        const int2 io = aux[o];
+        if (io.y - io.x == len && str_compare(bytes + io.x, len, b, len) == 0) {
+          found = o;
+          break;
+        }
+      }
+      s = (s + 1) & mask;
+    }
+    if (found < 0) raise_status(status, kDevCapacity);   // more distinct values than slots
+    rep[r] = found < 0 ? INT64_MAX : found;
+  }
+}
+
+__global__ void __launch_bounds__(256) predicate_pass_kernel(PredProg prog, ColSet cs, int64_t n, int32_t* pass) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    pass[r] = eval_pred(prog, cs, r) ? 1 : 0;
+}
+
+int32_t string_rep_rows(ghb_ctx* ctx, const ghb_column& c, const int32_t* pass, int64_t* rep,
+                        unsigned long long* table, int64_t slots, cudaStream_t stream) {
+  if (c.n >= (int64_t)UINT32_MAX - 1) return set_error(ctx, GHB_ERR_UNSUPPORTED, "STRING key of 2^32 rows");
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(table, 0, (size_t)slots * 8, stream));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((c.n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  string_rep_kernel<<<grid, 256, 0, stream>>>(c, pass, rep, table, slots - 1, ctx->d_status);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+int32_t predicate_pass(ghb_ctx* ctx, const PredProg& prog, const ghb_column* cols, int32_t ncols, int64_t n,
+                       int32_t* pass, cudaStream_t stream) {
+  ColSet cs;
+  std::memset(&cs, 0, sizeof(cs));
+  for (int i = 0; i < ncols; i++) cs.c[i] = cols[i];
+  cs.n = ncols;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  predicate_pass_kernel<<<grid, 256, 0, stream>>>(prog, cs, n, pass);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
 }
 
 // Plans the packing of the key columns and writes the packed keys (n int64

@@ -1,0 +1,392 @@
+// ghb_plan.cu — GHive's JNI marshaling (GTables in, GPUResult out) and a
+// vertex's operator chain run on device-resident intermediates.
+//
+// GHive's entry point GPUProcess (gpu_impl/src/ghive_JNIInterface.cu:13-215)
+// reads the Tez task's GTables object: per input table its column types,
+// row and key counts, and the columns as direct ByteBuffers, concatenated by
+// type over the tables in table order (each table takes its columns, in its
+// types[] order, from the next unused buffer of the type, :152-201).  It then
+// runs the vertex's plan, root_op->execute() (gpu_impl/src/Parser/
+// Parser.cu:675), where every operator copies its input in and its output
+// back to host columns (FilterOperator.cu:53-89, GroupByPredicate.cu:39-91),
+// and builds a GPUResult: the result's columns grouped by type (long[][],
+// double[][], int[][], String[][]) and sequence[i] = the index of result
+// column i in the concatenation long || double || int || string
+// (ghive_JNIInterface.cu:217-340).
+//
+// Here:
+//   ghb_gtables_table   one input table's columns as descriptors over the
+//                       JVM's buffers (no copy), NULLs as GHive's sentinels;
+//   ghb_run_plan        the vertex's chain of operators on one input table
+//                       (and build tables made from the others): the input
+//                       columns are copied to the device once, each
+//                       operator's output stays on the device as the next
+//                       one's input, and only the final table comes back,
+//                       with GPUResult's grouping and sequence.
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
+#include "ghb_ctx.hpp"
+
+namespace ghb {
+namespace {
+
+size_t width_of(int32_t t) { return type_width(t); }
+
+// A device column the plan owns.
+struct DevCol {
+  int32_t type = GHB_LONG;
+  void* data = nullptr;
+  uint8_t* is_null = nullptr;   // NULL map (nullptr: no NULLs, or sentinels)
+  int32_t null_mode = GHB_NULLS_NONE;
+};
+
+struct DevTable {
+  std::vector<DevCol> cols;
+  int64_t rows = 0;
+};
+
+struct Plan {
+  ghb_ctx* ctx;
+  cudaStream_t s;
+  std::vector<void*> owned;
+
+  ~Plan() {
+    cudaStreamSynchronize(s);
+    for (void* p : owned) cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+  }
+  int32_t alloc(size_t bytes, void** out) {
+    *out = nullptr;
+    if (cudaMallocAsync(out, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate %zu bytes of device memory", bytes);
+    }
+    owned.push_back(*out);
+    return GHB_OK;
+  }
+  // an output column of `rows` rows with a NULL map
+  int32_t out_col(int32_t type, int64_t rows, DevCol* c, ghb_out_column* o) {
+    int32_t st;
+    c->type = type;
+    if ((st = alloc((size_t)std::max<int64_t>(rows, 1) * width_of(type), &c->data))) return st;
+    if ((st = alloc((size_t)std::max<int64_t>(rows, 1), (void**)&c->is_null))) return st;
+    c->null_mode = GHB_NULLS_BYTEMAP;
+    *o = ghb_out_column{type, 0, c->data, c->is_null};
+    return GHB_OK;
+  }
+  int32_t read_count(const int64_t* d, int64_t* h) {
+    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(h, d, 8, cudaMemcpyDeviceToHost, s));
+    return ghb_sync(ctx, s);
+  }
+};
+
+ghb_column desc(const DevCol& c, int64_t rows) {
+  return ghb_column{c.type, c.null_mode, c.data, c.null_mode == GHB_NULLS_BYTEMAP ? c.is_null : nullptr,
+                    nullptr, rows};
+}
+
+// Copies host table columns to the device (GHive's sentinels kept).
+int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTable* t) {
+  t->rows = rows;
+  t->cols.assign(ncols, DevCol{});
+  for (int c = 0; c < ncols; c++) {
+    if (h[c].type == GHB_STRING)
+      return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "column %d: STRING columns are not on the device path", c);
+    DevCol& d = t->cols[c];
+    d.type = h[c].type;
+    d.null_mode = h[c].null_mode;
+    int32_t st = P.alloc((size_t)std::max<int64_t>(rows, 1) * width_of(d.type), &d.data);
+    if (st) return st;
+    if (rows > 0) {
+      if (!h[c].data) return set_error(P.ctx, GHB_ERR_INVALID, "column %d: data is NULL", c);
+      GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.data, h[c].data, rows * width_of(d.type), cudaMemcpyHostToDevice, P.s));
+    }
+    if (h[c].null_mode == GHB_NULLS_BYTEMAP) {
+      if ((st = P.alloc((size_t)std::max<int64_t>(rows, 1), (void**)&d.is_null))) return st;
+      if (rows > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.is_null, h[c].is_null, rows, cudaMemcpyHostToDevice, P.s));
+    }
+  }
+  return GHB_OK;
+}
+
+std::vector<ghb_column> descs(const DevTable& t) {
+  std::vector<ghb_column> v;
+  for (const DevCol& c : t.cols) v.push_back(desc(c, t.rows));
+  return v;
+}
+
+int32_t run_filter(Plan& P, const ghb_plan_op& op, DevTable& t) {
+  std::vector<ghb_column> in = descs(t);
+  std::vector<int32_t> proj;
+  if (op.idx)
+    proj.assign(op.idx, op.idx + op.nidx);
+  else
+    for (int c = 0; c < (int)t.cols.size(); c++) proj.push_back(c);
+  if (proj.size() > (size_t)kMaxCols) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "projection of %zu columns", proj.size());
+  for (int32_t c : proj)
+    if (c < 0 || c >= (int)t.cols.size()) return set_error(P.ctx, GHB_ERR_INVALID, "projection column %d", c);
+  DevTable o;
+  std::vector<ghb_out_column> out(proj.size());
+  o.cols.resize(proj.size());
+  int32_t st;
+  for (size_t j = 0; j < proj.size(); j++)
+    if ((st = P.out_col(t.cols[proj[j]].type, t.rows, &o.cols[j], &out[j]))) return st;
+  int64_t* d_rows = nullptr;
+  if ((st = P.alloc(8, (void**)&d_rows))) return st;
+  if ((st = ghb_filter(P.ctx, op.pred, in.data(), (int32_t)in.size(), proj.data(), (int32_t)proj.size(),
+                       out.data(), t.rows, d_rows, P.s)))
+    return st;
+  if ((st = P.read_count(d_rows, &o.rows))) return st;
+  t = std::move(o);
+  return GHB_OK;
+}
+
+int32_t agg_type(int32_t agg, int32_t in) {
+  if (agg == GHB_AGG_CNT) return GHB_LONG;
+  if (agg == GHB_AGG_AVG) return GHB_DOUBLE;
+  if (agg == GHB_AGG_SUM) return in == GHB_DOUBLE ? GHB_DOUBLE : GHB_LONG;
+  return in;
+}
+
+int32_t run_groupby(Plan& P, const ghb_plan_op& op, DevTable& t) {
+  std::vector<ghb_column> in = descs(t);
+  const int32_t nkeys = op.nidx, naggs = op.naggs;
+  if (nkeys < 0 || naggs < 0 || nkeys + naggs > GHB_MAX_RESULT_COLS || (nkeys > 0 && !op.idx) ||
+      (naggs > 0 && !op.aggs))
+    return set_error(P.ctx, GHB_ERR_INVALID, "group-by: %d keys, %d aggregates", nkeys, naggs);
+  int64_t cap = nkeys == 0 ? 1 : (op.max_groups > 0 ? op.max_groups : std::max<int64_t>(t.rows, 1));
+  DevTable o;
+  o.cols.resize(nkeys + naggs);
+  std::vector<ghb_out_column> out(nkeys + naggs);
+  int32_t st;
+  for (int j = 0; j < nkeys; j++) {
+    if (op.idx[j] < 0 || op.idx[j] >= (int)t.cols.size())
+      return set_error(P.ctx, GHB_ERR_INVALID, "group-by key column %d", op.idx[j]);
+    if ((st = P.out_col(t.cols[op.idx[j]].type, cap, &o.cols[j], &out[j]))) return st;
+  }
+  for (int a = 0; a < naggs; a++) {
+    const int32_t c = op.aggs[a].col;
+    const int32_t in_t = c >= 0 && c < (int)t.cols.size() ? t.cols[c].type : GHB_LONG;
+    if ((st = P.out_col(agg_type(op.aggs[a].type, in_t), cap, &o.cols[nkeys + a], &out[nkeys + a]))) return st;
+  }
+  int64_t* d_groups = nullptr;
+  if ((st = P.alloc(8, (void**)&d_groups))) return st;
+  ghb_groupby_cfg cfg{};
+  cfg.max_groups = cap;
+  if ((st = ghb_filter_groupby(P.ctx, nullptr, in.data(), (int32_t)in.size(), op.idx, nkeys, op.aggs, naggs,
+                               out.data(), cap, d_groups, &cfg, P.s)))
+    return st;
+  if ((st = P.read_count(d_groups, &o.rows))) return st;
+  t = std::move(o);
+  return GHB_OK;
+}
+
+// The current table probes a hash table built from input table op.build_table:
+// output = the current table's columns, then the kept build columns.
+int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable& t) {
+  if (!op.idx || op.nidx != 2)
+    return set_error(P.ctx, GHB_ERR_INVALID, "join: idx must hold the probe and the build key column");
+  ghb_column hb[kMaxCols];
+  int32_t nb = 0;
+  int64_t brows = 0;
+  int32_t st = ghb_gtables_table(in, op.build_table, hb, kMaxCols, &nb, &brows);
+  if (st) return set_error(P.ctx, st, "join: build table %d is missing or malformed", op.build_table);
+  const int32_t pk = op.idx[0], bk = op.idx[1];
+  if (pk < 0 || pk >= (int)t.cols.size() || bk < 0 || bk >= nb)
+    return set_error(P.ctx, GHB_ERR_INVALID, "join key columns %d / %d", pk, bk);
+  if ((int)t.cols.size() > 8 || op.nbuild_keep > 8 || op.nbuild_keep < 0)
+    return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "join: at most 8 columns from each side");
+  // the build side's key and kept columns on the device
+  std::vector<ghb_column> bsel;
+  bsel.push_back(hb[bk]);
+  for (int j = 0; j < op.nbuild_keep; j++) {
+    const int32_t c = op.build_keep[j];
+    if (c < 0 || c >= nb) return set_error(P.ctx, GHB_ERR_INVALID, "join: build column %d", c);
+    bsel.push_back(hb[c]);
+  }
+  DevTable b;
+  if ((st = upload(P, bsel.data(), (int32_t)bsel.size(), brows, &b))) return st;
+  std::vector<ghb_column> bd = descs(b);
+  ghb_join_table* jt = nullptr;
+  if ((st = ghb_join_build(P.ctx, &bd[0], bd.data() + 1, op.nbuild_keep, nullptr, &jt, P.s))) return st;
+  int64_t rows = 0, max_dup = 1, slots = 0;
+  if ((st = ghb_sync(P.ctx, P.s)) || (st = ghb_join_table_info(P.ctx, jt, &rows, &max_dup, &slots))) {
+    ghb_join_table_free(P.ctx, jt);
+    return st;
+  }
+  int64_t per = op.join_type == GHB_LEFT_SEMI_JOIN ? 1 : std::max<int64_t>(1, max_dup);
+  const int64_t cap = std::max<int64_t>(1, t.rows * per);
+  std::vector<ghb_column> probe = descs(t);
+  DevTable o;
+  const int np = (int)t.cols.size();
+  o.cols.resize(np + op.nbuild_keep);
+  std::vector<ghb_out_column> op_out(np), ob_out(op.nbuild_keep);
+  for (int j = 0; j < np && !st; j++) st = P.out_col(t.cols[j].type, cap, &o.cols[j], &op_out[j]);
+  for (int j = 0; j < op.nbuild_keep && !st; j++)
+    st = P.out_col(b.cols[1 + j].type, cap, &o.cols[np + j], &ob_out[j]);
+  int64_t* d_rows = nullptr;
+  if (!st) st = P.alloc(8, (void**)&d_rows);
+  if (!st)
+    st = ghb_join_probe(P.ctx, jt, &probe[pk], op.join_type, ob_out.data(), probe.data(), np, op_out.data(),
+                        nullptr, nullptr, cap, d_rows, P.s);
+  if (!st) st = P.read_count(d_rows, &o.rows);
+  ghb_join_table_free(P.ctx, jt);
+  if (st) return st;
+  t = std::move(o);
+  return GHB_OK;
+}
+
+// ORDER BY: the key columns first, then the others (GHive's Sink keeps that
+// order, SinkOperator.cu:98-306).
+int32_t run_sort(Plan& P, const ghb_plan_op& op, DevTable& t) {
+  if (!op.idx || op.nidx < 1) return set_error(P.ctx, GHB_ERR_INVALID, "sort without keys");
+  std::vector<ghb_column> in = descs(t);
+  std::vector<bool> is_key(t.cols.size(), false);
+  std::vector<ghb_column> keys, pay;
+  std::vector<int32_t> pay_idx;
+  for (int j = 0; j < op.nidx; j++) {
+    const int32_t c = op.idx[j];
+    if (c < 0 || c >= (int)t.cols.size() || is_key[c])
+      return set_error(P.ctx, GHB_ERR_INVALID, "sort key column %d", c);
+    is_key[c] = true;
+    keys.push_back(in[c]);
+  }
+  for (int c = 0; c < (int)t.cols.size(); c++)
+    if (!is_key[c]) {
+      pay.push_back(in[c]);
+      pay_idx.push_back(c);
+    }
+  DevTable o;
+  o.rows = t.rows;
+  o.cols.resize(t.cols.size());
+  std::vector<ghb_out_column> ok(keys.size()), opay(pay.size());
+  int32_t st;
+  for (size_t j = 0; j < keys.size(); j++)
+    if ((st = P.out_col(keys[j].type, t.rows, &o.cols[j], &ok[j]))) return st;
+  for (size_t j = 0; j < pay.size(); j++)
+    if ((st = P.out_col(pay[j].type, t.rows, &o.cols[keys.size() + j], &opay[j]))) return st;
+  if ((st = ghb_sort(P.ctx, keys.data(), op.orders, op.null_orders, (int32_t)keys.size(), pay.data(),
+                     (int32_t)pay.size(), ok.data(), opay.data(), nullptr, nullptr, P.s)))
+    return st;
+  if ((st = ghb_sync(P.ctx, P.s))) return st;
+  t = std::move(o);
+  return GHB_OK;
+}
+
+}  // namespace
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" {
+
+int32_t ghb_gtables_table(const ghb_gtables* in, int32_t table, ghb_column* cols, int32_t cap,
+                          int32_t* ncols, int64_t* rows) {
+  if (!in || !ncols || table < 0 || table >= in->ntables || !in->ncols || !in->types || !in->row_cnt)
+    return GHB_ERR_INVALID;
+  if (in->vertex_name && !in->vertex_name[table]) return GHB_ERR_INVALID;   // the table is missing
+  // the next unused buffer of each type: the tables before this one took theirs
+  int32_t next[4] = {0, 0, 0, 0};
+  for (int t = 0; t < table; t++)
+    for (int c = 0; c < in->ncols[t]; c++) {
+      const int32_t ty = in->types[t][c];
+      if (ty < 0 || ty > 3) return GHB_ERR_INVALID;
+      next[ty]++;
+    }
+  const int32_t n = in->ncols[table];
+  if (n > cap) return GHB_ERR_INVALID;
+  const int64_t r = in->row_cnt[table];
+  const int32_t have[4] = {in->nlong, in->ndouble, in->nint, in->nstring};
+  const void* const* bufs[4] = {in->long_cols, in->double_cols, in->int_cols, in->string_cols};
+  for (int c = 0; c < n; c++) {
+    const int32_t ty = in->types[table][c];
+    if (ty < 0 || ty > 3 || next[ty] >= have[ty] || !bufs[ty]) return GHB_ERR_INVALID;
+    ghb_column& d = cols[c];
+    d.type = ty;
+    d.null_mode = GHB_NULLS_SENTINEL;
+    d.data = bufs[ty][next[ty]];
+    d.is_null = nullptr;
+    d.aux = ty == GHB_STRING && in->string_idx_cols ? in->string_idx_cols[next[ty]] : nullptr;
+    d.n = r;
+    next[ty]++;
+  }
+  *ncols = n;
+  if (rows) *rows = r;
+  return GHB_OK;
+}
+
+int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const ghb_plan_op* ops,
+                     int32_t nops, ghb_plan_result* out) {
+  if (!ctx || !in || !out || (nops > 0 && !ops) || nops < 0) return GHB_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  ghb_column hc[kMaxCols];
+  int32_t nc = 0;
+  int64_t rows = 0;
+  if (ghb_gtables_table(in, input, hc, kMaxCols, &nc, &rows))
+    return set_error(ctx, GHB_ERR_INVALID, "input table %d is missing or malformed", input);
+  if (!ctx->hstream[1]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[1], cudaStreamNonBlocking));
+  Plan P{ctx, ctx->hstream[1], {}};
+  DevTable t;
+  int32_t st = upload(P, hc, nc, rows, &t);
+  if (st) return st;
+  for (int i = 0; i < nops && !st; i++) {
+    switch (ops[i].op) {
+      case GHB_OP_FILTER: st = run_filter(P, ops[i], t); break;
+      case GHB_OP_GROUPBY: st = run_groupby(P, ops[i], t); break;
+      case GHB_OP_JOIN_PROBE: st = run_join(P, ops[i], in, t); break;
+      case GHB_OP_SORT: st = run_sort(P, ops[i], t); break;
+      default: st = set_error(ctx, GHB_ERR_INVALID, "plan op %d: unknown operator %d", i, ops[i].op);
+    }
+  }
+  if (st) return st;
+  if ((int)t.cols.size() > GHB_MAX_RESULT_COLS)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "result of %zu columns", t.cols.size());
+  // the result: host columns (NULLs as GHive's sentinels, and a NULL map),
+  // grouped by type the way GPUResult holds them
+  out->ncols = (int32_t)t.cols.size();
+  out->rows = t.rows;
+  int32_t count[4] = {0, 0, 0, 0};
+  for (const DevCol& c : t.cols) count[c.type]++;
+  out->n_long = count[GHB_LONG];
+  out->n_double = count[GHB_DOUBLE];
+  out->n_int = count[GHB_INT];
+  out->n_string = count[GHB_STRING];
+  const int32_t base[4] = {0, count[0], count[0] + count[1], count[0] + count[1] + count[2]};
+  int32_t seen[4] = {0, 0, 0, 0};
+  for (int c = 0; c < out->ncols; c++) {
+    const DevCol& d = t.cols[c];
+    out->types[c] = d.type;
+    out->sequence[c] = base[d.type] + seen[d.type]++;
+    const size_t bytes = (size_t)std::max<int64_t>(t.rows, 1) * width_of(d.type);
+    if (cudaMallocHost(&out->data[c], bytes) != cudaSuccess ||
+        (d.is_null && cudaMallocHost((void**)&out->is_null[c], std::max<int64_t>(t.rows, 1)) != cudaSuccess)) {
+      cudaGetLastError();
+      ghb_plan_result_free(out);
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned host memory for the result");
+    }
+    if (t.rows > 0) {
+      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out->data[c], d.data, t.rows * width_of(d.type), cudaMemcpyDeviceToHost, P.s));
+      if (d.is_null)
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out->is_null[c], d.is_null, t.rows, cudaMemcpyDeviceToHost, P.s));
+    }
+  }
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(P.s));
+  return GHB_OK;
+}
+
+int32_t ghb_plan_result_free(ghb_plan_result* r) {
+  if (!r) return GHB_ERR_INVALID;
+  for (int c = 0; c < GHB_MAX_RESULT_COLS; c++) {
+    if (r->data[c]) cudaFreeHost(r->data[c]);
+    if (r->is_null[c]) cudaFreeHost(r->is_null[c]);
+    r->data[c] = nullptr;
+    r->is_null[c] = nullptr;
+  }
+  r->ncols = 0;
+  r->rows = 0;
+  return GHB_OK;
+}
+
+}  // extern "C"

@@ -34,6 +34,8 @@ class Sentinel:
 
 
 def _split(c):
+    if isinstance(c, tuple) and len(c) == 3 and isinstance(c[0], str) and c[0] == "string":
+        return c, None, abi.NULLS_NONE
     if isinstance(c, Sentinel):
         return c.values, None, abi.NULLS_SENTINEL
     if isinstance(c, tuple):
@@ -63,6 +65,14 @@ class _Cols:
         descs = []
         for c in cols:
             v, isnull, mode = _split(c)
+            if isinstance(v, tuple):   # ("string", utf-8 bytes, int32 [start,end) pairs)
+                _, chars, idx = v
+                d = abi.Column()
+                d.type, d.null_mode = abi.STRING, abi.NULLS_NONE
+                d.data, d.aux, d.n = _ptr(chars), _ptr(idx), len(idx) // 2
+                self.keep += [chars, idx]
+                descs.append(d)
+                continue
             if torch is not None and isinstance(v, torch.Tensor):
                 v = v.contiguous()
                 if isnull is not None:
@@ -95,6 +105,16 @@ class _Outs:
         descs = []
         for t in types:
             n = max(1, cap)
+            if t == abi.STRING:   # [start,end) pairs into the input column's bytes
+                data = torch.empty(2 * n, dtype=torch.int32, device=device) if device is not None else \
+                    np.empty(2 * n, dtype=np.int32)
+                nul = (torch.empty(n, dtype=torch.uint8, device=device) if device is not None else
+                       np.empty(n, dtype=np.uint8)) if with_nulls else None
+                o = abi.OutColumn()
+                o.type, o.data, o.is_null = t, _ptr(data), _ptr(nul)
+                descs.append(o)
+                self.cols.append((data, nul))
+                continue
             if device is not None:
                 data = torch.empty(n, dtype=_TYPE_TORCH[t], device=device)
                 nul = torch.empty(n, dtype=torch.uint8, device=device) if with_nulls else None
@@ -112,8 +132,12 @@ class _Outs:
         return C.addressof(self.arr)
 
     def rows(self, k):
-        return [(d[:k], None if nl is None else nl[:k].bool() if torch is not None and
-                 isinstance(nl, torch.Tensor) else nl[:k].astype(bool)) for d, nl in self.cols]
+        out = []
+        for (d, nl), o in zip(self.cols, self.arr):
+            d = d[:2 * k] if o.type == abi.STRING else d[:k]
+            out.append((d, None if nl is None else nl[:k].bool() if torch is not None and
+                        isinstance(nl, torch.Tensor) else nl[:k].astype(bool)))
+        return out
 
 
 def _pred(pred):

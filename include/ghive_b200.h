@@ -60,7 +60,10 @@ extern "C" {
 #define GHB_LONG    0   /* int64  (Hive LongColumnVector.vector)   */
 #define GHB_DOUBLE  1   /* double (Hive DoubleColumnVector.vector) */
 #define GHB_INT     2   /* int32  (GHive INT column)               */
-#define GHB_STRING  3   /* UTF-8 blob + int32 [start,end) pairs in aux; oracle only */
+#define GHB_STRING  3   /* data: UTF-8 bytes; aux: int32 [start,end) per row,
+                            start < 0 = NULL (GTable.java:240-257).  As an
+                            output column: data holds the int32 [start,end)
+                            pairs into the input column's bytes */
 
 /* ---- NULL conventions ---------------------------------------------------- */
 #define GHB_NULLS_NONE      0  /* Hive noNulls == true                                   */
@@ -136,7 +139,12 @@ typedef struct ghb_out_column {
  * col2 >= 0 (column-vs-column; only the binary compare modes).  A literal is
  * read as double when lit_is_double != 0, else as int64; the comparison runs
  * in double when either side is double (Java binary numeric promotion), else
- * in int64.  AND/OR nodes name two children by node index. */
+ * in int64.  A leaf on a STRING column compares with the byte strings
+ * lit_s[k] (lit_s_len[k] bytes, not NUL-terminated; at most
+ * GHB_MAX_PRED_STR_BYTES over a tree) as Hive's StringExpr.compare does
+ * (storage-api/.../StringExpr.java:37-47: unsigned bytes, then length; GHive's
+ * filter_str_unary_* functors, FilterPredicate.hpp:416-683, compare signed
+ * chars instead).  AND/OR nodes name two children by node index. */
 typedef struct ghb_pred_node {
   int32_t mode;
   int32_t col;
@@ -145,7 +153,10 @@ typedef struct ghb_pred_node {
   int32_t child[2];
   int64_t lit_i[2];
   double lit_d[2];
+  const char* lit_s[2];
+  int32_t lit_s_len[2];
 } ghb_pred_node;
+#define GHB_MAX_PRED_STR_BYTES 512
 
 typedef struct ghb_predicate {
   int32_t n_nodes;   /* <= GHB_MAX_PRED_NODES */
@@ -219,7 +230,9 @@ int32_t ghb_ctx_set_spin_limit(ghb_ctx* ctx, int32_t polls);
  * FilterOperator::clean_data (FilterOperator.cu:36-93): evaluates the
  * predicate tree on `cols` and writes the selected rows of the columns listed
  * in `proj` (indices into cols) to `out[0..nproj)`, in input order.  The
- * inputs are not modified (the reference compacted them in place).
+ * inputs are not modified (the reference compacted them in place).  STRING
+ * columns may be predicate leaves and projections (a projected STRING row
+ * is its [start,end) pair into the input's bytes, GPU memory read only).
  * d_out_rows (device int64) receives the number of selected rows.  Rows
  * beyond out_capacity are counted but not written; ghb_sync then returns
  * GHB_ERR_CAPACITY. */
@@ -236,7 +249,15 @@ int32_t ghb_filter(ghb_ctx* ctx, const ghb_predicate* pred,
  * out[0..nkeys) = group keys, out[nkeys..nkeys+naggs) = aggregates, one row
  * per group in unspecified order (Hive's HashMap order is unspecified too).
  * With nkeys == 0 the result is one row (Hive's global aggregate, also on an
- * empty input).  d_out_groups (device int64) receives the group count. */
+ * empty input).  d_out_groups (device int64) receives the group count.
+ * Several key columns (GroupByPredicate.cu:24-105 sorts by all of them) are
+ * packed into one 64-bit key per row after one read of their ranges (a
+ * stream synchronisation); key columns whose ranges need more than 63 bits
+ * together are refused with GHB_ERR_UNSUPPORTED.  STRING key columns are
+ * first mapped to the row of their value's first occurrence on the device
+ * (GroupByPredicate.hpp:75-101 compares the bytes); a STRING key's output is
+ * [start,end) pairs into the key column's own bytes.  STRING columns may be
+ * predicate leaves too, not aggregate inputs. */
 int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred,
                            const ghb_column* cols, int32_t ncols,
                            const int32_t* key_cols, int32_t nkeys,
@@ -483,6 +504,90 @@ int32_t ghb_server_stats(ghb_server* server, int64_t* completed, int64_t* runnin
                          int64_t* queued, int64_t* bytes_admitted);
 const char* ghb_server_last_error(ghb_server* server);
 int32_t ghb_server_destroy(ghb_server* server);
+
+/* ---- GHive's JNI input and output, and a vertex's operator chain --------
+ * ghb_gtables is GHive's GTables object (ghive/GTables.java:13-31) with its
+ * fields read by the JNI shim (GetObjectField, GetIntArrayElements,
+ * GetDirectBufferAddress): per input table its column types (0 long,
+ * 1 double, 2 int, 3 string), row count, key count and vertex name, and the
+ * columns as direct buffers, concatenated by type over the tables in table
+ * order.  The buffers are the JVM's, valid during the call, and read only. */
+typedef struct ghb_gtables {
+  int32_t ntables;
+  const int32_t* ncols;                /* types[t].length                     */
+  const int32_t* const* types;         /* types[t][c]                         */
+  const int32_t* row_cnt;              /* rowCnt[t]                           */
+  const int32_t* key_cnt;              /* keyCnt[t]                           */
+  const char* const* vertex_name;      /* vertexName[t]; NULL entry: missing  */
+  int32_t nlong;
+  const void* const* long_cols;        /* longCols[i]: int64 little-endian    */
+  int32_t ndouble;
+  const void* const* double_cols;      /* doubleCols[i]                       */
+  int32_t nint;
+  const void* const* int_cols;         /* intCols[i]: int32                   */
+  int32_t nstring;
+  const void* const* string_cols;      /* stringCols[i]: UTF-8 bytes          */
+  const void* const* string_idx_cols;  /* stringIdxCols[i]: int32 [start,end) per row */
+} ghb_gtables;
+
+/* Input table `table`'s columns, in its types[] order, as descriptors over
+ * the JVM's buffers (no copy; NULLs are GHive's sentinels, GTable.java:
+ * 38-40): each column takes the next buffer of its type not taken by an
+ * earlier column or table, as GPUProcess does (ghive_JNIInterface.cu:
+ * 132-201).  GHB_ERR_INVALID when the table is missing (NULL vertex name),
+ * a type's buffers run out or more than `cap` columns would be written. */
+int32_t ghb_gtables_table(const ghb_gtables* in, int32_t table, ghb_column* cols,
+                          int32_t cap, int32_t* ncols, int64_t* rows);
+
+/* One operator of a vertex's chain (GHive's operator tree of one vertex,
+ * Parser.cu:675 root_op->execute(), run here as a chain).  Column indices
+ * refer to the table the previous operator produced (the input table for
+ * the first). */
+typedef struct ghb_plan_op {
+  int32_t op;                  /* GHB_OP_FILTER / GROUPBY / JOIN_PROBE / SORT */
+  int32_t join_type;           /* JOIN_PROBE                                   */
+  const ghb_predicate* pred;   /* FILTER                                       */
+  const int32_t* idx;          /* FILTER: projection (NULL = all columns);
+                                  GROUPBY: key columns; SORT: key columns;
+                                  JOIN_PROBE: {probe key column, build key
+                                  column of the build table}                  */
+  int32_t nidx;
+  int32_t naggs;               /* GROUPBY                                      */
+  const ghb_agg_desc* aggs;
+  int64_t max_groups;          /* GROUPBY: output capacity (0 = rows)         */
+  const int32_t* orders;       /* SORT (NULL = all ASC)                        */
+  const int32_t* null_orders;  /* SORT (NULL = Hive's defaults)                */
+  int32_t build_table;         /* JOIN_PROBE: input table of the build side    */
+  int32_t nbuild_keep;         /* JOIN_PROBE: build columns appended to the
+                                  output, after the probe table's columns     */
+  const int32_t* build_keep;
+} ghb_plan_op;
+
+/* The final table, host-side, grouped the way GPUResult holds it
+ * (GPUResult.java:29-39, built at ghive_JNIInterface.cu:217-340): column i
+ * has types[i], data[i] (NULLs as GHive's sentinels) and is_null[i]
+ * (NULL: no NULL map), and sequence[i] is its index in the concatenation
+ * long || double || int || string of GPUResult's arrays.  The arrays are
+ * pinned host memory owned by the library until ghb_plan_result_free. */
+typedef struct ghb_plan_result {
+  int32_t ncols;
+  int32_t types[GHB_MAX_RESULT_COLS];
+  void* data[GHB_MAX_RESULT_COLS];
+  uint8_t* is_null[GHB_MAX_RESULT_COLS];
+  int32_t sequence[GHB_MAX_RESULT_COLS];
+  int64_t rows;
+  int32_t n_long, n_double, n_int, n_string;
+} ghb_plan_result;
+
+/* Runs `nops` operators on input table `input` of `in`: the table's columns
+ * are copied to the device once, every operator's output stays on the device
+ * as the next one's input (GHive copied each operator's input in and output
+ * back, FilterOperator.cu:53-89, GroupByPredicate.cu:39-91), a JOIN_PROBE
+ * builds its hash table from another input table, and only the final table
+ * is copied back into `out`.  Synchronous; the context's own stream. */
+int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input,
+                     const ghb_plan_op* ops, int32_t nops, ghb_plan_result* out);
+int32_t ghb_plan_result_free(ghb_plan_result* result);
 
 /* ---- host-buffer entry points (end-to-end) -------------------------------
  * Same operators with every column in HOST memory (pageable or pinned).

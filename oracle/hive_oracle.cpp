@@ -60,6 +60,7 @@ namespace {
 constexpr int kBatch = 1024;  // VectorizedRowBatch.DEFAULT_SIZE
 
 inline bool col_is_null(const ghb_column& c, int64_t i) {
+  if (c.type == GHB_STRING) return ((const int32_t*)c.aux)[2 * i] < 0;   // GTable.java:240-257
   switch (c.null_mode) {
     case GHB_NULLS_BYTEMAP: return c.is_null && c.is_null[i] != 0;
     case GHB_NULLS_SENTINEL:
@@ -105,10 +106,58 @@ inline bool cmp_mode(int mode, T x, T a, T b) {
   return false;
 }
 
+// Hive's StringExpr.compare (storage-api/src/java/org/apache/hadoop/hive/ql/
+// exec/vector/expressions/StringExpr.java:37-47): unsigned bytes, then length.
+inline int string_compare(const uint8_t* a, int la, const uint8_t* b, int lb) {
+  for (int i = 0; i < la && i < lb; i++)
+    if (a[i] != b[i]) return (int)a[i] - (int)b[i];
+  return la - lb;
+}
+
+inline const uint8_t* string_at(const ghb_column& c, int64_t i, int* len) {
+  const int32_t* idx = (const int32_t*)c.aux;
+  *len = idx[2 * i + 1] - idx[2 * i];
+  return (const uint8_t*)c.data + idx[2 * i];
+}
+
+// A STRING leaf: FilterStringGroupColumnCompareStringGroupScalarBase.txt /
+// FilterStringColumnBetween.txt (ql/src/gen/vectorization/
+// ExpressionTemplates), with a column compare for col2 >= 0.
+bool string_leaf_pass(const ghb_pred_node& nd, const ghb_column* cols, int64_t i) {
+  int lx = 0;
+  const uint8_t* x = string_at(cols[nd.col], i, &lx);
+  int ca, cb = 0;
+  if (nd.col2 >= 0) {
+    int ly = 0;
+    const uint8_t* y = string_at(cols[nd.col2], i, &ly);
+    ca = string_compare(x, lx, y, ly);
+  } else {
+    ca = string_compare(x, lx, (const uint8_t*)nd.lit_s[0], nd.lit_s_len[0]);
+    cb = string_compare(x, lx, (const uint8_t*)nd.lit_s[1], nd.lit_s_len[1]);
+  }
+  switch (nd.mode) {
+    case GHB_FILTER_EQ: return ca == 0;
+    case GHB_FILTER_LE: return ca <= 0;
+    case GHB_FILTER_GE: return ca >= 0;
+    case GHB_FILTER_LT: return ca < 0;
+    case GHB_FILTER_GT: return ca > 0;
+    case GHB_FILTER_RANGE: return ca > 0 && cb < 0;
+    case GHB_FILTER_EQ_RANGE: return ca >= 0 && cb <= 0;
+    case GHB_FILTER_NOT_EQ: return ca != 0;
+    case GHB_FILTER_NOT_RANGE: return ca < 0 || cb > 0;
+    case GHB_FILTER_NOT_EQ_RANGE: return ca <= 0 || cb >= 0;
+  }
+  return false;
+}
+
 bool leaf_pass(const ghb_pred_node& nd, const ghb_column* cols, int64_t i) {
   const ghb_column& c = cols[nd.col];
   if (col_is_null(c, i)) return false;
   if (nd.mode == GHB_FILTER_NOT_NULL) return true;
+  if (c.type == GHB_STRING) {
+    if (nd.col2 >= 0 && col_is_null(cols[nd.col2], i)) return false;
+    return string_leaf_pass(nd, cols, i);
+  }
   if (nd.col2 >= 0) {
     const ghb_column& c2 = cols[nd.col2];
     if (col_is_null(c2, i)) return false;

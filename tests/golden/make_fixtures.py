@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ from the reference's tests.
 
 Run in a checkout where the GHive reference tree is available (its root is
-the first argument, default /root/reference).  The script reads the test
+the one, required argument).  The script reads the test
 sources AS TEXT and extracts their input values and expected outputs; it runs
 none of the reference's code.  The JSON it writes is committed, so the test
 suite never needs the reference tree.
@@ -15,7 +15,7 @@ Sources (paths inside the GHive project):
   gpu_impl/test/JoinPredicateTest.cu     SEMI_OUTER_TEST_TABLE result_offsets
   gpu_impl/test/FilterPredicateTest.cu   simpleOneColTest expected rows
 
-Usage:  python tests/golden/make_fixtures.py [/path/to/reference]
+Usage:  python tests/golden/make_fixtures.py <root of the GHive reference tree>
 """
 import json
 import os
@@ -342,4 +342,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_fixtures.py <root of the GHive reference tree>")
+    main(sys.argv[1])

@@ -33,11 +33,13 @@ def test_struct_layout_matches_header(tmp_path):
 #include <stddef.h>
 #include "ghive_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(ghb_column),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(ghb_column),
          sizeof(ghb_out_column), sizeof(ghb_pred_node), sizeof(ghb_predicate),
          sizeof(ghb_agg_desc), sizeof(ghb_groupby_cfg), sizeof(ghb_join_cfg),
          sizeof(ghb_sort_cfg), offsetof(ghb_pred_node, lit_d), sizeof(ghb_groupby_instance),
-         sizeof(ghb_batch_cfg), offsetof(ghb_batch_cfg, load_factor));
+         sizeof(ghb_batch_cfg), offsetof(ghb_batch_cfg, load_factor), sizeof(ghb_gtables),
+         sizeof(ghb_plan_op), sizeof(ghb_plan_result), offsetof(ghb_plan_result, rows),
+         offsetof(ghb_plan_op, build_keep));
   return 0;
 }
 """)
@@ -48,7 +50,9 @@ int main(void) {
     exp = [C.sizeof(abi.Column), C.sizeof(abi.OutColumn), C.sizeof(abi.PredNode),
            C.sizeof(abi.Predicate), C.sizeof(abi.AggDesc), C.sizeof(abi.GroupByCfg),
            C.sizeof(abi.JoinCfg), C.sizeof(abi.SortCfg), abi.PredNode.lit_d.offset,
-           C.sizeof(abi.GroupByInstance), C.sizeof(abi.BatchCfg), abi.BatchCfg.load_factor.offset]
+           C.sizeof(abi.GroupByInstance), C.sizeof(abi.BatchCfg), abi.BatchCfg.load_factor.offset,
+           C.sizeof(abi.GTables), C.sizeof(abi.PlanOp), C.sizeof(abi.PlanResult),
+           abi.PlanResult.rows.offset, abi.PlanOp.build_keep.offset]
     assert got == exp
 
 

@@ -680,3 +680,143 @@ def test_host_join_in_chunks_short_output(ctx):
     pr, br = oracle.hash_join(bkey, fk)
     assert r["rows"] == len(pr) and np.array_equal(r["probe_rowid"], pr)
     assert np.array_equal(r["build"][0][0], bpay[0][br])
+
+
+# ---------------------------------------------------------------- strings
+def _strings(values):
+    """("string", utf-8 bytes, int32 [start,end) pairs) of a list of str/None
+    (None: NULL as (-1, -1), GTable.java:240-257)."""
+    chars, idx, pos = bytearray(), [], 0
+    for v in values:
+        if v is None:
+            idx += [-1, -1]
+            continue
+        b = v.encode()
+        idx += [pos, pos + len(b)]
+        chars += b
+        pos += len(b)
+    return ("string", bytes(chars) or b"\0", np.array(idx, dtype=np.int32))
+
+
+def _dev_strings(s):
+    import torch
+    return ("string", torch.frombuffer(bytearray(s[1]), dtype=torch.uint8).cuda(), dev(s[2]))
+
+
+def _decode(col_str, pairs):
+    b = col_str[1]
+    p = pairs.reshape(-1, 2)
+    return [None if s < 0 else b[s:e].decode() for s, e in p]
+
+
+def _words(g, n, nulls=0.1):
+    pool = ["", "a", "ab", "abc", "b", "MFGR#12", "MFGR#1221", "MFGR#1238", "zz", "été", "Z", "abd"]
+    return [None if g.random() < nulls else pool[g.integers(0, len(pool))] for _ in range(n)]
+
+
+def test_filter_string_predicates_every_mode_and_projection(ctx):
+    g = np.random.default_rng(95)
+    n = 40_000
+    words = _words(g, n)
+    s = _strings(words)
+    v = g.integers(-100, 100, n, dtype=np.int64)
+    ds = _dev_strings(s)
+    for mode in range(abi.FILTER_NOT_NULL + 1):
+        for a, b in (("ab", "b"), ("MFGR#12", "MFGR#1238"), ("", "zz"), ("é", "été~")):
+            p = abi.Pred.leaf(mode, 0, a=a, b=b)
+            sel = oracle.filter_rows(p, [s, v])
+            outs, k = ctx.filter(p, [ds, dev(v)], proj=[1, 0])
+            assert k == len(sel), (mode, a, b)
+            assert np.array_equal(host(outs[0][0]), v[sel])
+            assert _decode(s, host(outs[1][0])) == [words[i] for i in sel]
+    # a STRING leaf inside a tree with a numeric one, and column vs column
+    t = _strings(_words(g, n, 0.05))
+    p = abi.Pred.and_(abi.Pred.leaf(abi.FILTER_GE, 0, a="abc"), abi.Pred.leaf(abi.FILTER_LT, 1, a=50))
+    sel = oracle.filter_rows(p, [s, v])
+    _, k = ctx.filter(p, [ds, dev(v)])
+    assert k == len(sel)
+    p2 = abi.Pred.leaf(abi.FILTER_LT, 0, col2=2)
+    sel = oracle.filter_rows(p2, [s, v, t])
+    _, k = ctx.filter(p2, [ds, dev(v), _dev_strings(t)])
+    assert k == len(sel)
+
+
+@pytest.mark.parametrize("with_pred", [False, True])
+def test_groupby_string_keys(ctx, with_pred):
+    """GROUP BY a STRING key, and (INT, STRING) keys: each STRING key becomes
+    the row of its value's first occurrence on the device; the output holds
+    [start,end) pairs into the key column's bytes."""
+    g = np.random.default_rng(96 + with_pred)
+    n = 150_000
+    words = _words(g, n)
+    s = _strings(words)
+    year = g.integers(1992, 1999, n, dtype=np.int32)
+    rev = g.integers(1, 10_000_000, n) / 100.0
+    qty = g.integers(1, 51, n, dtype=np.int64)
+    pred = abi.Pred.leaf(abi.FILTER_GT, 3, a=10) if with_pred else None
+    aggs = [(abi.CNT, -1), (abi.SUM, 3), (abi.SUM, 2), (abi.AVG, 2), (abi.MAX, 1)]
+    ds = _dev_strings(s)
+    for keys in ([0], [1, 0]):
+        exp = oracle.groupby_string_key([s, year, rev, qty], keys, aggs) if not with_pred else None
+        if with_pred:
+            m = qty > 10
+            exp = oracle.groupby_string_key([_strings([w for w, k in zip(words, m) if k]), year[m], rev[m],
+                                             qty[m]], keys, aggs)
+        gk, ga, ng = ctx.filter_groupby(pred, [ds, dev(year), dev(rev), dev(qty)], keys, aggs,
+                                        capacity=256, max_groups=200)
+        assert ng == len(exp)
+        kcols = []
+        for j, k in enumerate(keys):
+            if k == 0:
+                kcols.append(_decode(s, host(gk[j][0])[:2 * ng]))
+            else:
+                vals, nl = host(gk[j][0]), host(gk[j][1])
+                kcols.append([None if nl[i] else int(vals[i]) for i in range(ng)])
+        rows = []
+        for i in range(ng):
+            r = [kc[i] for kc in kcols]
+            for v, nl in ga:
+                r.append(None if host(nl)[i] else host(v)[i].item())
+            rows.append(tuple(r))
+        key = lambda r: tuple((x is not None, x if x is not None else "") for x in r[:len(keys)])  # noqa: E731
+        got, want = sorted(rows, key=key), sorted(exp, key=key)
+        for a, b in zip(got, want):
+            assert a[:len(keys) + 2] == b[:len(keys) + 2] and a[-1] == b[-1], (a, b)
+            for x, y in zip(a[len(keys) + 2:-1], b[len(keys) + 2:-1]):
+                assert abs(x - y) <= REL_TOL * abs(y)
+
+
+def test_groupby_ghive_golden_string_keys(ctx):
+    """GHive's shouldSuccess (one STRING key) and multipleKeysTest (INT and
+    STRING keys) through the GPU: Table::toString rows as the test expects."""
+    with open(os.path.join(os.path.dirname(__file__), "golden", "ghive_groupby.json")) as f:
+        cases = json.load(f)["cases"]
+    ran = 0
+    for case in cases:
+        if not any(case["columns"][k][0] == "string" for k in case["keys"]):
+            continue
+        cols, hcols = [], []
+        for c in case["columns"]:
+            if c[0] == "string":
+                chars = c[1].encode()
+                hc = ("string", chars, np.array(c[2], dtype=np.int32))
+                hcols.append(hc)
+                cols.append(_dev_strings(hc))
+            else:
+                a = np.array(c[1], dtype={"long": np.int64, "double": np.float64, "int": np.int32}[c[0]])
+                hcols.append(a)
+                cols.append(dev(a))
+        aggs = [(abi.AGG_NAMES[t.lower()], c) for t, c in case["aggs"]]
+        gk, ga, g = ctx.filter_groupby(None, cols, case["keys"], aggs, capacity=64, max_groups=32)
+        out = []
+        for j, k in enumerate(case["keys"]):
+            if case["columns"][k][0] == "string":
+                out.append(_decode(hcols[k], host(gk[j][0])[:2 * g]))
+            else:
+                out.append([str(x) for x in host(gk[j][0])[:g]])
+        for (v, _), t in zip(ga, case["expected_types"][len(case["keys"]):]):
+            out.append([("%f" % x) if t == abi.DOUBLE else str(x) for x in host(v)[:g]])
+        rows = sorted(tuple(col[i] for col in out) for i in range(g))
+        assert rows == sorted(tuple(r) for r in case["expected_rows"]), case["test"]
+        ran += 1
+    assert ran == 2

@@ -1,0 +1,110 @@
+"""A vertex's operator chain on device-resident intermediates, fed the way
+GHive's JNI entry point is fed (a GTables object) and answered the way it
+answers (GPUResult's arrays grouped by type, plus sequence).
+
+Each chain's result equals the oracle's Hive operators applied one after the
+other: bit-exact for keys, counts, integer sums, MIN/MAX and row order;
+DOUBLE SUM/AVG within REL_TOL of the oracle's sequential sums.
+"""
+import numpy as np
+import pytest
+
+from ghive_b200 import abi, workloads
+from ghive_b200.gtables import GTables, op_filter, op_groupby, op_join, op_sort, run_plan
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from ghive_b200.ops import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _sequence(types):
+    base = {0: 0, 1: types.count(0), 2: types.count(0) + types.count(1)}
+    seen = {0: 0, 1: 0, 2: 0}
+    out = []
+    for t in types:
+        out.append(base[t] + seen[t])
+        seen[t] += 1
+    return out
+
+
+def _assert_cols(got, exp, types):
+    for j, ((gv, gn), (ev, en)) in enumerate(zip(got, exp)):
+        assert np.array_equal(gn, en), j
+        if types[j] == abi.DOUBLE:
+            e, g = ev[~en], gv[~gn]
+            assert np.all(np.abs(g - e) <= REL_TOL * np.maximum(np.abs(e), 1e-300)), j
+        else:
+            assert np.array_equal(gv[~gn], ev[~en]), j
+
+
+def test_filter_groupby_sort_chain(ctx):
+    """TableScan -> Filter (d < 1263) -> GroupBy k -> Sink ORDER BY k DESC."""
+    cols = workloads.fact_table(2_000_000, seed_idx=90, groups=700)
+    gt = GTables([("Map 1", 0, cols)])
+    pred = workloads.fact_predicate()
+    aggs = workloads.AGGS_FACT
+    r = run_plan(ctx, gt, 0, [op_filter(pred), op_groupby([0], aggs, max_groups=700),
+                              op_sort([0], orders=[abi.DESC])])
+    ok, oa = oracle.filter_groupby(pred, cols, [0], aggs)
+    exp = [(c[0][::-1], c[1][::-1]) for c in ok + oa]   # the oracle orders groups by key ASC
+    assert r["rows"] == 700
+    types = [abi.INT, abi.LONG, abi.LONG, abi.DOUBLE, abi.DOUBLE, abi.INT, abi.INT]
+    assert r["types"] == types
+    _assert_cols(r["columns"], exp, types)
+    assert r["sequence"] == _sequence(types)
+    assert len(r["longCols"]) == 2 and len(r["doubleCols"]) == 2 and len(r["intCols"]) == 3
+
+
+def test_join_groupby_chain_with_two_input_tables(ctx):
+    """A map-join vertex: the fact table (input 0) probes a dimension table
+    (input 1, key + attribute), then GROUP BY the attribute, ORDER BY it."""
+    g = np.random.default_rng(91)
+    nd, nf = 5_000, 1_500_000
+    dkey = g.permutation(np.arange(1, nd + 1, dtype=np.int64))
+    dattr = g.integers(0, 40, nd, dtype=np.int32)
+    fk = g.integers(1, nd + 500, nf, dtype=np.int64)
+    qty = g.integers(1, 51, nf, dtype=np.int64)
+    price = g.integers(90000, 10500001, nf) / 100.0
+    gt = GTables([("Map 1", 0, [fk, qty, price]), ("Map 2", 1, [dkey, dattr])])
+    aggs = [(abi.CNT, -1), (abi.SUM, 1), (abi.AVG, 2)]
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0, build_keep=[1]),          # -> fk, qty, price, attr
+                              op_groupby([3], aggs, max_groups=64), op_sort([0])])
+    pr, br = oracle.hash_join(dkey, fk)
+    joined = [fk[pr], qty[pr], price[pr], dattr[br]]
+    ok, oa = oracle.filter_groupby(None, joined, [3], aggs)
+    types = [abi.INT, abi.LONG, abi.LONG, abi.DOUBLE]
+    assert r["rows"] == len(ok[0][0]) == 40
+    _assert_cols(r["columns"], ok + oa, types)
+    assert r["sequence"] == _sequence(types)
+
+
+def test_semi_join_filter_projection_chain(ctx):
+    g = np.random.default_rng(92)
+    keys = np.arange(0, 2000, 3, dtype=np.int64)
+    fk = g.integers(0, 2000, 300_000, dtype=np.int64)
+    v = g.integers(-50, 50, 300_000, dtype=np.int64)
+    gt = GTables([("Map 1", 0, [fk, v]), ("Map 2", 0, [keys])])
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0, join_type=abi.LEFT_SEMI_JOIN),
+                              op_filter(abi.Pred.leaf(abi.FILTER_GT, 1, a=0), proj=[1, 0])])
+    m = np.isin(fk, keys) & (v > 0)
+    assert r["rows"] == int(m.sum())
+    assert np.array_equal(r["columns"][0][0], v[m]) and np.array_equal(r["columns"][1][0], fk[m])
+
+
+def test_missing_input_table_is_refused(ctx):
+    from ghive_b200._lib import GhbError
+    gt = GTables([("Map 1", 0, [np.arange(10, dtype=np.int64)]), (None, 0, [np.arange(3, dtype=np.int64)])])
+    with pytest.raises(GhbError) as e:
+        run_plan(ctx, gt, 0, [op_join(0, 1, 0)])
+    assert e.value.code == abi.ERR_INVALID
+    r = run_plan(ctx, gt, 0, [op_sort([0], orders=[abi.DESC])])
+    assert np.array_equal(r["columns"][0][0], np.arange(10)[::-1])
