@@ -1,17 +1,22 @@
 """Host side of running the operators on several GPUs (one rank per GPU).
 
-Every operator shards without a data-path exchange on this path:
   filter, group-by  each rank takes a contiguous row range (shard_range);
                     group-by ranks compute mergeable partial aggregates
                     (AVG travels as SUM + COUNT) and the partials are merged
                     on one rank (merge_groupby), the all-gather form that suits
                     small group counts;
   join              the build side is replicated, each rank probes its probe
-                    row range; probe row ids are offset by the range start.
+                    row range; probe row ids are offset by the range start;
+  sort              sample sort (sort_sharded): splitters from an all-gathered
+                    sample of every rank's leading key, each rank's rows
+                    range-partitioned by them, one all-to-all per column
+                    (NCCL over NVLink between GPUs), then the stable local sort.
 """
 import numpy as np
 
 from . import abi
+
+I64_MIN, I64_MAX = -(1 << 63), (1 << 63) - 1
 
 
 def shard_range(n, rank, world):
@@ -97,3 +102,101 @@ def merge_groupby(parts, aggs, has_key=True):
             np.logical_or.at(seen, gid[~n], True)
             out.append((r, ~seen))
     return key, out
+
+
+# ------------------------------------------------------------ sample sort
+def order_image(values, isnull, desc, nulls_first):
+    """int64 values whose signed order is the ORDER BY order of one key column
+    (BinarySortable order: integers by value, doubles by IEEE total order;
+    DESC reversed; NULLs first or last).  Monotone but not one-to-one: rows
+    that tie here are told apart by the local sort."""
+    import torch
+    if values.dtype == torch.float64:
+        b = values.view(torch.int64)
+        # IEEE total order as a signed int64: negative doubles' bits reversed
+        img = torch.where(b < 0, b ^ I64_MAX, b)
+    else:
+        img = values.to(torch.int64)
+    if desc:
+        img = ~img
+    if isnull is not None:
+        img = torch.where(isnull.bool(), torch.full_like(img, I64_MIN if nulls_first else I64_MAX), img)
+    return img
+
+
+def choose_splitters(samples, world):
+    """world - 1 splitters from the all-gathered sorted sample."""
+    import torch
+    s, _ = torch.sort(samples)
+    if s.numel() == 0:
+        return s[:0]
+    idx = torch.tensor([(i * s.numel()) // world for i in range(1, world)], dtype=torch.int64,
+                       device=s.device)
+    return s[idx]
+
+
+def sort_sharded(keys, payload, local_sort, orders=None, null_orders=None, group=None,
+                 sample_per_rank=4096):
+    """Stable ORDER BY over the rows of all ranks, each rank holding a shard.
+
+    keys / payload: this rank's columns, each a tensor or (values, isnull)
+    pair (a CUDA tensor under NCCL, a CPU tensor under gloo).  local_sort(keys,
+    payload, orders, null_orders) sorts one rank's received rows and returns
+    (keys, payload) in the same column forms (the device sort, Context.sort,
+    on a GPU).  The result on rank r is the r-th range of the global order;
+    rows with equal keys keep the order of (rank, row) of the input, because
+    equal leading keys always go to one rank and the all-to-all delivers the
+    source ranks in order.  Returns this rank's sorted (keys, payload)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    nk = len(keys)
+    orders = orders or [abi.ASC] * nk
+    null_orders = null_orders or [abi.NULLS_DEFAULT] * nk
+
+    def split(c):
+        return (c[0], c[1]) if isinstance(c, tuple) else (c, None)
+
+    v0, n0 = split(keys[0])
+    desc = orders[0] == abi.DESC
+    nf = null_orders[0] == abi.NULLS_FIRST or (null_orders[0] == abi.NULLS_DEFAULT and not desc)
+    img = order_image(v0, n0, desc, nf)
+    n = img.numel()
+    dev = img.device
+    # splitters from an evenly spaced sample of every rank's leading key
+    m = min(sample_per_rank, n)
+    pick = (torch.arange(m, device=dev, dtype=torch.int64) * n) // max(m, 1)
+    local = img[pick] if m else img[:0]
+    counts = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(world)]
+    dist.all_gather(counts, torch.tensor([m], dtype=torch.int64, device=dev), group=group)
+    sizes = [int(c.item()) for c in counts]
+    mx = max(sizes)
+    padded = torch.full((mx,), I64_MAX, dtype=torch.int64, device=dev)
+    padded[:m] = local
+    gathered = [torch.empty(mx, dtype=torch.int64, device=dev) for _ in range(world)]
+    dist.all_gather(gathered, padded, group=group)
+    samples = torch.cat([g[:sz] for g, sz in zip(gathered, sizes)])
+    splitters = choose_splitters(samples, world)
+    # destination rank of each row; rows keep their order within a destination
+    dest = torch.searchsorted(splitters, img, right=True) if world > 1 else \
+        torch.zeros(n, dtype=torch.int64, device=dev)
+    order = torch.argsort(dest, stable=True)
+    send = torch.bincount(dest, minlength=world).to(torch.int64)
+    recv = torch.empty_like(send)
+    dist.all_to_all_single(recv, send, group=group)
+    send_l, recv_l = send.tolist(), recv.tolist()
+
+    def exchange(t):
+        t = t[order].contiguous()
+        out = torch.empty((sum(recv_l),) + tuple(t.shape[1:]), dtype=t.dtype, device=dev)
+        dist.all_to_all_single(out, t, recv_l, send_l, group=group)
+        return out
+
+    def move(c):
+        v, nl = split(c)
+        v2 = exchange(v)
+        if nl is None:
+            return v2
+        return (v2, exchange(nl.to(torch.uint8)))
+
+    return local_sort([move(c) for c in keys], [move(c) for c in payload], orders, null_orders)

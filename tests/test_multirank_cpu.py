@@ -63,6 +63,59 @@ def _join_rank(rank, world, port, q):
         dist.destroy_process_group()
 
 
+def _sort_table(n):
+    g = np.random.default_rng(53)
+    d = g.integers(0, 40, n, dtype=np.int32)
+    dn = g.random(n) < 0.05
+    k = g.integers(-1000, 1000, n, dtype=np.int64)
+    x = np.round(g.normal(0, 10, n), 1)
+    return d, dn, k, x
+
+
+def _np_local_sort(keys, payload, orders, null_orders):
+    """The stable local sort of one rank's received rows: the CPU oracle here
+    (the ranks are CPU processes); on a GPU it is the device sort."""
+    import torch
+
+    from oracle import oracle
+
+    def np_col(c):
+        return (c[0].numpy(), c[1].numpy().astype(bool)) if isinstance(c, tuple) else c.numpy()
+
+    perm = oracle.sort_perm([np_col(c) for c in keys], orders, null_orders)
+    pt = torch.from_numpy(perm)
+
+    def take(c):
+        return (c[0][pt], c[1][pt]) if isinstance(c, tuple) else c[pt]
+    return [take(c) for c in keys], [take(c) for c in payload]
+
+
+def _sort_rank(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        d, dn, k, x = _sort_table(100_003)
+        lo, hi = shard.shard_range(len(d), rank, world)
+        rid = np.arange(lo, hi, dtype=np.int64)
+        keys = [(torch.from_numpy(d[lo:hi]), torch.from_numpy(dn[lo:hi].astype(np.uint8))),
+                torch.from_numpy(x[lo:hi])]
+        pay = [torch.from_numpy(k[lo:hi]), torch.from_numpy(rid)]
+        out = {}
+        for name, orders, nulls in (("asc", [abi.ASC, abi.DESC], None),
+                                    ("desc", [abi.DESC, abi.ASC], [abi.NULLS_FIRST, abi.NULLS_DEFAULT])):
+            ok, op = shard.sort_sharded(keys, pay, _np_local_sort, orders, nulls, sample_per_rank=500)
+            out[name] = (ok[0][0].numpy(), ok[0][1].numpy(), ok[1].numpy(), op[1].numpy())
+        gathered = [None] * world
+        dist.all_gather_object(gathered, out)
+        if rank == 0:
+            q.put(gathered)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
 def _spawn(fn):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
@@ -111,6 +164,38 @@ def test_sharded_join_probe_unions_to_the_whole():
                      *[np.concatenate([g[1][j] for g in gathered]).tolist() for j in range(len(bpay))]))
     exp = sorted(zip(np.asarray(prow).tolist(), *[np.asarray(o).tolist() for o in outs]))
     assert got == exp
+
+
+def test_sharded_sort_is_the_global_stable_order():
+    """Sample sort over two ranks: the ranks' outputs, concatenated in rank
+    order, are the oracle's stable order of all rows (row ids compared, so
+    ties keep the input order across ranks too), ASC and DESC, NULLs."""
+    from oracle import oracle
+    gathered = _spawn(_sort_rank)
+    d, dn, k, x = _sort_table(100_003)
+    for name, orders, nulls in (("asc", [abi.ASC, abi.DESC], None),
+                                ("desc", [abi.DESC, abi.ASC], [abi.NULLS_FIRST, abi.NULLS_DEFAULT])):
+        perm = oracle.sort_perm([(d, dn), x], orders, nulls)
+        rid = np.concatenate([g[name][3] for g in gathered])
+        assert np.array_equal(rid, perm), name
+        assert all(len(g[name][3]) > 0 for g in gathered)   # both ranks got rows
+        got_x = np.concatenate([g[name][2] for g in gathered])
+        assert np.array_equal(got_x.view(np.uint64), x[perm].view(np.uint64))
+
+
+def test_order_image_is_monotone():
+    import torch
+    g = np.random.default_rng(4)
+    v = np.concatenate([g.normal(0, 1e3, 2000), [0.0, np.inf, -np.inf, 1e-300, -1e-300]])
+    img = shard.order_image(torch.from_numpy(v), None, False, True).numpy()
+    o = np.argsort(v, kind="stable")
+    assert np.all(np.diff(img[o]) >= 0)
+    z = shard.order_image(torch.tensor([-0.0, 0.0], dtype=torch.float64), None, False, True).numpy()
+    assert z[0] < z[1]   # IEEE total order: -0.0 before +0.0
+    iv = g.integers(-(1 << 62), 1 << 62, 3000, dtype=np.int64)
+    img = shard.order_image(torch.from_numpy(iv), None, True, False).numpy()
+    o = np.argsort(-iv, kind="stable")
+    assert np.all(np.diff(img[o]) >= 0)
 
 
 def test_global_aggregate_partials_merge():
