@@ -220,6 +220,9 @@ struct BatchSetting {
   int32_t smem_cap;     // shared-table slots at most; 0 = none (a global aggregate keeps 64)
   int32_t skip_large;   // 1: instances with more than 16 * smem_cap groups skip the shared table
   float load_factor;    // global tables
+  // per group-count class (group_class): the global tables' load factor,
+  // 0 = load_factor.  The autotuner's second stage sets these class by class.
+  float lf_class[4];
 };
 
 static const char* kRowClass[] = {"<1e4", "1e4-1e5", "1e5-1e6", ">=1e6"};
@@ -263,7 +266,8 @@ static int32_t setup_inst(ghb_ctx* ctx, const InstSpec& s, int32_t ncols, const 
   GbSetup su{};
   su.max_groups = s.groups;
   su.smem_slots = inst_slots(s, nkeys, bs);
-  su.load_factor = bs.load_factor;
+  const float lfc = bs.lf_class[group_class(s.groups)];
+  su.load_factor = lfc > 0.f ? lfc : bs.load_factor;
   su.threads = bs.threads;
   su.tile_rows = tile_rows;
   su.smem_table_slots = reserve;
@@ -450,7 +454,7 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
   const int forced_threads =
       (cfg && (cfg->block_threads == 512 || cfg->block_threads == 1024)) ? cfg->block_threads : 0;
   const float lf = (cfg && cfg->load_factor > 0.f) ? cfg->load_factor : 0.5f;
-  BatchSetting base{forced_threads ? forced_threads : kGbThreads, 2048, 0, lf};
+  BatchSetting base{forced_threads ? forced_threads : kGbThreads, 2048, 0, lf, {0.f, 0.f, 0.f, 0.f}};
   if (cfg && cfg->smem_slots < 0) base.smem_cap = 0;
   if (cfg && cfg->smem_slots > 0) base.smem_cap = (int32_t)next_pow2_i64(cfg->smem_slots);
   std::vector<BatchSetting> cands{base};
@@ -461,7 +465,8 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
       std::vector<int> caps{0, 512, 1024, 2048, 4096};
       if (cfg && cfg->smem_slots) caps = {base.smem_cap};
       for (int cap : caps)
-        for (int skip = 0; skip < (cap > 0 && nkeys == 1 ? 2 : 1); skip++) cands.push_back({th, cap, skip, lf});
+        for (int skip = 0; skip < (cap > 0 && nkeys == 1 ? 2 : 1); skip++)
+          cands.push_back({th, cap, skip, lf, {0.f, 0.f, 0.f, 0.f}});
     }
   }
   std::string trials = "[";
@@ -484,6 +489,35 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
         best = c;
       }
     }
+    // Second stage, per size class: the load factor of the global tables of
+    // the instances of one group-count class (the others keep theirs), tried
+    // class by class on the batch itself, kept when the batch gets faster.
+    // A sparser table has fewer collisions; a denser one stays in L2.
+    if (nkeys == 1 && !(cfg && cfg->load_factor > 0.f)) {
+      for (int gc = 0; gc < 4; gc++) {
+        bool present = false;
+        for (const InstSpec& sp : spec) present |= group_class(sp.groups) == gc;
+        if (!present) continue;
+        for (float cand : {0.25f, 0.75f}) {
+          BatchSetting c = best;
+          c.lf_class[gc] = cand;
+          BatchImage im;
+          int32_t st = plan_image(ctx, spec, sig, c, stream, &im, nullptr);
+          double ms = st ? -1.0 : time_image(ctx, im, stream, 2);
+          cudaStreamSynchronize(stream);
+          image_free(&im);
+          if (st) ctx->last_error.clear();
+          char tb[200];
+          snprintf(tb, sizeof(tb), ", {\"groups\": \"%s\", \"load_factor\": %.2f, \"ms\": %.4f}",
+                   kGroupClass[gc], cand, ms);
+          trials += tb;
+          if (ms > 0 && ms < best_ms) {
+            best_ms = ms;
+            best = c;
+          }
+        }
+      }
+    }
     // a tuning launch may have raised a device status (a short output): clear it
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t), stream);
   }
@@ -497,6 +531,7 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
   std::string rep_s = "{\"block_threads\": " + std::to_string(best.threads) +
                       ", \"smem_cap\": " + std::to_string(best.smem_cap) +
                       ", \"skip_large\": " + std::to_string(best.skip_large) +
+                      ", \"load_factor\": " + std::to_string(best.load_factor) +
                       ", \"tile_rows\": " + std::to_string(ps[0].tile_rows) +
                       ", \"grid\": " + std::to_string(b->im.grid) +
                       ", \"chunks\": " + std::to_string(b->im.bp.nchunks) +
@@ -517,8 +552,9 @@ static int32_t batch_create(ghb_ctx* ctx, const ghb_groupby_instance* inst, int3
     if (!cnt) continue;
     snprintf(buf, sizeof(buf),
              "%s{\"rows\": \"%s\", \"groups\": \"%s\", \"instances\": %d, \"total_rows\": %.0f, "
-             "\"smem_slots\": %d}",
-             first ? "" : ", ", kRowClass[k / 4], kGroupClass[k % 4], cnt, rows, slots);
+             "\"smem_slots\": %d, \"load_factor\": %.2f}",
+             first ? "" : ", ", kRowClass[k / 4], kGroupClass[k % 4], cnt, rows, slots,
+             best.lf_class[k % 4] > 0.f ? best.lf_class[k % 4] : best.load_factor);
     rep_s += buf;
     first = false;
   }

@@ -173,6 +173,11 @@ int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* pac
 // `table` (cleared here).  A full table raises GHB_ERR_CAPACITY on the device.
 int32_t string_rep_rows(ghb_ctx* ctx, const ghb_column& c, const int32_t* pass, int64_t* rep,
                         unsigned long long* table, int64_t slots, cudaStream_t stream);
+// The key tuples of a join's two sides (nkeys columns each, same types)
+// packed with one plan into int64 columns with NULL maps (a tuple with a NULL
+// component is NULL and matches nothing).  GHB_ERR_UNSUPPORTED past 63 bits.
+int32_t keypack_join(ghb_ctx* ctx, const ghb_column* a, const ghb_column* b, int32_t nkeys, int64_t* a_packed,
+                     uint8_t* a_null, int64_t* b_packed, uint8_t* b_null, cudaStream_t stream);
 // pass[r] = 1 when row r passes the predicate program, else 0.
 int32_t predicate_pass(ghb_ctx* ctx, const PredProg& prog, const ghb_column* cols, int32_t ncols, int64_t n,
                        int32_t* pass, cudaStream_t stream);

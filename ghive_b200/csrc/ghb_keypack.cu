@@ -276,6 +276,91 @@ int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key
   return GHB_OK;
 }
 
+// Packs the key tuples of a join's two sides with one plan (the ranges of
+// both sides), so that equal tuples pack to equal values across the sides.
+// A tuple with a NULL component never matches (SQL equality): its packed
+// value is NULL (null_out = 1).
+__global__ void __launch_bounds__(256) keypack_join_kernel(KeyPackPlan p, int64_t n, int64_t* out,
+                                                           uint8_t* null_out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t v = 0;
+    bool anynull = false;
+#pragma unroll
+    for (int j = 0; j < kMaxPackKeys; j++) {
+      if (j >= p.nkeys) break;
+      const ghb_column& c = p.col[j];
+      const int64_t raw = ld_raw_cs(c, r);
+      const bool null = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, r);
+      anynull |= null;
+      if (!null && p.vbits[j] > 0) v |= (kp_image(c, raw) - p.umin[j]) << p.vshift[j];
+    }
+    out[r] = anynull ? 0 : (int64_t)v;
+    null_out[r] = anynull ? 1 : 0;
+  }
+}
+
+int32_t keypack_join(ghb_ctx* ctx, const ghb_column* a, const ghb_column* b, int32_t nkeys, int64_t* a_packed,
+                     uint8_t* a_null, int64_t* b_packed, uint8_t* b_null, cudaStream_t stream) {
+  if (nkeys < 1 || nkeys > kMaxPackKeys)
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d join key columns: at most %d", nkeys, kMaxPackKeys);
+  for (int j = 0; j < nkeys; j++) {
+    if (a[j].type == GHB_STRING || b[j].type == GHB_STRING)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "join key %d: STRING join keys are not on the device path", j);
+    if (a[j].type != b[j].type)
+      return set_error(ctx, GHB_ERR_INVALID, "join key %d: types %d and %d differ", j, a[j].type, b[j].type);
+  }
+  unsigned long long* d_mm = nullptr;
+  int32_t st = scratch_alloc(ctx, 3 * 8 * kMaxPackKeys, (void**)&d_mm, stream);
+  if (st) return st;
+  unsigned long long init[3 * kMaxPackKeys];
+  for (int j = 0; j < kMaxPackKeys; j++) {
+    init[3 * j] = ~0ull;
+    init[3 * j + 1] = 0;
+    init[3 * j + 2] = 0;
+  }
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(d_mm, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+  for (int side = 0; side < 2; side++) {
+    const ghb_column* c = side ? b : a;
+    KpMinMaxParams mp;
+    std::memset(&mp, 0, sizeof(mp));
+    mp.nkeys = nkeys;
+    mp.n = c[0].n;
+    for (int j = 0; j < nkeys; j++) mp.col[j] = c[j];
+    mp.out = d_mm;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((mp.n + 255) / 256, (int64_t)ctx->num_sms * 8));
+    keypack_minmax_kernel<<<grid, 256, 0, stream>>>(mp);
+    GHB_LAUNCH_CHECK(ctx);
+  }
+  unsigned long long mm[3 * kMaxPackKeys];
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost, stream));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+  KeyPackPlan P;
+  std::memset(&P, 0, sizeof(P));
+  P.nkeys = nkeys;
+  int bits = 0;
+  for (int j = 0; j < nkeys; j++) {
+    const bool anyval = mm[3 * j] <= mm[3 * j + 1];
+    P.umin[j] = anyval ? mm[3 * j] : 0;
+    const uint64_t range = anyval ? mm[3 * j + 1] - mm[3 * j] : 0;
+    P.vbits[j] = (int8_t)(range == 0 ? 0 : 64 - __builtin_clzll(range));
+    P.vshift[j] = (int8_t)bits;
+    P.fshift[j] = -1;
+    bits += P.vbits[j];
+    if (bits > 63)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "the %d join key columns' ranges need more than 63 bits", nkeys);
+  }
+  for (int side = 0; side < 2; side++) {
+    const ghb_column* c = side ? b : a;
+    for (int j = 0; j < nkeys; j++) P.col[j] = c[j];
+    const int64_t n = c[0].n;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+    keypack_join_kernel<<<grid, 256, 0, stream>>>(P, n, side ? b_packed : a_packed, side ? b_null : a_null);
+    GHB_LAUNCH_CHECK(ctx);
+  }
+  return GHB_OK;
+}
+
 int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* packed,
                        const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
                        cudaStream_t stream) {

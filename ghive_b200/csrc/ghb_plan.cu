@@ -186,21 +186,23 @@ int32_t run_groupby(Plan& P, const ghb_plan_op& op, DevTable& t) {
 // The current table probes a hash table built from input table op.build_table:
 // output = the current table's columns, then the kept build columns.
 int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable& t) {
-  if (!op.idx || op.nidx != 2)
-    return set_error(P.ctx, GHB_ERR_INVALID, "join: idx must hold the probe and the build key column");
+  // idx: the probe key columns, then as many build key columns
+  if (!op.idx || op.nidx < 2 || op.nidx % 2 || op.nidx / 2 > kMaxPackKeys)
+    return set_error(P.ctx, GHB_ERR_INVALID, "join: idx must hold k probe and k build key columns");
+  const int nk = op.nidx / 2;
   ghb_column hb[kMaxCols];
   int32_t nb = 0;
   int64_t brows = 0;
   int32_t st = ghb_gtables_table(in, op.build_table, hb, kMaxCols, &nb, &brows);
   if (st) return set_error(P.ctx, st, "join: build table %d is missing or malformed", op.build_table);
-  const int32_t pk = op.idx[0], bk = op.idx[1];
-  if (pk < 0 || pk >= (int)t.cols.size() || bk < 0 || bk >= nb)
-    return set_error(P.ctx, GHB_ERR_INVALID, "join key columns %d / %d", pk, bk);
+  for (int j = 0; j < nk; j++)
+    if (op.idx[j] < 0 || op.idx[j] >= (int)t.cols.size() || op.idx[nk + j] < 0 || op.idx[nk + j] >= nb)
+      return set_error(P.ctx, GHB_ERR_INVALID, "join key columns %d / %d", op.idx[j], op.idx[nk + j]);
   if ((int)t.cols.size() > 8 || op.nbuild_keep > 8 || op.nbuild_keep < 0)
     return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "join: at most 8 columns from each side");
   // the build side's key and kept columns on the device
   std::vector<ghb_column> bsel;
-  bsel.push_back(hb[bk]);
+  for (int j = 0; j < nk; j++) bsel.push_back(hb[op.idx[nk + j]]);
   for (int j = 0; j < op.nbuild_keep; j++) {
     const int32_t c = op.build_keep[j];
     if (c < 0 || c >= nb) return set_error(P.ctx, GHB_ERR_INVALID, "join: build column %d", c);
@@ -209,8 +211,31 @@ int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable
   DevTable b;
   if ((st = upload(P, bsel.data(), (int32_t)bsel.size(), brows, &b))) return st;
   std::vector<ghb_column> bd = descs(b);
+  std::vector<ghb_column> probe = descs(t);
+  ghb_column bkey = bd[0], pkey = probe[op.idx[0]];
+  if (nk > 1) {
+    // several key columns: both sides' tuples packed with one plan
+    std::vector<ghb_column> pk(nk);
+    for (int j = 0; j < nk; j++) pk[j] = probe[op.idx[j]];
+    DevCol pp, bp;
+    for (DevCol* c : {&pp, &bp}) {
+      const int64_t rows = c == &pp ? t.rows : b.rows;
+      c->type = GHB_LONG;
+      c->null_mode = GHB_NULLS_BYTEMAP;
+      if ((st = P.alloc((size_t)std::max<int64_t>(rows, 1) * 8, &c->data)) ||
+          (st = P.alloc((size_t)std::max<int64_t>(rows, 1), (void**)&c->is_null)))
+        return st;
+    }
+    scratch_reset(P.ctx);
+    if ((st = scratch_reserve(P.ctx, 4096, P.s))) return st;
+    if ((st = keypack_join(P.ctx, pk.data(), bd.data(), nk, (int64_t*)pp.data, pp.is_null, (int64_t*)bp.data,
+                           bp.is_null, P.s)))
+      return st;
+    pkey = desc(pp, t.rows);
+    bkey = desc(bp, b.rows);
+  }
   ghb_join_table* jt = nullptr;
-  if ((st = ghb_join_build(P.ctx, &bd[0], bd.data() + 1, op.nbuild_keep, nullptr, &jt, P.s))) return st;
+  if ((st = ghb_join_build(P.ctx, &bkey, bd.data() + nk, op.nbuild_keep, nullptr, &jt, P.s))) return st;
   int64_t rows = 0, max_dup = 1, slots = 0;
   if ((st = ghb_sync(P.ctx, P.s)) || (st = ghb_join_table_info(P.ctx, jt, &rows, &max_dup, &slots))) {
     ghb_join_table_free(P.ctx, jt);
@@ -218,18 +243,17 @@ int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable
   }
   int64_t per = op.join_type == GHB_LEFT_SEMI_JOIN ? 1 : std::max<int64_t>(1, max_dup);
   const int64_t cap = std::max<int64_t>(1, t.rows * per);
-  std::vector<ghb_column> probe = descs(t);
   DevTable o;
   const int np = (int)t.cols.size();
   o.cols.resize(np + op.nbuild_keep);
   std::vector<ghb_out_column> op_out(np), ob_out(op.nbuild_keep);
   for (int j = 0; j < np && !st; j++) st = P.out_col(t.cols[j].type, cap, &o.cols[j], &op_out[j]);
   for (int j = 0; j < op.nbuild_keep && !st; j++)
-    st = P.out_col(b.cols[1 + j].type, cap, &o.cols[np + j], &ob_out[j]);
+    st = P.out_col(b.cols[nk + j].type, cap, &o.cols[np + j], &ob_out[j]);
   int64_t* d_rows = nullptr;
   if (!st) st = P.alloc(8, (void**)&d_rows);
   if (!st)
-    st = ghb_join_probe(P.ctx, jt, &probe[pk], op.join_type, ob_out.data(), probe.data(), np, op_out.data(),
+    st = ghb_join_probe(P.ctx, jt, &pkey, op.join_type, ob_out.data(), probe.data(), np, op_out.data(),
                         nullptr, nullptr, cap, d_rows, P.s);
   if (!st) st = P.read_count(d_rows, &o.rows);
   ghb_join_table_free(P.ctx, jt);

@@ -96,7 +96,13 @@ def op_groupby(keys, aggs, max_groups=0):
 
 
 def op_join(probe_key, build_table, build_key, build_keep=(), join_type=abi.INNER_JOIN):
-    return {"op": abi.OP_JOIN_PROBE, "idx": [probe_key, build_key], "build_table": build_table,
+    """probe_key / build_key: one column index each, or equally long lists
+    (a key of several columns)."""
+    pk = list(probe_key) if isinstance(probe_key, (list, tuple)) else [probe_key]
+    bk = list(build_key) if isinstance(build_key, (list, tuple)) else [build_key]
+    if len(pk) != len(bk):
+        raise ValueError("probe and build keys differ in length")
+    return {"op": abi.OP_JOIN_PROBE, "idx": pk + bk, "build_table": build_table,
             "build_keep": list(build_keep), "join_type": join_type}
 
 

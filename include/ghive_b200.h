@@ -549,8 +549,10 @@ typedef struct ghb_plan_op {
   const ghb_predicate* pred;   /* FILTER                                       */
   const int32_t* idx;          /* FILTER: projection (NULL = all columns);
                                   GROUPBY: key columns; SORT: key columns;
-                                  JOIN_PROBE: {probe key column, build key
-                                  column of the build table}                  */
+                                  JOIN_PROBE: the k probe key columns, then
+                                  the k build key columns of the build table
+                                  (k > 1: the tuples are packed into one key,
+                                  fixed-width columns, 63 bits at most)        */
   int32_t nidx;
   int32_t naggs;               /* GROUPBY                                      */
   const ghb_agg_desc* aggs;

@@ -108,3 +108,40 @@ def test_missing_input_table_is_refused(ctx):
     assert e.value.code == abi.ERR_INVALID
     r = run_plan(ctx, gt, 0, [op_sort([0], orders=[abi.DESC])])
     assert np.array_equal(r["columns"][0][0], np.arange(10)[::-1])
+
+
+def test_three_table_chain_with_two_column_keys(ctx):
+    """An N-way map-join chain (SortMergeJoinPredicate.cu:257-454 joins each
+    further table to the tuples so far): lineorder probes a (year, month)
+    calendar on two key columns, then a supplier table on one, then GROUP BY
+    the calendar's quarter and the supplier's region."""
+    g = np.random.default_rng(93)
+    n = 400_000
+    year = g.integers(1992, 1999, n, dtype=np.int32)
+    month = g.integers(1, 13, n, dtype=np.int32)
+    supp = g.integers(0, 2_200, n, dtype=np.int64)
+    rev = g.integers(1, 100_000, n, dtype=np.int64)
+    cy = np.repeat(np.arange(1992, 1998, dtype=np.int32), 12)        # 1998 missing: no match
+    cm = np.tile(np.arange(1, 13, dtype=np.int32), 6)
+    cq = ((cm - 1) // 3 + 1).astype(np.int32)
+    skey = np.arange(0, 2_000, dtype=np.int64)                        # keys >= 2000 missing
+    sreg = g.integers(0, 5, 2_000, dtype=np.int32)
+    gt = GTables([("Map 1", 0, [year, month, supp, rev]), ("Map 2", 2, [cy, cm, cq]),
+                  ("Map 3", 1, [skey, sreg])])
+    aggs = [(abi.CNT, -1), (abi.SUM, 3)]
+    r = run_plan(ctx, gt, 0, [op_join([0, 1], 1, [0, 1], build_keep=[2]),
+                              op_join(2, 2, 0, build_keep=[1]),            # + quarter (4), region (5)
+                              op_groupby([4, 5], aggs, max_groups=64), op_sort([0, 1])])
+    cal = {(y, m): q for y, m, q in zip(cy, cm, cq)}
+    reg = dict(zip(skey.tolist(), sreg.tolist()))
+    exp = {}
+    for y, m, s, v in zip(year.tolist(), month.tolist(), supp.tolist(), rev.tolist()):
+        if (y, m) in cal and s in reg:
+            k = (int(cal[(y, m)]), reg[s])
+            c, t = exp.get(k, (0, 0))
+            exp[k] = (c + 1, t + v)
+    keys = sorted(exp)
+    assert r["rows"] == len(keys)
+    (q, _), (rg, _), (cnt, _), (sm, _) = r["columns"]
+    assert list(zip(q.tolist(), rg.tolist())) == keys
+    assert cnt.tolist() == [exp[k][0] for k in keys] and sm.tolist() == [exp[k][1] for k in keys]
