@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -159,11 +160,26 @@ struct KeyPackPlan {
 };
 // Scratch bytes the packing needs beside the group-by itself.
 inline size_t keypack_scratch_bytes(int64_t n, int64_t cap) {
+  int64_t slots = 64;   // a tuple table of twice the groups (keys too wide to pack)
+  while (slots < 2 * std::min<int64_t>(std::max<int64_t>(n, 1), std::max<int64_t>(cap, 1))) slots <<= 1;
   return 3 * 8 * kMaxPackKeys + 256 + (((size_t)n * 8 + 255) & ~(size_t)255) +
-         (((size_t)cap * 8 + 255) & ~(size_t)255) + 512;
+         (((size_t)cap * 8 + 255) & ~(size_t)255) + (size_t)slots * 8 + 1024;
 }
+// Plans the packing and writes the packed keys; *too_wide (and nothing
+// written) when the tuples need more than 63 bits.
 int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys,
-                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream);
+                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream, bool* too_wide);
+// Tuples too wide to pack: rep[r] = the row of row r's tuple's first
+// occurrence (INT64_MAX where pass is 0); `slots` (power of two, >= twice the
+// distinct tuples) of table, cleared here.  A full table raises
+// GHB_ERR_CAPACITY on the device.
+int32_t tuple_rep_rows(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys, int64_t n,
+                       const int32_t* pass, int64_t* rep, unsigned long long* table, int64_t slots,
+                       cudaStream_t stream);
+// The key tuple of each output group, from the group's first row.
+int32_t tuple_unpack(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, const KeyPackPlan& plan,
+                     const int64_t* rows, const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
+                     cudaStream_t stream);
 int32_t keypack_unpack(ghb_ctx* ctx, const KeyPackPlan& plan, const int64_t* packed,
                        const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
                        cudaStream_t stream);

@@ -367,7 +367,7 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
                                                                                             : out_capacity));
     const int64_t slots = next_pow2_i64(std::max<int64_t>(64, 2 * hint));
     if (ctx->scratch_used == 0) {
-      size_t need = keypack_scratch_bytes(n, out_capacity) + (size_t)n * 4 + 512 +
+      size_t need = keypack_scratch_bytes(n, out_capacity) + (size_t)n * 4 + 512 + (size_t)slots * 8 + 512 +
                     (size_t)nstr * (((size_t)n * 8 + 255) + (size_t)slots * 8 + 512);
       if ((st = scratch_reserve(ctx, need, stream))) return st;
     }
@@ -417,8 +417,25 @@ int32_t filter_groupby_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_c
     if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 8, (void**)&packed, stream))) return st;
     if ((st = scratch_alloc(ctx, (size_t)out_capacity * 8, (void**)&kout, stream))) return st;
     KeyPackPlan plan;
-    if ((st = keypack_prepare(ctx, pc, kc, nkeys, n, packed, &plan, stream))) return st;
+    bool too_wide = false;
+    if ((st = keypack_prepare(ctx, pc, kc, nkeys, n, packed, &plan, stream, &too_wide))) return st;
     for (int j = 0; j < nkeys; j++) plan.str_aux[j] = str_aux[j];
+    if (too_wide) {
+      // group by the row of each tuple's first occurrence, then read each
+      // group's tuple back from that row
+      unsigned long long* table = nullptr;
+      if ((st = scratch_alloc(ctx, (size_t)slots * 8, (void**)&table, stream))) return st;
+      if ((st = tuple_rep_rows(ctx, pc, kc, nkeys, n, pass, packed, table, slots, stream))) return st;
+      pc[pn] = ghb_column{GHB_LONG, GHB_NULLS_SENTINEL, packed, nullptr, nullptr, n};
+      ghb_out_column po[kMaxAggs + 1];
+      po[0] = ghb_out_column{GHB_LONG, 0, kout, nullptr};
+      for (int i = 0; i < naggs && i < kMaxAggs; i++) po[1 + i] = out[nkeys + i];
+      const int32_t pk = pn++;
+      st = filter_groupby_impl(ctx, fpred, pc, pn, &pk, 1, aggs, naggs, po, out_capacity, d_out_groups, cfg,
+                               stream, nullptr, 0);
+      if (st) return st;
+      return tuple_unpack(ctx, pc, kc, plan, kout, d_out_groups, out_capacity, out, stream);
+    }
     pc[pn] = ghb_column{GHB_LONG, GHB_NULLS_NONE, packed, nullptr, nullptr, n};
     ghb_out_column po[kMaxAggs + 1];
     po[0] = ghb_out_column{GHB_LONG, 0, kout, nullptr};

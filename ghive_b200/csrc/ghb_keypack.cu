@@ -20,7 +20,9 @@
 //   4. after the group-by, the packed key of each output group is unpacked
 //      into the caller's key output columns (NULL components as NULL).
 //
-// Key tuples that need more than 63 bits are refused (GHB_ERR_UNSUPPORTED).
+// Key tuples that need more than 63 bits (a DOUBLE key of both signs, two
+// full-range LONG keys) are grouped instead by the row of each tuple's first
+// occurrence, found through a lock-free device hash table of the tuples.
 #include <algorithm>
 
 #include "ghb_ctx.hpp"
@@ -220,7 +222,7 @@ int32_t predicate_pass(ghb_ctx* ctx, const PredProg& prog, const ghb_column* col
 // values) to `packed`.  Reads the keys' ranges back to the host (one
 // stream synchronisation).
 int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys,
-                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream) {
+                        int64_t n, int64_t* packed, KeyPackPlan* plan, cudaStream_t stream, bool* too_wide) {
   if (nkeys < 1 || nkeys > kMaxPackKeys)
     return set_error(ctx, GHB_ERR_UNSUPPORTED, "%d key columns: at most %d", nkeys, kMaxPackKeys);
   KeyPackPlan& P = *plan;
@@ -267,11 +269,143 @@ int32_t keypack_prepare(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key
       P.fshift[j] = (int8_t)bits;
       bits++;
     }
-    if (bits > 63)
-      return set_error(ctx, GHB_ERR_UNSUPPORTED,
-                       "the %d key columns' value ranges need more than 63 bits together", nkeys);
+    if (bits > 63) {   // the caller groups by first occurrences instead
+      *too_wide = true;
+      return GHB_OK;
+    }
   }
+  *too_wide = false;
   keypack_pack_kernel<<<grid, 256, 0, stream>>>(P, n, packed);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+// ---- key tuples too wide to pack: the row of each tuple's first occurrence
+struct TupleCols {
+  int32_t nkeys;
+  ghb_column col[kMaxPackKeys];
+};
+
+__device__ __forceinline__ uint64_t tuple_hash(const TupleCols& t, int64_t r) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+#pragma unroll
+  for (int j = 0; j < kMaxPackKeys; j++) {
+    if (j >= t.nkeys) break;
+    const int64_t raw = ld_raw(t.col[j], r);
+    const bool null = t.col[j].null_mode != GHB_NULLS_NONE && raw_is_null(t.col[j], raw, r);
+    h = mix64(h ^ (null ? 0x5bd1e9955bd1e995ull : (uint64_t)raw) ^ ((uint64_t)j << 56));
+  }
+  return h;
+}
+
+// Equal tuples: per key both NULL, or both non-NULL with the same raw value
+// (the single-key group-by's rule: a double key by its bits).
+__device__ __forceinline__ bool tuple_equal(const TupleCols& t, int64_t a, int64_t b) {
+#pragma unroll
+  for (int j = 0; j < kMaxPackKeys; j++) {
+    if (j >= t.nkeys) break;
+    const ghb_column& c = t.col[j];
+    const int64_t x = ld_raw(c, a), y = ld_raw(c, b);
+    const bool nx = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, x, a);
+    const bool ny = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, y, b);
+    if (nx != ny || (!nx && x != y)) return false;
+  }
+  return true;
+}
+
+// The same lock-free table of (hash tag << 32 | row + 1) words as the STRING
+// keys': the first row of a tuple claims a slot, later rows compare tuples
+// with the claiming row's own.
+__global__ void __launch_bounds__(256) tuple_rep_kernel(TupleCols t, const int32_t* pass, int64_t n, int64_t* rep,
+                                                         unsigned long long* table, int64_t mask, int32_t* status) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    if (pass && pass[r] == 0) {
+      rep[r] = INT64_MAX;
+      continue;
+    }
+    const uint64_t h = tuple_hash(t, r);
+    const uint32_t tag = (uint32_t)(h >> 32) | 1u;
+    const unsigned long long mine = ((unsigned long long)tag << 32) | (unsigned long long)(r + 1);
+    int64_t s = (int64_t)(h & (uint64_t)mask), found = -1;
+    for (int64_t probe = 0; probe <= mask; probe++) {
+      unsigned long long w = *(volatile unsigned long long*)&table[s];
+      if (w == 0) {
+        const unsigned long long old = atomicCAS(&table[s], 0ull, mine);
+        if (old == 0) {
+          found = r;
+          break;
+        }
+        w = old;
+      }
+      if ((uint32_t)(w >> 32) == tag) {
+        const int64_t o = (int64_t)(w & 0xffffffffull) - 1;
+        if (tuple_equal(t, o, r)) {
+          found = o;
+          break;
+        }
+      }
+      s = (s + 1) & mask;
+    }
+    if (found < 0) raise_status(status, kDevCapacity);   // more distinct tuples than slots
+    rep[r] = found < 0 ? INT64_MAX : found;
+  }
+}
+
+// Each output group's key tuple from its first row: the key columns' values
+// (NULL as GHive's sentinel and in the NULL map), a STRING key's [start,end).
+__global__ void __launch_bounds__(256) tuple_unpack_kernel(TupleCols t, KeyPackPlan p, const int64_t* rows,
+                                                            const int64_t* d_groups, int64_t cap, KeyOuts outs) {
+  const int64_t g = min(*d_groups, cap);
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < g; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = rows[r];
+#pragma unroll
+    for (int j = 0; j < kMaxPackKeys; j++) {
+      if (j >= t.nkeys) break;
+      const ghb_column& c = t.col[j];
+      const ghb_out_column& o = outs.o[j];
+      const int64_t raw = ld_raw(c, row);
+      const bool null = c.null_mode != GHB_NULLS_NONE && raw_is_null(c, raw, row);
+      if (o.is_null) o.is_null[r] = null ? 1 : 0;
+      if (p.str_aux[j]) {
+        ((int2*)o.data)[r] = null ? make_int2(-1, -1) : p.str_aux[j][raw];
+        continue;
+      }
+      switch (o.type) {
+        case GHB_LONG: ((int64_t*)o.data)[r] = null ? INT64_MAX : raw; break;
+        case GHB_INT: ((int32_t*)o.data)[r] = null ? INT32_MAX : (int32_t)raw; break;
+        case GHB_DOUBLE: ((int64_t*)o.data)[r] = null ? 0x7ff8000000000000ll : raw; break;
+      }
+    }
+  }
+}
+
+int32_t tuple_rep_rows(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, int32_t nkeys, int64_t n,
+                       const int32_t* pass, int64_t* rep, unsigned long long* table, int64_t slots,
+                       cudaStream_t stream) {
+  if (n >= (int64_t)UINT32_MAX - 1) return set_error(ctx, GHB_ERR_UNSUPPORTED, "key tuples of 2^32 rows");
+  TupleCols t;
+  std::memset(&t, 0, sizeof(t));
+  t.nkeys = nkeys;
+  for (int j = 0; j < nkeys; j++) t.col[j] = cols[key_cols[j]];
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(table, 0, (size_t)slots * 8, stream));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  tuple_rep_kernel<<<grid, 256, 0, stream>>>(t, pass, n, rep, table, slots - 1, ctx->d_status);
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
+int32_t tuple_unpack(ghb_ctx* ctx, const ghb_column* cols, const int32_t* key_cols, const KeyPackPlan& plan,
+                     const int64_t* rows, const int64_t* d_groups, int64_t cap, const ghb_out_column* key_out,
+                     cudaStream_t stream) {
+  TupleCols t;
+  std::memset(&t, 0, sizeof(t));
+  t.nkeys = plan.nkeys;
+  for (int j = 0; j < plan.nkeys; j++) t.col[j] = cols[key_cols[j]];
+  KeyOuts outs;
+  std::memset(&outs, 0, sizeof(outs));
+  for (int j = 0; j < plan.nkeys; j++) outs.o[j] = key_out[j];
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->num_sms * 4));
+  tuple_unpack_kernel<<<grid, 256, 0, stream>>>(t, plan, rows, d_groups, cap, outs);
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;
 }

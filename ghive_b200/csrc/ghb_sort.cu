@@ -257,8 +257,6 @@ struct PassParams {
   uint64_t* keys_out;
   void* vals_out;
   ghb_column pay_src;        // single carried payload (when !carry_rowid)
-  int32_t nsub;              // the first pass of a segment packs from these
-  SubPlan sub[kMaxSub];
   ghb_out_column out_keys[kMaxSortKeys];
   int32_t npay;
   ghb_column pay[kMaxSortPay];
@@ -337,30 +335,14 @@ __device__ __forceinline__ void decode_write(const PassParams& p, uint64_t k, ui
   }
 }
 
-// Streamed (evict-first) loads and stores of the carried 32- or 64-bit values.
-__device__ __forceinline__ uint32_t ld_val_cs(const uint32_t* a) { return __ldcs((const unsigned int*)a); }
-__device__ __forceinline__ uint64_t ld_val_cs(const uint64_t* a) {
-  return __ldcs((const unsigned long long*)a);
-}
-__device__ __forceinline__ void st_val_cs(uint32_t* a, uint32_t v) { __stcs((unsigned int*)a, v); }
-__device__ __forceinline__ void st_val_cs(uint64_t* a, uint64_t v) {
-  __stcs((unsigned long long*)a, (unsigned long long)v);
-}
-
-// One LSD pass over the digit at `p.shift`, onesweep-style: each CTA claims
-// tiles in launch order; per tile it counts the warps' digits (publishing the
-// tile's per-digit counts at once), ranks each row stably among the tile's
-// rows of its digit, reorders the tile in shared memory by digit, gets each
-// digit's global offset by decoupled look-back over earlier tiles, and
-// writes one run per digit.
 template <typename V, int SRC, int DST>
-__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(PassParams p) {
-  // per-warp digit counts, then each warp's first tile-local position per digit
-  __shared__ uint32_t s_cnt[kSortThreads / 32][kBins];
-  __shared__ int64_t s_gbase[kBins];          // global position of tile-local position 0, per digit
+__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
+  __shared__ uint32_t s_whist[kSortThreads / 32][kBins];  // per-warp counts, then exclusive over warps
+  __shared__ uint32_t s_bexcl[kBins];                      // block-local exclusive offset per digit
+  __shared__ uint64_t s_gbase[kBins];                      // global destination of each digit's run
   __shared__ uint32_t s_wsum[kSortThreads / 32];
   __shared__ int64_t s_tile;
-  extern __shared__ uint64_t s_dyn[];          // reordered tile: keys, then values
+  extern __shared__ uint64_t s_dyn[];                      // reordered tile: keys, then values
   uint64_t* s_keys = s_dyn;
   V* s_vals = (V*)(s_dyn + kSortTile);
   const int lane = threadIdx.x & 31;
@@ -378,170 +360,147 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(PassParams p
       if (*(volatile int32_t*)p.dev_status == kDevTimeout) t = p.ntiles;
       s_tile = t;
     }
-    for (int i = threadIdx.x; i < (kSortThreads / 32) * kBins; i += kSortThreads) (&s_cnt[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < (kSortThreads / 32) * kBins; i += kSortThreads) (&s_whist[0][0])[i] = 0;
     __syncthreads();
     const int64_t tile = s_tile;
     if (tile >= p.ntiles) break;
-    // this warp's rows: 32 * kSortItems consecutive rows, item k at k * 32 + lane
     const int64_t wbase = tile * kSortTile + (int64_t)warp * (32 * kSortItems);
-    const int64_t left = p.n - wbase;
-    const int wlive = left <= 0 ? 0 : (left >= 32 * kSortItems ? 32 * kSortItems : (int)left);
 
     uint64_t key[kSortItems];
     V val[kSortItems];
     if (SRC == kSrcPacked) {
 #pragma unroll
       for (int k = 0; k < kSortItems; k++) {
-        const int r = k * 32 + lane;
-        key[k] = r < wlive ? __ldcs((const unsigned long long*)p.keys_in + wbase + r) : ~0ull;
+        int64_t row = wbase + k * 32 + lane;
+        key[k] = row < p.n ? __ldcs((const unsigned long long*)p.keys_in + row) : ~0ull;
       }
 #pragma unroll
       for (int k = 0; k < kSortItems; k++) {
-        const int r = k * 32 + lane;
-        val[k] = r < wlive ? ld_val_cs(vals_in + wbase + r) : (V)0;
+        int64_t row = wbase + k * 32 + lane;
+        val[k] = row < p.n ? vals_in[row] : (V)0;
       }
-    } else if (SRC == kSrcCols) {
-      // the first pass packs the key from the user's columns: one sub-field
-      // at a time over all items (independent loads), constant plan indices
-#pragma unroll
-      for (int k = 0; k < kSortItems; k++) key[k] = 0;
-#pragma unroll
-      for (int i = 0; i < kMaxSub; i++) {
-        if (i >= p.nsub) break;
-        const SubPlan& sp = p.sub[i];
-        int64_t raw[kSortItems];
-#pragma unroll
-        for (int k = 0; k < kSortItems; k++) {
-          const int r = k * 32 + lane;
-          raw[k] = r < wlive ? ld_raw_cs(sp.col, wbase + r) : 0;
-        }
-#pragma unroll
-        for (int k = 0; k < kSortItems; k++) {
-          const int r = k * 32 + lane;
-          if (r < wlive) key[k] |= sub_bits_plan(sp, raw[k], wbase + r);
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < kSortItems; k++) {
-        const int r = k * 32 + lane;
-        if (r >= wlive) key[k] = ~0ull;
-        if (p.carry_rowid) val[k] = (V)(wbase + r);
-        else val[k] = r < wlive ? (V)ld_raw_cs(p.pay_src, wbase + r) : (V)0;
-      }
-    } else {  // kSrcPerm: a later segment, packed from the row order the previous one left
+    } else {
       int64_t src[kSortItems];
 #pragma unroll
       for (int k = 0; k < kSortItems; k++) {
-        const int r = k * 32 + lane;
+        int64_t row = wbase + k * 32 + lane;
         key[k] = 0;
-        src[k] = r < wlive ? (int64_t)vals_in[wbase + r] : 0;
+        if (SRC == kSrcPerm) src[k] = row < p.n ? (int64_t)vals_in[row] : 0;
+        else src[k] = row;
       }
+      // one sub-field at a time over all items: the loads are independent
       for (int i = 0; i < p.seg.n; i++) {
         const SubField sf = p.seg.f[i];
 #pragma unroll
         for (int k = 0; k < kSortItems; k++) {
-          const int r = k * 32 + lane;
-          if (r < wlive) key[k] |= sub_bits(p.K, sf, src[k]);
+          int64_t row = wbase + k * 32 + lane;
+          if (row < p.n) key[k] |= sub_bits(p.K, sf, src[k]);
         }
       }
 #pragma unroll
       for (int k = 0; k < kSortItems; k++) {
-        const int r = k * 32 + lane;
-        if (r >= wlive) key[k] = ~0ull;
-        val[k] = (V)src[k];
+        int64_t row = wbase + k * 32 + lane;
+        if (row >= p.n) key[k] = ~0ull;
+        if (p.carry_rowid) val[k] = (V)src[k];
+        else val[k] = row < p.n ? (V)ld_raw(p.pay_src, row) : (V)0;
       }
     }
-
-    // 1. counts of the warp's digits: one shared atomic per distinct digit of
-    // an item (the lowest lane of its peers adds their number).  Rows past the
-    // end take a digit value no row has.
+    // stable rank of each key among the warp's keys with the same digit
+    uint32_t rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; k++) {
-      const bool live = k * 32 + lane < wlive;
-      const uint32_t d = live ? (uint32_t)(key[k] >> p.shift) & (kBins - 1) : 0xFFFFFFFFu;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      if (live && (peers & lt) == 0) atomicAdd(&s_cnt[warp][d], (uint32_t)__popc(peers));
+      int64_t row = wbase + k * 32 + lane;
+      bool live = row < p.n;
+      uint32_t d = (uint32_t)(key[k] >> p.shift) & (kBins - 1);
+      unsigned peers = __ballot_sync(0xffffffffu, live);
+#pragma unroll
+      for (int b = 0; b < kDigitBits; b++) {
+        unsigned bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? bb : ~bb;
+      }
+      uint32_t before = live ? s_whist[warp][d] : 0;
+      __syncwarp();
+      if (live && (peers & lt) == 0) s_whist[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[k] = before + __popc(peers & lt);
     }
     __syncthreads();
-    // 2. per digit (a thread each): the tile's count, published at once so
-    // later tiles' look-backs can pass this one; each warp's offset within
-    // the digit; the digit's tile-local start by a block-wide scan
+    // per digit (one thread each): exclusive over warps, block total
     const int d = threadIdx.x;  // kSortThreads == kBins
     uint32_t total = 0;
 #pragma unroll
     for (int w = 0; w < kSortThreads / 32; w++) {
-      const uint32_t c = s_cnt[w][d];
-      s_cnt[w][d] = total;
+      uint32_t c = s_whist[w][d];
+      s_whist[w][d] = total;
       total += c;
     }
-    uint64_t* st = p.status + tile * kBins;
-    lb_store(&st[d], lb_pack(p.epoch, tile == 0 ? kFlagPrefix : kFlagAgg, total));
-    uint32_t incl = total;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) s_wsum[warp] = incl;
-    __syncthreads();
-    uint32_t wpre = 0;
-#pragma unroll
-    for (int w = 0; w < kSortThreads / 32; w++) wpre += w < warp ? s_wsum[w] : 0;
-    const uint32_t bexcl = wpre + incl - total;
-#pragma unroll
-    for (int w = 0; w < kSortThreads / 32; w++) s_cnt[w][d] += bexcl;
-    __syncthreads();
-    // 3. stable rank and scatter into shared memory in digit order: the warp
-    // walks its items in row order; the lowest lane of each digit's peers
-    // claims their positions (the previous item's claims of this warp are
-    // complete: the shuffle below waits for each claim's result)
-#pragma unroll
-    for (int k = 0; k < kSortItems; k++) {
-      const bool live = k * 32 + lane < wlive;
-      const uint32_t dk = live ? (uint32_t)(key[k] >> p.shift) & (kBins - 1) : 0xFFFFFFFFu;
-      const unsigned peers = __match_any_sync(0xffffffffu, dk);
-      const int leader = __ffs(peers) - 1;
-      uint32_t first = 0;
-      if (live && lane == leader) first = atomicAdd(&s_cnt[warp][dk], (uint32_t)__popc(peers));
-      first = __shfl_sync(0xffffffffu, first, leader);
-      if (live) {
-        const uint32_t at = first + __popc(peers & lt);
-        s_keys[at] = key[k];
-        s_vals[at] = val[k];
-      }
-    }
-    // 4. the digit's global offset: decoupled look-back over earlier tiles
+    // publish this tile's count of digit d, then look back for its prefix
     {
+      uint64_t* st = p.status + tile * kBins;
       uint64_t excl = 0;
-      if (tile > 0) {
+      if (tile == 0) {
+        lb_store(&st[d], lb_pack(p.epoch, kFlagPrefix, total));
+      } else {
+        lb_store(&st[d], lb_pack(p.epoch, kFlagAgg, total));
         int64_t t = tile - 1;
         int spins = 0;
         while (t >= 0) {
-          const uint64_t v = lb_load(&p.status[t * kBins + d]);
-          const bool ok = ((v >> kEpochShift) & kEpochMask) == (p.epoch & kEpochMask);
+          uint64_t v = lb_load(&p.status[t * kBins + d]);
+          bool ok = ((v >> kEpochShift) & kEpochMask) == (p.epoch & kEpochMask);
           if (ok && (v & kFlagPrefix)) { excl += v & kCountMask; break; }
           if (ok && (v & kFlagAgg)) { excl += v & kCountMask; t--; continue; }
           if (++spins >= p.spin_limit) { raise_status(p.dev_status, kDevTimeout); break; }
         }
         lb_store(&st[d], lb_pack(p.epoch, kFlagPrefix, excl + total));
       }
-      s_gbase[d] = (int64_t)p.digit_base[d] + (int64_t)excl - (int64_t)bexcl;
+      s_gbase[d] = (uint64_t)p.digit_base[d] + excl;
+    }
+    // block-wide exclusive scan of the per-digit totals
+    {
+      uint32_t incl = total;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) s_wsum[warp] = incl;
+      __syncthreads();
+      if (warp == 0) {
+        uint32_t v = lane < kSortThreads / 32 ? s_wsum[lane] : 0;
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += t;
+        }
+        if (lane < kSortThreads / 32) s_wsum[lane] = x - v;
+      }
+      __syncthreads();
+      s_bexcl[d] = s_wsum[warp] + incl - total;
     }
     __syncthreads();
-    // 5. write the reordered tile: element i goes to s_gbase[digit] + i, one
-    // run per digit
-    const int tile_n = (int)min((int64_t)kSortTile, p.n - tile * kSortTile);
-#pragma unroll 4
+    // scatter into shared memory in digit order (stable)
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+      int64_t row = wbase + k * 32 + lane;
+      if (row >= p.n) continue;
+      uint32_t dk = (uint32_t)(key[k] >> p.shift) & (kBins - 1);
+      uint32_t at = s_bexcl[dk] + s_whist[warp][dk] + rank[k];
+      s_keys[at] = key[k];
+      s_vals[at] = val[k];
+    }
+    __syncthreads();
+    // write runs: element i of the reordered tile goes to gbase[d] + (i - bexcl[d])
+    const int64_t tile_n = min((int64_t)kSortTile, p.n - tile * kSortTile);
     for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
-      const uint64_t k = s_keys[i];
-      const uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
-      const int64_t pos = s_gbase[dk] + i;
+      uint64_t k = s_keys[i];
+      uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
+      int64_t pos = (int64_t)(s_gbase[dk] + (i - s_bexcl[dk]));
       if (DST == kDstDecode) {
         decode_write(p, k, (uint64_t)s_vals[i], pos);
       } else if (DST == kDstGather) {
         gather_write(p, (int64_t)s_vals[i], pos);
       } else {
         __stcs((unsigned long long*)p.keys_out + pos, (unsigned long long)k);
-        st_val_cs(vals_out + pos, s_vals[i]);
+        vals_out[pos] = s_vals[i];
       }
     }
     __syncthreads();
@@ -613,27 +572,8 @@ static int32_t set_smem(ghb_ctx* ctx, size_t dyn) {
   return GHB_OK;
 }
 
-// The sub-fields of segment `sg` as self-contained plans (constant indices
-// in the kernels that pack keys).
-static int fill_sub_plans(const KeySet& K, const Segment& sg, SubPlan* out) {
-  for (int i = 0; i < sg.n; i++) {
-    const SubField& sf = sg.f[i];
-    const KeyField& kf = K.k[sf.key];
-    SubPlan& sp = out[i];
-    sp.col = kf.col;
-    sp.umin = kf.umin;
-    sp.shift = sf.shift;
-    sp.is_flag = sf.is_flag;
-    sp.desc = (int8_t)kf.desc;
-    sp.nulls_first = (int8_t)kf.nulls_first;
-    sp.has_null = (int8_t)kf.has_null;
-  }
-  return sg.n;
-}
-
 // kb / vb: key and value ping-pong buffers; packed: kb[0] / vb[0] already
-// hold the packed keys and values of a one-segment key (else the first pass
-// packs them from the key columns).
+// hold the packed keys and values of a one-segment key.
 template <typename V>
 static int32_t run_passes(ghb_ctx* ctx, PassParams& pp, const std::vector<Segment>& segs,
                           const std::vector<std::vector<int>>& run, const std::vector<uint32_t>& hist,
@@ -666,7 +606,6 @@ static int32_t run_passes(ghb_ctx* ctx, PassParams& pp, const std::vector<Segmen
   int cur = 0;
   for (size_t s = 0; s < segs.size(); s++) {
     pp.seg = segs[s];
-    pp.nsub = fill_sub_plans(pp.K, segs[s], pp.sub);
     for (size_t i = 0; i < run[s].size(); i++) {
       int q = run[s][i];
       bool last = ++done == total;
@@ -792,7 +731,8 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     if ((st = scratch_alloc(ctx, (size_t)n * vw, &vb[i], stream))) return st;
   }
 
-  // histograms of every segment, one read each, then one sync
+  // histograms of every segment, one read each, then one sync; a
+  // one-segment key is packed on the way
   GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_hist, 0, segs.size() * kMaxPasses * kBins * 4, stream));
   for (size_t s = 0; s < segs.size(); s++) {
     int np = (segs[s].bits + kDigitBits - 1) / kDigitBits;
@@ -803,11 +743,19 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     hp.n = n;
     hp.npasses = np;
     hp.hist = d_hist + s * kMaxPasses * kBins;
-    fill_sub_plans(K, segs[s], hp.sub);
-    // the first radix pass packs the keys from the columns itself: reading
-    // the columns there costs no more than reading packed keys, and the
-    // histogram pass then writes nothing
-    hp.keys_out = nullptr;
+    for (int i = 0; i < segs[s].n; i++) {
+      const SubField& sf = segs[s].f[i];
+      const KeyField& kf = K.k[sf.key];
+      SubPlan& sp = hp.sub[i];
+      sp.col = kf.col;
+      sp.umin = kf.umin;
+      sp.shift = sf.shift;
+      sp.is_flag = sf.is_flag;
+      sp.desc = (int8_t)kf.desc;
+      sp.nulls_first = (int8_t)kf.nulls_first;
+      sp.has_null = (int8_t)kf.has_null;
+    }
+    hp.keys_out = multi ? nullptr : kb[0];
     hp.vals_out = vb[0];
     hp.vals_wide = wide ? 1 : 0;
     hp.carry_rowid = carry_rowid ? 1 : 0;
@@ -858,7 +806,7 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   pp.counters = ctx->d_counters + 2;
   pp.dev_status = ctx->d_status;
   pp.spin_limit = ctx->spin_limit;
-  const bool packed = false;
+  const bool packed = !multi;
   if (wide) return run_passes<uint64_t>(ctx, pp, segs, run, hist, kb, vb, packed, stream);
   return run_passes<uint32_t>(ctx, pp, segs, run, hist, kb, vb, packed, stream);
 }

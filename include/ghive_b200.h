@@ -252,8 +252,9 @@ int32_t ghb_filter(ghb_ctx* ctx, const ghb_predicate* pred,
  * empty input).  d_out_groups (device int64) receives the group count.
  * Several key columns (GroupByPredicate.cu:24-105 sorts by all of them) are
  * packed into one 64-bit key per row after one read of their ranges (a
- * stream synchronisation); key columns whose ranges need more than 63 bits
- * together are refused with GHB_ERR_UNSUPPORTED.  STRING key columns are
+ * stream synchronisation); key tuples whose ranges need more than 63 bits
+ * together are grouped by the row of each tuple's first occurrence (a device
+ * hash table of the tuples).  STRING key columns are
  * first mapped to the row of their value's first occurrence on the device
  * (GroupByPredicate.hpp:75-101 compares the bytes); a STRING key's output is
  * [start,end) pairs into the key column's own bytes.  STRING columns may be

@@ -612,18 +612,22 @@ def test_groupby_several_keys_nulls_types_and_extremes(ctx):
     _check_groupby(ctx, None, [b[:0], c[:0], v[:0]], [0, 1], [(abi.SUM, 2)], max_groups=4)
 
 
-def test_groupby_several_keys_too_wide_is_refused(ctx):
-    from ghive_b200._lib import GhbError
+def test_groupby_several_keys_too_wide_to_pack(ctx):
+    """Key tuples whose ranges need more than 63 bits (two full-range LONG
+    keys, a DOUBLE key of both signs beside them) are grouped by the row of
+    each tuple's first occurrence instead of a packed key."""
     g = np.random.default_rng(62)
-    n = 10_000
+    n = 60_000
     i64 = np.iinfo(np.int64)
-    a = g.integers(i64.min, i64.max, n, dtype=np.int64)
-    b = g.integers(i64.min, i64.max, n, dtype=np.int64)
-    with pytest.raises(GhbError) as e:
-        ctx.filter_groupby(None, [dev(a), dev(b)], [0, 1], [(abi.CNT, -1)], capacity=n, max_groups=n)
-    assert e.value.code == abi.ERR_UNSUPPORTED
-    # the context stays usable
-    _check_groupby(ctx, None, [a % 10, b % 10], [0, 1], [(abi.CNT, -1)], max_groups=400)
+    a = g.integers(i64.min, i64.max, 300, dtype=np.int64)[g.integers(0, 300, n)]
+    b = g.integers(i64.min, i64.max, 7, dtype=np.int64)[g.integers(0, 7, n)]
+    bn = g.random(n) < 0.1
+    c = g.normal(0, 1e6, 5)[g.integers(0, 5, n)]
+    v = g.integers(-1000, 1000, n, dtype=np.int64)
+    aggs = [(abi.CNT, -1), (abi.SUM, 3), (abi.MIN, 3)]
+    _check_groupby(ctx, None, [a, (b, bn), c, v], [0, 1], aggs, max_groups=300 * 8)
+    _check_groupby(ctx, abi.Pred.leaf(abi.FILTER_GT, 3, a=0), [a, (b, bn), c, v], [2, 0, 1], aggs,
+                   max_groups=300 * 8 * 5)
 
 
 def test_groupby_several_keys_host_entry_point(ctx):
