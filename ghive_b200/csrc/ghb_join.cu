@@ -298,6 +298,12 @@ __global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool unique = p.stats[1] <= 1;
+  // every key of [min, max] present once (a dense surrogate key): a probe key
+  // in the range matches, with no table load
+  const bool full = unique && p.stats[2] == (unsigned long long)L.drange;
+  // the lean write pass recomputes a direct table's slot from the key, so
+  // this pass writes no slots for it
+  const bool keep_slots = !(p.lean && p.out_brow == nullptr && unique);
   const int woff = warp * (32 * IT) + lane;
   auto load_chunk_keys = [&](int64_t c, long long* raw) {
     const int64_t cbase = c * kChunk;
@@ -327,14 +333,15 @@ __global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
       const int off = woff + k * 32;
       const bool valid = off < left && !(NULLABLE && raw_is_null(p.pkey, raw[k], cbase + off));
       d[k] = (unsigned long long)raw[k] - (unsigned long long)L.dmin;
-      cnt[k] = (valid && d[k] < (unsigned long long)L.drange) ? p.meta[d[k]].y : 0;
+      const bool inr = valid && d[k] < (unsigned long long)L.drange;
+      cnt[k] = inr ? (full ? 1 : p.meta[d[k]].y) : 0;
     }
     uint64_t m_sum = 0;
 #pragma unroll
     for (int k = 0; k < IT; k++) {
       const int off = woff + k * 32;
       if (off < left) {
-        p.slot_of_row[cbase + off] = cnt[k] > 0 ? (int32_t)d[k] : -1;
+        if (keep_slots) p.slot_of_row[cbase + off] = cnt[k] > 0 ? (int32_t)d[k] : -1;
         m_sum += (uint64_t)out_rows_of(p.join_type, unique ? (cnt[k] > 0 ? 1 : 0) : cnt[k]);
       }
     }
@@ -636,20 +643,44 @@ __global__ void __launch_bounds__(TH) join_write_lean_kernel(ProbeParams p) {
   if (!(p.lean && p.out_brow == nullptr && p.stats[1] <= 1)) return;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  int32_t next_s[IT];
+  // a direct table: the slot is the key's offset from the minimum, read from
+  // the key itself (the count pass wrote no slots); a full one (every key of
+  // the range present) needs no check of the slot
+  const JoinLayout L = join_layout(p.stats, p.build_rows, p.slots);
+  const bool from_keys = L.direct;
+  const bool full = from_keys && p.stats[2] == (unsigned long long)L.drange;
+  const bool kint = p.pkey.type == GHB_INT;
+  const bool knull = p.pkey.null_mode != GHB_NULLS_NONE;
+  // a row's next input: its probe key (direct table) or its slot (hashed)
+  auto fetch = [&](int64_t row) -> long long {
+    if (row >= p.n) return 0;
+    if (!from_keys) return (long long)__ldcs(p.slot_of_row + row);
+    return kint ? (long long)__ldcs((const int*)p.pkey.data + row) : __ldcs((const long long*)p.pkey.data + row);
+  };
+  long long next_r[IT];
 #pragma unroll
-  for (int k = 0; k < IT; k++) {
-    const int64_t row = (int64_t)blockIdx.x * kChunk + (int64_t)warp * (32 * IT) + k * 32 + lane;
-    next_s[k] = row < p.n ? __ldcs(p.slot_of_row + row) : -1;
-  }
+  for (int k = 0; k < IT; k++)
+    next_r[k] = fetch((int64_t)blockIdx.x * kChunk + (int64_t)warp * (32 * IT) + k * 32 + lane);
   for (int64_t c = blockIdx.x; c < p.nchunks; c += gridDim.x) {
     const int64_t wbase = c * kChunk + (int64_t)warp * (32 * IT);
     int32_t s[IT];
 #pragma unroll
     for (int k = 0; k < IT; k++) {
-      s[k] = next_s[k];
-      const int64_t nrow = wbase + (int64_t)gridDim.x * kChunk + k * 32 + lane;
-      next_s[k] = nrow < p.n ? __ldcs(p.slot_of_row + nrow) : -1;
+      const int64_t row = wbase + k * 32 + lane;
+      const long long r = next_r[k];
+      next_r[k] = fetch(wbase + (int64_t)gridDim.x * kChunk + k * 32 + lane);
+      if (!from_keys) {
+        s[k] = row < p.n ? (int32_t)r : -1;
+      } else {
+        const unsigned long long d = (unsigned long long)r - (unsigned long long)L.dmin;
+        const bool hit = row < p.n && d < (unsigned long long)L.drange && !(knull && raw_is_null(p.pkey, r, row));
+        s[k] = hit ? (int32_t)d : -1;
+      }
+    }
+    if (from_keys && !full) {
+#pragma unroll
+      for (int k = 0; k < IT; k++)
+        if (s[k] >= 0 && p.meta[s[k]].y == 0) s[k] = -1;   // a hole of the key range
     }
     ulonglong2 w[IT];
 #pragma unroll

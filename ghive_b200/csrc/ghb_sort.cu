@@ -18,7 +18,8 @@
 //                segment's passes at once; passes whose digit is constant are
 //                skipped;
 //   4. passes    onesweep-style: each CTA claims a tile, ranks its keys by
-//                digit with warp ballots (stable), gets each digit's global
+//                digit within each warp (stable: a lane's peers of an item
+//                from one shared atomicOr per lane), gets each digit's global
 //                offset by decoupled look-back over earlier tiles, reorders
 //                the tile in shared memory and writes one run per digit.
 // A one-segment key (the common case, e.g. (int32 d, int64 k) with the ranges
@@ -341,6 +342,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
   __shared__ uint32_t s_bexcl[kBins];                      // block-local exclusive offset per digit
   __shared__ uint64_t s_gbase[kBins];                      // global destination of each digit's run
   __shared__ uint32_t s_wsum[kSortThreads / 32];
+  __shared__ uint32_t s_match[kSortThreads / 32][kBins];   // lanes of each digit, per warp
   __shared__ int64_t s_tile;
   extern __shared__ uint64_t s_dyn[];                      // reordered tile: keys, then values
   uint64_t* s_keys = s_dyn;
@@ -360,7 +362,10 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
       if (*(volatile int32_t*)p.dev_status == kDevTimeout) t = p.ntiles;
       s_tile = t;
     }
-    for (int i = threadIdx.x; i < (kSortThreads / 32) * kBins; i += kSortThreads) (&s_whist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < (kSortThreads / 32) * kBins; i += kSortThreads) {
+      (&s_whist[0][0])[i] = 0;
+      (&s_match[0][0])[i] = 0;
+    }
     __syncthreads();
     const int64_t tile = s_tile;
     if (tile >= p.ntiles) break;
@@ -412,12 +417,15 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
       int64_t row = wbase + k * 32 + lane;
       bool live = row < p.n;
       uint32_t d = (uint32_t)(key[k] >> p.shift) & (kBins - 1);
-      unsigned peers = __ballot_sync(0xffffffffu, live);
-#pragma unroll
-      for (int b = 0; b < kDigitBits; b++) {
-        unsigned bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-        peers &= ((d >> b) & 1u) ? bb : ~bb;
-      }
+      // the warp's lanes holding digit d: each lane sets its bit in the
+      // digit's word (one shared atomic, no per-bit ballots), reads the word
+      // back, and the lowest of them clears it for the next item
+      unsigned peers = 0;
+      if (live) atomicOr(&s_match[warp][d], 1u << lane);
+      __syncwarp();
+      if (live) peers = s_match[warp][d];
+      __syncwarp();
+      if (live && (peers & lt) == 0) s_match[warp][d] = 0;
       uint32_t before = live ? s_whist[warp][d] : 0;
       __syncwarp();
       if (live && (peers & lt) == 0) s_whist[warp][d] = before + __popc(peers);

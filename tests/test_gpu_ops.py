@@ -824,3 +824,41 @@ def test_groupby_ghive_golden_string_keys(ctx):
         assert rows == sorted(tuple(r) for r in case["expected_rows"]), case["test"]
         ran += 1
     assert ran == 2
+
+
+@pytest.mark.parametrize("full", [True, False])
+@pytest.mark.parametrize("key_int", [False, True])
+def test_join_lean_pass_on_direct_tables(ctx, full, key_int):
+    """The lean write pass (INNER, unique build keys, inline payloads, no
+    build row ids) on a direct table reads each probe key again instead of a
+    slot array: with every key of the range present (a full table, no table
+    load in the count pass) and with holes in the range; NULL probe keys and
+    keys outside the range match nothing."""
+    import torch
+    from ghive_b200.ops import _Outs
+    g = np.random.default_rng(97 + 2 * full + key_int)
+    nb, m = 40_000, 700_000
+    dt = np.int32 if key_int else np.int64
+    if full:
+        bkey = g.permutation(np.arange(-500, nb - 500)).astype(dt)
+    else:
+        bkey = g.choice(np.arange(-500, int(1.3 * nb) - 500), nb, replace=False).astype(dt)
+    pay = [g.integers(0, 1 << 40, nb, dtype=np.int64), g.random(nb)]
+    pkey = g.integers(-2000, int(1.4 * nb), m).astype(dt)
+    pnull = g.random(m) < 0.03
+    pr, br = oracle.hash_join(bkey, (pkey, pnull))
+    t = ctx.join_build(dev(bkey), build_payload=[dev(c) for c in pay])
+    ob = _Outs([abi.LONG, abi.DOUBLE], m, "cuda:0", with_nulls=False)
+    op = _Outs([], m, "cuda:0")
+    prow = torch.empty(m, dtype=torch.int32, device="cuda:0")
+    d_rows = torch.zeros(1, dtype=torch.int64, device="cuda:0")
+    ctx.join_probe(t, (dev(pkey), dev(pnull.astype(np.uint8))), abi.INNER_JOIN, capacity=m, rowids=False,
+                   outs=(ob, op, prow, None, d_rows))
+    k = int(d_rows.item())
+    assert k == len(pr)
+    assert np.array_equal(host(prow[:k]), pr)
+    assert np.array_equal(host(ob.cols[0][0][:k]), pay[0][br])
+    assert np.array_equal(host(ob.cols[1][0][:k]).view(np.uint64), pay[1][br].view(np.uint64))
+    _, _, slots = t.info()
+    assert slots == int(bkey.max()) - int(bkey.min()) + 1   # a direct table
+    t.free()
