@@ -819,6 +819,144 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
   return run_passes<uint32_t>(ctx, pp, segs, run, hist, kb, vb, packed, stream);
 }
 
+// ---------------------------------------------------------------- STRING keys
+// A STRING sort key compares as Hive's StringExpr.compare (storage-api/src/
+// java/org/apache/hadoop/hive/ql/exec/vector/expressions/StringExpr.java:
+// 37-47): unsigned bytes, then length.  It is sorted as the tuple
+// (chunk 0, ..., chunk m-1, length) of fixed-width keys, chunk i being bytes
+// [8i, 8i + 8) big-endian with 0x00 past the end (top bit flipped, so the
+// signed order of the int64 is the unsigned order of the bytes): equal
+// chunks with a shorter length sort first, as the byte compare does.  A NULL
+// string is NULL in every part.
+__global__ void __launch_bounds__(256) string_maxlen_kernel(ghb_column c, unsigned long long* out) {
+  const int2* aux = (const int2*)c.aux;
+  unsigned long long mx = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < c.n; r += (int64_t)gridDim.x * blockDim.x) {
+    const int2 ix = aux[r];
+    if (ix.x >= 0) mx = max(mx, (unsigned long long)(ix.y - ix.x));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx) atomicMax(out, mx);
+}
+
+__global__ void __launch_bounds__(256) string_parts_kernel(ghb_column c, int32_t nchunks, int64_t* chunks,
+                                                            int32_t* lens, uint8_t* nulls) {
+  const int2* aux = (const int2*)c.aux;
+  const uint8_t* bytes = (const uint8_t*)c.data;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < c.n; r += (int64_t)gridDim.x * blockDim.x) {
+    const int2 ix = aux[r];
+    const bool null = ix.x < 0;
+    const int len = null ? 0 : ix.y - ix.x;
+    nulls[r] = null ? 1 : 0;
+    lens[r] = len;
+    for (int k = 0; k < nchunks; k++) {
+      uint64_t w = 0;
+      for (int b = 0; b < 8; b++) {
+        const int at = 8 * k + b;
+        w = (w << 8) | (at < len ? (uint64_t)bytes[ix.x + at] : 0ull);
+      }
+      chunks[(int64_t)k * c.n + r] = (int64_t)(w ^ 0x8000000000000000ull);
+    }
+  }
+}
+
+// out[i] = the [start,end) of row rowid[i] of a STRING column (NULL: -1, -1).
+__global__ void __launch_bounds__(256) string_gather_kernel(ghb_column c, const int32_t* rowid, int64_t n,
+                                                             ghb_out_column out) {
+  const int2* aux = (const int2*)c.aux;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int2 ix = aux[rowid[i]];
+    ((int2*)out.data)[i] = ix;
+    if (out.is_null) out.is_null[i] = ix.x < 0 ? 1 : 0;
+  }
+}
+
+// ORDER BY with STRING keys: each STRING key becomes its parts; the sort
+// runs on the parts with the row ids carried; the STRING outputs are
+// gathered from the row ids.
+static int32_t sort_with_strings(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
+                                 const int32_t* null_orders, int32_t nkeys, const ghb_column* payload,
+                                 int32_t npayload, ghb_out_column* out_keys, ghb_out_column* out_payload,
+                                 int32_t* out_rowid, const ghb_sort_cfg* cfg, cudaStream_t stream) {
+  int64_t n = 0;
+  int32_t st = validate_columns(ctx, keys, nkeys, &n, true);
+  if (st) return st;
+  if (n >= (int64_t)INT32_MAX) return set_error(ctx, GHB_ERR_UNSUPPORTED, "sort of 2^31 rows or more");
+  if (!out_keys) return set_error(ctx, GHB_ERR_INVALID, "out_keys is NULL");
+  // the longest string of each STRING key (one read, one synchronisation)
+  unsigned long long* d_len = nullptr;
+  if ((st = scratch_alloc(ctx, 8 * kMaxSortKeys, (void**)&d_len, stream))) return st;
+  GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_len, 0, 8 * kMaxSortKeys, stream));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+  for (int j = 0; j < nkeys; j++)
+    if (keys[j].type == GHB_STRING) {
+      string_maxlen_kernel<<<grid, 256, 0, stream>>>(keys[j], d_len + j);
+      GHB_LAUNCH_CHECK(ctx);
+    }
+  unsigned long long len[kMaxSortKeys];
+  GHB_CUDA_TRY(ctx, cudaMemcpyAsync(len, d_len, sizeof(len), cudaMemcpyDeviceToHost, stream));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(stream));
+  std::vector<ghb_column> ek;
+  std::vector<int32_t> eo, en;
+  std::vector<ghb_out_column> eout;
+  for (int j = 0; j < nkeys; j++) {
+    const int32_t o = orders ? orders[j] : GHB_ASC, no = null_orders ? null_orders[j] : GHB_NULLS_DEFAULT;
+    if (keys[j].type != GHB_STRING) {
+      ek.push_back(keys[j]);
+      eo.push_back(o);
+      en.push_back(no);
+      eout.push_back(out_keys[j]);
+      continue;
+    }
+    const int m = (int)((len[j] + 7) / 8);
+    if ((int)ek.size() + m + 1 > kMaxSortKeys)
+      return set_error(ctx, GHB_ERR_UNSUPPORTED, "STRING sort key %d of up to %llu bytes needs more than %d key "
+                       "parts in all", j, len[j], kMaxSortKeys);
+    int64_t* chunks = nullptr;
+    int32_t* lens = nullptr;
+    uint8_t* nulls = nullptr;
+    if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 8 * std::max(m, 1), (void**)&chunks, stream)) ||
+        (st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 4, (void**)&lens, stream)) ||
+        (st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1), (void**)&nulls, stream)))
+      return st;
+    string_parts_kernel<<<grid, 256, 0, stream>>>(keys[j], m, chunks, lens, nulls);
+    GHB_LAUNCH_CHECK(ctx);
+    for (int k = 0; k <= m; k++) {
+      ghb_column pc{k < m ? GHB_LONG : GHB_INT, GHB_NULLS_BYTEMAP, k < m ? (const void*)(chunks + (int64_t)k * n)
+                                                                         : (const void*)lens,
+                    nulls, nullptr, n};
+      ek.push_back(pc);
+      eo.push_back(o);
+      en.push_back(no);
+      // the parts' sorted values are not kept
+      void* od = nullptr;
+      if ((st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * type_width(pc.type), &od, stream))) return st;
+      eout.push_back(ghb_out_column{pc.type, 0, od, nullptr});
+    }
+  }
+  int32_t* rowid = out_rowid;
+  if (!rowid && (st = scratch_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * 4, (void**)&rowid, stream))) return st;
+  st = sort_impl(ctx, ek.data(), eo.data(), en.data(), (int32_t)ek.size(), payload, npayload, eout.data(),
+                 out_payload, rowid, cfg, stream);
+  if (st) return st;
+  for (int j = 0; j < nkeys; j++)
+    if (keys[j].type == GHB_STRING) {
+      if (out_keys[j].type != GHB_STRING || (!out_keys[j].data && n > 0))
+        return set_error(ctx, GHB_ERR_INVALID, "out_keys[%d]: bad type or data", j);
+      string_gather_kernel<<<grid, 256, 0, stream>>>(keys[j], rowid, n, out_keys[j]);
+      GHB_LAUNCH_CHECK(ctx);
+    }
+  return GHB_OK;
+}
+
+// Scratch a sort with STRING keys needs beside the sort's own.
+static size_t string_sort_scratch_bytes(const ghb_column* keys, int32_t nkeys, int64_t n) {
+  size_t b = 4096 + (size_t)n * 4 + 256;
+  for (int j = 0; j < nkeys; j++)
+    if (keys[j].type == GHB_STRING) b += (size_t)n * (2 * 8 * kMaxSortKeys + 4 + 4 + 1) + 8 * 1024;
+  return b;
+}
+
 }  // namespace ghb
 
 using namespace ghb;
@@ -830,8 +968,14 @@ extern "C" int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t*
   if (!ctx) return GHB_ERR_INVALID;
   scratch_reset(ctx);
   int64_t n = keys && nkeys > 0 ? keys[0].n : 0;
-  int32_t st = scratch_reserve(ctx, sort_scratch_bytes(n), (cudaStream_t)stream);
+  bool strings = false;
+  for (int j = 0; keys && j < nkeys && j < kMaxSortKeys; j++) strings |= keys[j].type == GHB_STRING;
+  const size_t extra = strings ? string_sort_scratch_bytes(keys, nkeys, n) : 0;
+  int32_t st = scratch_reserve(ctx, sort_scratch_bytes(n) + extra, (cudaStream_t)stream);
   if (st) return st;
+  if (strings)
+    return sort_with_strings(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys, out_payload,
+                             out_rowid, cfg, (cudaStream_t)stream);
   return sort_impl(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys, out_payload,
                    out_rowid, cfg, (cudaStream_t)stream);
 }

@@ -315,7 +315,11 @@ int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table,
  * 921-960: signed integers and IEEE doubles in numeric order, per-key ASC/DESC
  * and NULLS FIRST/LAST).  Writes the sorted key columns to out_keys and the
  * payload columns, permuted the same way, to out_payload; out_rowid (nullable,
- * int32) receives the permutation.  Ties keep input order. */
+ * int32) receives the permutation.  Ties keep input order.  A STRING key
+ * sorts by unsigned bytes, then length (StringExpr.java:37-47), as the
+ * tuple of its 8-byte parts and its length (one read finds the longest
+ * string; at most 8 key parts in all); its output is [start,end) pairs into
+ * the key column's bytes.  Payloads are fixed-width. */
 int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
                  const int32_t* null_orders, int32_t nkeys,
                  const ghb_column* payload, int32_t npayload,

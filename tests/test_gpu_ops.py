@@ -862,3 +862,26 @@ def test_join_lean_pass_on_direct_tables(ctx, full, key_int):
     _, _, slots = t.info()
     assert slots == int(bkey.max()) - int(bkey.min()) + 1   # a direct table
     t.free()
+
+
+def test_sort_string_keys(ctx):
+    """ORDER BY a STRING key (Hive's unsigned byte order, then length; NULLs
+    first for ASC) and a STRING key behind an INT key, ASC and DESC: the sort
+    runs on each string's 8-byte parts and length, and the STRING outputs are
+    [start,end) pairs gathered by row id."""
+    g = np.random.default_rng(98)
+    n = 90_000
+    pool = ["", "a", "a\x00", "ab", "abc", "abcdefgh", "abcdefghi", "abcdefgh\x01", "MFGR#1221",
+            "MFGR#12", "zz", "été", "Z", "b" * 23]
+    words = [None if g.random() < 0.07 else pool[g.integers(0, len(pool))] for _ in range(n)]
+    s = _strings(words)
+    yr = g.integers(1992, 1995, n, dtype=np.int32)
+    rid = np.arange(n, dtype=np.int32)
+    ds = _dev_strings(s)
+    for keys, hkeys, orders in (([ds], [s], [abi.ASC]), ([ds], [s], [abi.DESC]),
+                                ([dev(yr), ds], [yr, s], [abi.DESC, abi.ASC])):
+        perm = oracle.sort_perm(hkeys, orders)
+        ok, op, _ = ctx.sort(keys, orders, payload=[dev(rid)])
+        assert np.array_equal(host(op[0][0]), perm), orders
+        got = _decode(s, host(ok[-1][0]))
+        assert got == [words[i] for i in perm]
