@@ -566,7 +566,8 @@ def bench_sort(ctx, args, dev, stream, peak, peak_kind):
                  "roofline_per_pass_formula": roofline(
                      per_pass_bytes, ms, peak, peak_kind,
                      kernel="whole sort against N*12 + P*N*24 + N*16 bytes, P = %d executed "
-                            "radix passes" % passes),
+                            "radix passes" % passes,
+                     traffic=profile_traffic("sort_passes_20M.md")),
                  "e2e": {"value": N_SORT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                          "h2d_bytes_per_step": N_SORT * 16, "d2h_bytes_per_step": N_SORT * 16,
                          "api": "ghb_sort_host (pinned host columns)"}}

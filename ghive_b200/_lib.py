@@ -23,6 +23,7 @@ _PROTOS = {
     "ghb_sync": (I32, [P, P]),
     "ghb_kernel_launches": (I64, [P]),
     "ghb_ctx_set_spin_limit": (I32, [P, I32]),
+    "ghb_ctx_set_log": (I32, [P, C.c_char_p, I32, C.c_double]),
     "ghb_filter": (I32, [P, P, P, I32, P, I32, P, I64, P, P]),
     "ghb_filter_groupby": (I32, [P, P, P, I32, P, I32, P, I32, P, I64, P, P, P]),
     "ghb_join_build": (I32, [P, P, P, I32, P, C.POINTER(C.c_void_p), P]),

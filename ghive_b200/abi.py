@@ -140,7 +140,8 @@ class PlanResult(C.Structure):
                 ("data", C.c_void_p * MAX_RESULT_COLS), ("is_null", C.c_void_p * MAX_RESULT_COLS),
                 ("sequence", C.c_int32 * MAX_RESULT_COLS), ("rows", C.c_int64),
                 ("n_long", C.c_int32), ("n_double", C.c_int32), ("n_int", C.c_int32),
-                ("n_string", C.c_int32)]
+                ("n_string", C.c_int32), ("str_bytes", C.c_void_p * MAX_RESULT_COLS),
+                ("str_nbytes", C.c_int64 * MAX_RESULT_COLS)]
 
 
 class BatchCfg(C.Structure):

@@ -5,6 +5,7 @@
 // with an explicit context per caller, and its stdout-and-nullptr error
 // convention (gpu_impl/src/ghive_JNIInterface.cu:111-118) with status codes.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -284,6 +285,15 @@ int32_t ghb_ctx_create(int32_t device, int64_t arena_bytes, ghb_ctx** out) {
     ghb_ctx_destroy(ctx);
     return GHB_ERR_CUDA;
   }
+  // the per-call log named by the environment, if any
+  if (const char* path = std::getenv("GHB_LOG")) {
+    const char* lv = std::getenv("GHB_LOG_LEVEL");
+    const char* pk = std::getenv("GHB_LOG_PEAK_GBS");
+    if (*path && ghb_ctx_set_log(ctx, path, lv ? std::atoi(lv) : 1, pk ? std::atof(pk) : 0) != GHB_OK) {
+      ghb_ctx_destroy(ctx);
+      return GHB_ERR_INVALID;
+    }
+  }
   *out = ctx;
   return GHB_OK;
 }
@@ -302,7 +312,28 @@ int32_t ghb_ctx_destroy(ghb_ctx* ctx) {
   for (auto& row : ctx->hev)
     for (cudaEvent_t& e : row)
       if (e) cudaEventDestroy(e);
+  ghb_ctx_set_log(ctx, nullptr, 0, 0);
   delete ctx;
+  return GHB_OK;
+}
+
+int32_t ghb_ctx_set_log(ghb_ctx* ctx, const char* path, int32_t level, double peak_gbs) {
+  if (!ctx) return GHB_ERR_INVALID;
+  if (ctx->log) std::fclose(ctx->log);
+  ctx->log = nullptr;
+  ctx->log_level = 0;
+  for (cudaEvent_t& e : ctx->log_ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
+  if (!path || level <= 0) return GHB_OK;
+  ctx->log = std::fopen(path, "a");
+  if (!ctx->log) return set_error(ctx, GHB_ERR_INVALID, "cannot open the log file %s", path);
+  ctx->log_level = level;
+  ctx->log_peak_gbs = peak_gbs > 0 ? peak_gbs : 0;
+  if (level >= 2)
+    for (cudaEvent_t& e : ctx->log_ev) GHB_CUDA_TRY(ctx, cudaEventCreate(&e));
   return GHB_OK;
 }
 

@@ -65,6 +65,13 @@ struct ghb_ctx {
   // Pool for those stream-ordered allocations (nullptr = the device's
   // default pool).
   cudaMemPool_t pool = nullptr;
+
+  // per-call JSON log (ghb_ctx_set_log): the file, its level, the peak the
+  // roofline fraction divides by (0: none), and level 2's events
+  FILE* log = nullptr;
+  int32_t log_level = 0;
+  double log_peak_gbs = 0;
+  cudaEvent_t log_ev[2] = {nullptr, nullptr};
 };
 
 namespace ghb {

@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "ghb_ctx.hpp"
+#include "ghb_log.hpp"
 
 namespace ghb {
 
@@ -182,7 +183,10 @@ extern "C" int32_t ghb_filter(ghb_ctx* ctx, const ghb_predicate* pred, const ghb
                               int32_t ncols, const int32_t* proj, int32_t nproj, ghb_out_column* out,
                               int64_t out_capacity, int64_t* d_out_rows, void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
+  CallScope cs(ctx, "filter", (cudaStream_t)stream);
+  cs.rows(ncols > 0 && cols ? cols[0].n : 0);
+  cs.bytes(cols_bytes(cols, ncols));
   scratch_reset(ctx);
-  return filter_impl(ctx, pred, cols, ncols, proj, nproj, out, out_capacity, d_out_rows,
-                     (cudaStream_t)stream);
+  return cs.done(filter_impl(ctx, pred, cols, ncols, proj, nproj, out, out_capacity, d_out_rows,
+                             (cudaStream_t)stream));
 }

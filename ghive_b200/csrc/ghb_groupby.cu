@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include "ghb_groupby.cuh"
+#include "ghb_log.hpp"
 
 namespace ghb {
 
@@ -548,7 +549,10 @@ extern "C" int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred, c
                                       int64_t out_capacity, int64_t* d_out_groups,
                                       const ghb_groupby_cfg* cfg, void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
+  CallScope cs(ctx, "filter_groupby", (cudaStream_t)stream);
+  cs.rows(ncols > 0 && cols ? cols[0].n : 0);
+  cs.bytes(cols_bytes(cols, ncols));
   scratch_reset(ctx);
-  return filter_groupby_impl(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, out_capacity,
-                             d_out_groups, cfg, (cudaStream_t)stream, nullptr, 0);
+  return cs.done(filter_groupby_impl(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out, out_capacity,
+                                     d_out_groups, cfg, (cudaStream_t)stream, nullptr, 0));
 }

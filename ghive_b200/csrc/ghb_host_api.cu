@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "ghb_ctx.hpp"
+#include "ghb_log.hpp"
 
 namespace ghb {
 
@@ -116,7 +117,7 @@ using namespace ghb;
 
 extern "C" {
 
-int32_t ghb_filter_host(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
+static int32_t ghb_filter_host_body(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
                         int32_t ncols, const int32_t* proj, int32_t nproj, ghb_out_column* out,
                         int64_t out_capacity, int64_t* out_rows) {
   if (!ctx || !out_rows) return GHB_ERR_INVALID;
@@ -149,7 +150,16 @@ int32_t ghb_filter_host(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_colum
   return GHB_OK;
 }
 
-int32_t ghb_filter_groupby_host(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
+int32_t ghb_filter_host(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,
+                        const int32_t* proj, int32_t nproj, ghb_out_column* out, int64_t out_capacity,
+                        int64_t* out_rows) {
+  CallScope cs(ctx, "filter_host", 0, true);
+  cs.rows(ncols > 0 && cols ? cols[0].n : 0);
+  cs.bytes(cols_bytes(cols, ncols));
+  return cs.done(ghb_filter_host_body(ctx, pred, cols, ncols, proj, nproj, out, out_capacity, out_rows));
+}
+
+static int32_t ghb_filter_groupby_host_body(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols,
                                 int32_t ncols, const int32_t* key_cols, int32_t nkeys,
                                 const ghb_agg_desc* aggs, int32_t naggs, ghb_out_column* out,
                                 int64_t out_capacity, int64_t* out_groups,
@@ -186,14 +196,26 @@ int32_t ghb_filter_groupby_host(ghb_ctx* ctx, const ghb_predicate* pred, const g
   return GHB_OK;
 }
 
-int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* probe_key,
+int32_t ghb_filter_groupby_host(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,
+                                const int32_t* key_cols, int32_t nkeys, const ghb_agg_desc* aggs, int32_t naggs,
+                                ghb_out_column* out, int64_t out_capacity, int64_t* out_groups,
+                                const ghb_groupby_cfg* cfg) {
+  CallScope cs(ctx, "filter_groupby_host", 0, true);
+  cs.rows(ncols > 0 && cols ? cols[0].n : 0);
+  cs.bytes(cols_bytes(cols, ncols));
+  return cs.done(ghb_filter_groupby_host_body(ctx, pred, cols, ncols, key_cols, nkeys, aggs, naggs, out,
+                                              out_capacity, out_groups, cfg));
+}
+
+static int32_t ghb_hash_join_host_body(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* probe_key,
                            int32_t join_type, const ghb_column* build_payload, int32_t nbp,
                            ghb_out_column* out_build, const ghb_column* probe_payload, int32_t npp,
                            ghb_out_column* out_probe, int32_t* out_probe_rowid,
                            int32_t* out_build_rowid, int64_t out_capacity, int64_t* out_rows,
                            const ghb_join_cfg* cfg) {
   if (!ctx || !out_rows || !build_key || !probe_key) return GHB_ERR_INVALID;
-  if (nbp < 0 || nbp > 8 || npp < 0 || npp > 8) return set_error(ctx, GHB_ERR_INVALID, "payload counts");
+  if (nbp < 0 || nbp > GHB_MAX_JOIN_PAYLOAD || npp < 0 || npp > GHB_MAX_JOIN_PAYLOAD)
+    return set_error(ctx, GHB_ERR_INVALID, "payload counts");
   if ((nbp > 0 && (!build_payload || !out_build)) || (npp > 0 && (!probe_payload || !out_probe)))
     return set_error(ctx, GHB_ERR_INVALID, "payload columns or their outputs are NULL");
   if (out_capacity < 0) return set_error(ctx, GHB_ERR_INVALID, "negative out_capacity");
@@ -425,7 +447,21 @@ int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_
   return GHB_OK;
 }
 
-int32_t ghb_sort_host(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
+int32_t ghb_hash_join_host(ghb_ctx* ctx, const ghb_column* build_key, const ghb_column* probe_key,
+                           int32_t join_type, const ghb_column* build_payload, int32_t nbp, ghb_out_column* out_build,
+                           const ghb_column* probe_payload, int32_t npp, ghb_out_column* out_probe,
+                           int32_t* out_probe_rowid, int32_t* out_build_rowid, int64_t out_capacity,
+                           int64_t* out_rows, const ghb_join_cfg* cfg) {
+  CallScope cs(ctx, "hash_join_host", 0, true);
+  cs.rows(probe_key ? probe_key->n : 0);
+  cs.bytes(cols_bytes(build_key, build_key ? 1 : 0) + cols_bytes(probe_key, probe_key ? 1 : 0) +
+           cols_bytes(build_payload, nbp) + cols_bytes(probe_payload, npp));
+  return cs.done(ghb_hash_join_host_body(ctx, build_key, probe_key, join_type, build_payload, nbp, out_build,
+                                         probe_payload, npp, out_probe, out_probe_rowid, out_build_rowid,
+                                         out_capacity, out_rows, cfg));
+}
+
+static int32_t ghb_sort_host_body(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
                       const int32_t* null_orders, int32_t nkeys, const ghb_column* payload,
                       int32_t npayload, ghb_out_column* out_keys, ghb_out_column* out_payload,
                       int32_t* out_rowid, const ghb_sort_cfg* cfg) {
@@ -461,6 +497,16 @@ int32_t ghb_sort_host(ghb_ctx* ctx, const ghb_column* keys, const int32_t* order
     GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out_rowid, d_rowid, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
   GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s));
   return GHB_OK;
+}
+
+int32_t ghb_sort_host(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders, const int32_t* null_orders,
+                      int32_t nkeys, const ghb_column* payload, int32_t npayload, ghb_out_column* out_keys,
+                      ghb_out_column* out_payload, int32_t* out_rowid, const ghb_sort_cfg* cfg) {
+  CallScope cs(ctx, "sort_host", 0, true);
+  cs.rows(keys && nkeys > 0 ? keys[0].n : 0);
+  cs.bytes(cols_bytes(keys, nkeys) + cols_bytes(payload, npayload));
+  return cs.done(ghb_sort_host_body(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys,
+                                    out_payload, out_rowid, cfg));
 }
 
 }  // extern "C"

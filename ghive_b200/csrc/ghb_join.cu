@@ -46,6 +46,7 @@
 #include <mutex>
 
 #include "ghb_ctx.hpp"
+#include "ghb_log.hpp"
 
 namespace ghb {
 
@@ -61,7 +62,7 @@ namespace ghb {
 constexpr int kJThreads = 256;
 constexpr int kJItems = 4;
 constexpr int kChunk = kJThreads * kJItems;   // probe rows per chunk
-constexpr int kMaxPay = 8;
+constexpr int kMaxPay = GHB_MAX_JOIN_PAYLOAD;
 constexpr int kInline = 2;
 
 // Bucket of a key image: Fibonacci (multiplicative) hashing, the top bits of
@@ -1082,8 +1083,11 @@ int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key, const ghb_colu
                        int32_t n_build_payload, const ghb_join_cfg* cfg, ghb_join_table** out,
                        void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
-  return join_build_impl(ctx, build_key, build_payload, n_build_payload, cfg, out,
-                         (cudaStream_t)stream);
+  CallScope cs(ctx, "join_build", (cudaStream_t)stream);
+  cs.rows(build_key ? build_key->n : 0);
+  cs.bytes(cols_bytes(build_key, build_key ? 1 : 0) + cols_bytes(build_payload, n_build_payload));
+  return cs.done(join_build_impl(ctx, build_key, build_payload, n_build_payload, cfg, out,
+                                 (cudaStream_t)stream));
 }
 
 int32_t ghb_join_table_free(ghb_ctx* ctx, ghb_join_table* table) {
@@ -1133,13 +1137,16 @@ int32_t ghb_join_probe(ghb_ctx* ctx, const ghb_join_table* table, const ghb_colu
                        int32_t* out_build_rowid, int64_t out_capacity, int64_t* d_out_rows,
                        void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
-  scratch_reset(ctx);
+  CallScope cs(ctx, "join_probe", (cudaStream_t)stream);
   int64_t n = probe_key ? probe_key->n : 0;
+  cs.rows(n);
+  cs.bytes(cols_bytes(probe_key, probe_key ? 1 : 0) + cols_bytes(probe_payload, n_probe_payload));
+  scratch_reset(ctx);
   int32_t st = scratch_reserve(ctx, join_probe_scratch_bytes(n), (cudaStream_t)stream);
-  if (st) return st;
-  return join_probe_impl(ctx, table, probe_key, join_type, out_build, probe_payload, n_probe_payload,
-                         out_probe, out_probe_rowid, out_build_rowid, out_capacity, d_out_rows,
-                         (cudaStream_t)stream, 0);
+  if (st) return cs.done(st);
+  return cs.done(join_probe_impl(ctx, table, probe_key, join_type, out_build, probe_payload, n_probe_payload,
+                                 out_probe, out_probe_rowid, out_build_rowid, out_capacity, d_out_rows,
+                                 (cudaStream_t)stream, 0));
 }
 
 }  // extern "C"

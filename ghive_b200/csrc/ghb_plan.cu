@@ -28,19 +28,54 @@
 #include <vector>
 
 #include "ghb_ctx.hpp"
+#include "ghb_log.hpp"
 
 namespace ghb {
 namespace {
 
 size_t width_of(int32_t t) { return type_width(t); }
 
-// A device column the plan owns.
+// Columns of an input table or an intermediate the plan holds (each
+// operator checks the columns it touches against its own limit).
+constexpr int kPlanCols = 64;
+
+// A device column the plan owns.  A STRING column is its int32 [start,end)
+// pairs (start < 0: NULL) in `data` and the bytes they index in `bytes`,
+// which operators pass through unchanged: a filter, group-by, join or sort
+// moves pairs, never bytes, and the result gathers the bytes it references.
 struct DevCol {
   int32_t type = GHB_LONG;
   void* data = nullptr;
   uint8_t* is_null = nullptr;   // NULL map (nullptr: no NULLs, or sentinels)
   int32_t null_mode = GHB_NULLS_NONE;
+  const uint8_t* bytes = nullptr;
+  int64_t nbytes = 0;
 };
+
+// (start, end) + add for each non-NULL pair: the build side's pairs moved
+// behind the probe side's bytes in a joined dictionary.
+__global__ void __launch_bounds__(256) offset_pairs_kernel(const int2* in, int64_t n, int32_t add, int2* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int2 v = in[i];
+    if (v.x >= 0) {
+      v.x += add;
+      v.y += add;
+    }
+    out[i] = v;
+  }
+}
+
+// Copies each non-NULL row's bytes from src[from) to dst[to): the result's
+// strings packed one after the other.
+__global__ void __launch_bounds__(256) gather_string_bytes_kernel(const uint8_t* src, const int2* from,
+                                                                  const int2* to, int64_t n, uint8_t* dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int2 f = from[i];
+    if (f.x < 0) continue;
+    const int2 t = to[i];
+    for (int b = 0; b < f.y - f.x; b++) dst[t.x + b] = src[f.x + b];
+  }
+}
 
 struct DevTable {
   std::vector<DevCol> cols;
@@ -66,11 +101,19 @@ struct Plan {
     owned.push_back(*out);
     return GHB_OK;
   }
-  // an output column of `rows` rows with a NULL map
-  int32_t out_col(int32_t type, int64_t rows, DevCol* c, ghb_out_column* o) {
+  // an output column of `rows` rows with a NULL map; a STRING one is its
+  // pairs only (a NULL is a negative start) and takes `bytes` from its source
+  int32_t out_col(int32_t type, int64_t rows, DevCol* c, ghb_out_column* o, const DevCol* src = nullptr) {
     int32_t st;
     c->type = type;
     if ((st = alloc((size_t)std::max<int64_t>(rows, 1) * width_of(type), &c->data))) return st;
+    if (type == GHB_STRING) {
+      c->null_mode = GHB_NULLS_SENTINEL;
+      c->bytes = src ? src->bytes : nullptr;
+      c->nbytes = src ? src->nbytes : 0;
+      *o = ghb_out_column{type, 0, c->data, nullptr};
+      return GHB_OK;
+    }
     if ((st = alloc((size_t)std::max<int64_t>(rows, 1), (void**)&c->is_null))) return st;
     c->null_mode = GHB_NULLS_BYTEMAP;
     *o = ghb_out_column{type, 0, c->data, c->is_null};
@@ -83,8 +126,24 @@ struct Plan {
 };
 
 ghb_column desc(const DevCol& c, int64_t rows) {
+  if (c.type == GHB_STRING) return ghb_column{GHB_STRING, GHB_NULLS_SENTINEL, c.bytes, nullptr, c.data, rows};
   return ghb_column{c.type, c.null_mode, c.data, c.null_mode == GHB_NULLS_BYTEMAP ? c.is_null : nullptr,
                     nullptr, rows};
+}
+
+// A column as an operator's fixed-width payload: a STRING column travels as
+// its pairs, 8 bytes a row (a NULL string's pair is copied like any value).
+ghb_column payload_desc(const DevCol& c, int64_t rows) {
+  if (c.type == GHB_STRING) return ghb_column{GHB_LONG, GHB_NULLS_NONE, c.data, nullptr, nullptr, rows};
+  return desc(c, rows);
+}
+
+// The output slot of such a payload: a STRING column's pairs as LONG words
+// with no NULL map, so an outer join's miss writes the LONG sentinel, whose
+// low word -1 is a NULL pair.
+ghb_out_column payload_out(const ghb_out_column& o) {
+  if (o.type == GHB_STRING) return ghb_out_column{GHB_LONG, 0, o.data, nullptr};
+  return o;
 }
 
 // Copies host table columns to the device (GHive's sentinels kept).
@@ -92,8 +151,31 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
   t->rows = rows;
   t->cols.assign(ncols, DevCol{});
   for (int c = 0; c < ncols; c++) {
-    if (h[c].type == GHB_STRING)
-      return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "column %d: STRING columns are not on the device path", c);
+    if (h[c].type == GHB_STRING) {
+      // the pairs, and the bytes up to the largest end a non-NULL row uses
+      DevCol& d = t->cols[c];
+      d.type = GHB_STRING;
+      d.null_mode = GHB_NULLS_SENTINEL;
+      const int2* pairs = (const int2*)h[c].aux;
+      if (rows > 0 && (!pairs || !h[c].data))
+        return set_error(P.ctx, GHB_ERR_INVALID, "column %d: STRING without its bytes or index", c);
+      int64_t nb = 0;
+      for (int64_t r = 0; r < rows; r++)
+        if (pairs[r].x >= 0) {
+          if (pairs[r].y < pairs[r].x)
+            return set_error(P.ctx, GHB_ERR_INVALID, "column %d row %lld: end before start", c, (long long)r);
+          nb = std::max<int64_t>(nb, pairs[r].y);
+        }
+      int32_t st = P.alloc((size_t)std::max<int64_t>(rows, 1) * 8, &d.data);
+      void* bytes = nullptr;
+      if (!st) st = P.alloc((size_t)std::max<int64_t>(nb, 1), &bytes);
+      if (st) return st;
+      d.bytes = (const uint8_t*)bytes;
+      d.nbytes = nb;
+      if (rows > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.data, pairs, rows * 8, cudaMemcpyHostToDevice, P.s));
+      if (nb > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(bytes, h[c].data, nb, cudaMemcpyHostToDevice, P.s));
+      continue;
+    }
     DevCol& d = t->cols[c];
     d.type = h[c].type;
     d.null_mode = h[c].null_mode;
@@ -124,15 +206,24 @@ int32_t run_filter(Plan& P, const ghb_plan_op& op, DevTable& t) {
     proj.assign(op.idx, op.idx + op.nidx);
   else
     for (int c = 0; c < (int)t.cols.size(); c++) proj.push_back(c);
-  if (proj.size() > (size_t)kMaxCols) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "projection of %zu columns", proj.size());
+  if (proj.size() > (size_t)kPlanCols) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "projection of %zu columns", proj.size());
   for (int32_t c : proj)
     if (c < 0 || c >= (int)t.cols.size()) return set_error(P.ctx, GHB_ERR_INVALID, "projection column %d", c);
+  if (!op.pred || op.pred->n_nodes == 0) {
+    // a projection alone (GHive's SelectOperator): the columns, no copy
+    DevTable o;
+    o.rows = t.rows;
+    for (int32_t c : proj) o.cols.push_back(t.cols[c]);
+    t = std::move(o);
+    return GHB_OK;
+  }
+  if (proj.size() > (size_t)kMaxCols) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "projection of %zu columns", proj.size());
   DevTable o;
   std::vector<ghb_out_column> out(proj.size());
   o.cols.resize(proj.size());
   int32_t st;
   for (size_t j = 0; j < proj.size(); j++)
-    if ((st = P.out_col(t.cols[proj[j]].type, t.rows, &o.cols[j], &out[j]))) return st;
+    if ((st = P.out_col(t.cols[proj[j]].type, t.rows, &o.cols[j], &out[j], &t.cols[proj[j]]))) return st;
   int64_t* d_rows = nullptr;
   if ((st = P.alloc(8, (void**)&d_rows))) return st;
   if ((st = ghb_filter(P.ctx, op.pred, in.data(), (int32_t)in.size(), proj.data(), (int32_t)proj.size(),
@@ -164,7 +255,7 @@ int32_t run_groupby(Plan& P, const ghb_plan_op& op, DevTable& t) {
   for (int j = 0; j < nkeys; j++) {
     if (op.idx[j] < 0 || op.idx[j] >= (int)t.cols.size())
       return set_error(P.ctx, GHB_ERR_INVALID, "group-by key column %d", op.idx[j]);
-    if ((st = P.out_col(t.cols[op.idx[j]].type, cap, &o.cols[j], &out[j]))) return st;
+    if ((st = P.out_col(t.cols[op.idx[j]].type, cap, &o.cols[j], &out[j], &t.cols[op.idx[j]]))) return st;
   }
   for (int a = 0; a < naggs; a++) {
     const int32_t c = op.aggs[a].col;
@@ -183,23 +274,72 @@ int32_t run_groupby(Plan& P, const ghb_plan_op& op, DevTable& t) {
   return GHB_OK;
 }
 
+// A STRING join key of both sides as LONG ids that are equal exactly when the
+// strings are: the two sides' pairs over one byte array (the build side's
+// bytes behind the probe side's), each row mapped to the row of its value's
+// first occurrence in that joined column (a device hash table of the
+// strings, bytes compared on a tag match); a NULL string gets the LONG
+// sentinel and so matches nothing.
+int32_t string_key_ids(Plan& P, const DevCol& pc, int64_t prows, const DevCol& bc, int64_t brows, DevCol* pid,
+                       DevCol* bid) {
+  const int64_t n = prows + brows;
+  if (pc.nbytes + bc.nbytes >= INT32_MAX)
+    return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "join: STRING keys of 2^31 bytes together");
+  void *bytes = nullptr, *pairs = nullptr, *rep = nullptr, *table = nullptr;
+  int64_t slots = 1024;
+  while (slots < 2 * n) slots <<= 1;
+  int32_t st = P.alloc((size_t)std::max<int64_t>(pc.nbytes + bc.nbytes, 1), &bytes);
+  if (!st) st = P.alloc((size_t)std::max<int64_t>(n, 1) * 8, &pairs);
+  if (!st) st = P.alloc((size_t)std::max<int64_t>(n, 1) * 8, &rep);
+  if (!st) st = P.alloc((size_t)slots * 8, &table);
+  if (st) return st;
+  if (pc.nbytes > 0)
+    GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(bytes, pc.bytes, pc.nbytes, cudaMemcpyDeviceToDevice, P.s));
+  if (bc.nbytes > 0)
+    GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync((uint8_t*)bytes + pc.nbytes, bc.bytes, bc.nbytes, cudaMemcpyDeviceToDevice, P.s));
+  if (prows > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(pairs, pc.data, prows * 8, cudaMemcpyDeviceToDevice, P.s));
+  if (brows > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((brows + 255) / 256, (int64_t)P.ctx->num_sms * 8));
+    offset_pairs_kernel<<<grid, 256, 0, P.s>>>((const int2*)bc.data, brows, (int32_t)pc.nbytes,
+                                               (int2*)pairs + prows);
+    GHB_LAUNCH_CHECK(P.ctx);
+  }
+  const ghb_column joined{GHB_STRING, GHB_NULLS_SENTINEL, bytes, nullptr, pairs, n};
+  if ((st = string_rep_rows(P.ctx, joined, nullptr, (int64_t*)rep, (unsigned long long*)table, slots, P.s)))
+    return st;
+  for (DevCol* d : {pid, bid}) {
+    d->type = GHB_LONG;
+    d->null_mode = GHB_NULLS_SENTINEL;
+    d->is_null = nullptr;
+  }
+  pid->data = rep;
+  bid->data = (int64_t*)rep + prows;
+  return GHB_OK;
+}
+
 // The current table probes a hash table built from input table op.build_table:
-// output = the current table's columns, then the kept build columns.
+// output = the current table's columns, then the kept build columns.  Keys
+// of several columns are packed into one; STRING key columns first become
+// ids shared by both sides (string_key_ids); STRING payloads travel as
+// their pairs into their own side's bytes.
 int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable& t) {
   // idx: the probe key columns, then as many build key columns
   if (!op.idx || op.nidx < 2 || op.nidx % 2 || op.nidx / 2 > kMaxPackKeys)
     return set_error(P.ctx, GHB_ERR_INVALID, "join: idx must hold k probe and k build key columns");
   const int nk = op.nidx / 2;
-  ghb_column hb[kMaxCols];
+  ghb_column hb[kPlanCols];
   int32_t nb = 0;
   int64_t brows = 0;
-  int32_t st = ghb_gtables_table(in, op.build_table, hb, kMaxCols, &nb, &brows);
+  int32_t st = ghb_gtables_table(in, op.build_table, hb, kPlanCols, &nb, &brows);
   if (st) return set_error(P.ctx, st, "join: build table %d is missing or malformed", op.build_table);
-  for (int j = 0; j < nk; j++)
+  for (int j = 0; j < nk; j++) {
     if (op.idx[j] < 0 || op.idx[j] >= (int)t.cols.size() || op.idx[nk + j] < 0 || op.idx[nk + j] >= nb)
       return set_error(P.ctx, GHB_ERR_INVALID, "join key columns %d / %d", op.idx[j], op.idx[nk + j]);
-  if ((int)t.cols.size() > 8 || op.nbuild_keep > 8 || op.nbuild_keep < 0)
-    return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "join: at most 8 columns from each side");
+    if ((t.cols[op.idx[j]].type == GHB_STRING) != (hb[op.idx[nk + j]].type == GHB_STRING))
+      return set_error(P.ctx, GHB_ERR_INVALID, "join key %d: a STRING column against a numeric one", j);
+  }
+  if ((int)t.cols.size() > GHB_MAX_JOIN_PAYLOAD || op.nbuild_keep > GHB_MAX_JOIN_PAYLOAD || op.nbuild_keep < 0)
+    return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "join: at most %d columns from each side", GHB_MAX_JOIN_PAYLOAD);
   // the build side's key and kept columns on the device
   std::vector<ghb_column> bsel;
   for (int j = 0; j < nk; j++) bsel.push_back(hb[op.idx[nk + j]]);
@@ -210,13 +350,22 @@ int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable
   }
   DevTable b;
   if ((st = upload(P, bsel.data(), (int32_t)bsel.size(), brows, &b))) return st;
-  std::vector<ghb_column> bd = descs(b);
-  std::vector<ghb_column> probe = descs(t);
-  ghb_column bkey = bd[0], pkey = probe[op.idx[0]];
+  // the key columns of both sides: STRING ones as shared ids
+  std::vector<DevCol> pkc(nk), bkc(nk);
+  for (int j = 0; j < nk; j++) {
+    pkc[j] = t.cols[op.idx[j]];
+    bkc[j] = b.cols[j];
+    if (pkc[j].type == GHB_STRING && (st = string_key_ids(P, pkc[j], t.rows, bkc[j], b.rows, &pkc[j], &bkc[j])))
+      return st;
+  }
+  ghb_column pkey = desc(pkc[0], t.rows), bkey = desc(bkc[0], b.rows);
   if (nk > 1) {
     // several key columns: both sides' tuples packed with one plan
-    std::vector<ghb_column> pk(nk);
-    for (int j = 0; j < nk; j++) pk[j] = probe[op.idx[j]];
+    std::vector<ghb_column> pk(nk), bk(nk);
+    for (int j = 0; j < nk; j++) {
+      pk[j] = desc(pkc[j], t.rows);
+      bk[j] = desc(bkc[j], b.rows);
+    }
     DevCol pp, bp;
     for (DevCol* c : {&pp, &bp}) {
       const int64_t rows = c == &pp ? t.rows : b.rows;
@@ -228,14 +377,16 @@ int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable
     }
     scratch_reset(P.ctx);
     if ((st = scratch_reserve(P.ctx, 4096, P.s))) return st;
-    if ((st = keypack_join(P.ctx, pk.data(), bd.data(), nk, (int64_t*)pp.data, pp.is_null, (int64_t*)bp.data,
+    if ((st = keypack_join(P.ctx, pk.data(), bk.data(), nk, (int64_t*)pp.data, pp.is_null, (int64_t*)bp.data,
                            bp.is_null, P.s)))
       return st;
     pkey = desc(pp, t.rows);
     bkey = desc(bp, b.rows);
   }
+  std::vector<ghb_column> bpay;
+  for (int j = 0; j < op.nbuild_keep; j++) bpay.push_back(payload_desc(b.cols[nk + j], b.rows));
   ghb_join_table* jt = nullptr;
-  if ((st = ghb_join_build(P.ctx, &bkey, bd.data() + nk, op.nbuild_keep, nullptr, &jt, P.s))) return st;
+  if ((st = ghb_join_build(P.ctx, &bkey, bpay.data(), op.nbuild_keep, nullptr, &jt, P.s))) return st;
   int64_t rows = 0, max_dup = 1, slots = 0;
   if ((st = ghb_sync(P.ctx, P.s)) || (st = ghb_join_table_info(P.ctx, jt, &rows, &max_dup, &slots))) {
     ghb_join_table_free(P.ctx, jt);
@@ -247,9 +398,16 @@ int32_t run_join(Plan& P, const ghb_plan_op& op, const ghb_gtables* in, DevTable
   const int np = (int)t.cols.size();
   o.cols.resize(np + op.nbuild_keep);
   std::vector<ghb_out_column> op_out(np), ob_out(op.nbuild_keep);
-  for (int j = 0; j < np && !st; j++) st = P.out_col(t.cols[j].type, cap, &o.cols[j], &op_out[j]);
-  for (int j = 0; j < op.nbuild_keep && !st; j++)
-    st = P.out_col(b.cols[nk + j].type, cap, &o.cols[np + j], &ob_out[j]);
+  std::vector<ghb_column> probe(np);
+  for (int j = 0; j < np && !st; j++) {
+    probe[j] = payload_desc(t.cols[j], t.rows);
+    st = P.out_col(t.cols[j].type, cap, &o.cols[j], &op_out[j], &t.cols[j]);
+    op_out[j] = payload_out(op_out[j]);
+  }
+  for (int j = 0; j < op.nbuild_keep && !st; j++) {
+    st = P.out_col(b.cols[nk + j].type, cap, &o.cols[np + j], &ob_out[j], &b.cols[nk + j]);
+    ob_out[j] = payload_out(ob_out[j]);
+  }
   int64_t* d_rows = nullptr;
   if (!st) st = P.alloc(8, (void**)&d_rows);
   if (!st)
@@ -279,7 +437,7 @@ int32_t run_sort(Plan& P, const ghb_plan_op& op, DevTable& t) {
   }
   for (int c = 0; c < (int)t.cols.size(); c++)
     if (!is_key[c]) {
-      pay.push_back(in[c]);
+      pay.push_back(payload_desc(t.cols[c], t.rows));
       pay_idx.push_back(c);
     }
   DevTable o;
@@ -288,14 +446,58 @@ int32_t run_sort(Plan& P, const ghb_plan_op& op, DevTable& t) {
   std::vector<ghb_out_column> ok(keys.size()), opay(pay.size());
   int32_t st;
   for (size_t j = 0; j < keys.size(); j++)
-    if ((st = P.out_col(keys[j].type, t.rows, &o.cols[j], &ok[j]))) return st;
-  for (size_t j = 0; j < pay.size(); j++)
-    if ((st = P.out_col(pay[j].type, t.rows, &o.cols[keys.size() + j], &opay[j]))) return st;
+    if ((st = P.out_col(keys[j].type, t.rows, &o.cols[j], &ok[j], &t.cols[op.idx[j]]))) return st;
+  for (size_t j = 0; j < pay.size(); j++) {
+    const DevCol& src = t.cols[pay_idx[j]];
+    if ((st = P.out_col(src.type, t.rows, &o.cols[keys.size() + j], &opay[j], &src))) return st;
+    opay[j] = payload_out(opay[j]);
+  }
   if ((st = ghb_sort(P.ctx, keys.data(), op.orders, op.null_orders, (int32_t)keys.size(), pay.data(),
                      (int32_t)pay.size(), ok.data(), opay.data(), nullptr, nullptr, P.s)))
     return st;
   if ((st = ghb_sync(P.ctx, P.s))) return st;
   t = std::move(o);
+  return GHB_OK;
+}
+
+// A STRING result column: its rows' bytes packed one after the other into
+// out->str_bytes[c] and its pairs, rebased onto them, into out->data[c]
+// (GPUResult builds each row's String from its [start,end)).
+int32_t download_string(Plan& P, const DevCol& d, int64_t rows, ghb_plan_result* out, int c) {
+  std::vector<int2> from((size_t)std::max<int64_t>(rows, 1)), to((size_t)std::max<int64_t>(rows, 1));
+  if (rows > 0) {
+    GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(from.data(), d.data, rows * 8, cudaMemcpyDeviceToHost, P.s));
+    GHB_CUDA_TRY(P.ctx, cudaStreamSynchronize(P.s));
+  }
+  int64_t total = 0;
+  for (int64_t r = 0; r < rows; r++) {
+    if (from[r].x < 0) {
+      to[r] = make_int2(-1, -1);
+      continue;
+    }
+    to[r] = make_int2((int32_t)total, (int32_t)(total + (from[r].y - from[r].x)));
+    total += from[r].y - from[r].x;
+    if (total >= INT32_MAX) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "result column %d: 2^31 bytes of strings", c);
+  }
+  if (cudaMallocHost(&out->data[c], (size_t)std::max<int64_t>(rows, 1) * 8) != cudaSuccess ||
+      cudaMallocHost((void**)&out->str_bytes[c], (size_t)std::max<int64_t>(total, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(P.ctx, GHB_ERR_OOM, "cannot allocate pinned host memory for the result");
+  }
+  std::memcpy(out->data[c], to.data(), (size_t)rows * 8);
+  out->str_nbytes[c] = total;
+  if (total == 0) return GHB_OK;
+  void *d_to = nullptr, *d_bytes = nullptr;
+  int32_t st = P.alloc((size_t)rows * 8, &d_to);
+  if (!st) st = P.alloc((size_t)total, &d_bytes);
+  if (st) return st;
+  GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d_to, to.data(), rows * 8, cudaMemcpyHostToDevice, P.s));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, (int64_t)P.ctx->num_sms * 8));
+  gather_string_bytes_kernel<<<grid, 256, 0, P.s>>>(d.bytes, (const int2*)d.data, (const int2*)d_to, rows,
+                                                    (uint8_t*)d_bytes);
+  GHB_LAUNCH_CHECK(P.ctx);
+  GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(out->str_bytes[c], d_bytes, total, cudaMemcpyDeviceToHost, P.s));
+  GHB_CUDA_TRY(P.ctx, cudaStreamSynchronize(P.s));   // `to` is host memory the copy reads
   return GHB_OK;
 }
 
@@ -341,14 +543,14 @@ int32_t ghb_gtables_table(const ghb_gtables* in, int32_t table, ghb_column* cols
   return GHB_OK;
 }
 
-int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const ghb_plan_op* ops,
+static int32_t ghb_run_plan_body(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const ghb_plan_op* ops,
                      int32_t nops, ghb_plan_result* out) {
   if (!ctx || !in || !out || (nops > 0 && !ops) || nops < 0) return GHB_ERR_INVALID;
   std::memset(out, 0, sizeof(*out));
-  ghb_column hc[kMaxCols];
+  ghb_column hc[kPlanCols];
   int32_t nc = 0;
   int64_t rows = 0;
-  if (ghb_gtables_table(in, input, hc, kMaxCols, &nc, &rows))
+  if (ghb_gtables_table(in, input, hc, kPlanCols, &nc, &rows))
     return set_error(ctx, GHB_ERR_INVALID, "input table %d is missing or malformed", input);
   if (!ctx->hstream[1]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[1], cudaStreamNonBlocking));
   Plan P{ctx, ctx->hstream[1], {}};
@@ -366,7 +568,8 @@ int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const g
   }
   if (st) return st;
   if ((int)t.cols.size() > GHB_MAX_RESULT_COLS)
-    return set_error(ctx, GHB_ERR_UNSUPPORTED, "result of %zu columns", t.cols.size());
+    return set_error(ctx, GHB_ERR_UNSUPPORTED, "result of %zu columns (at most %d)", t.cols.size(),
+                     GHB_MAX_RESULT_COLS);
   // the result: host columns (NULLs as GHive's sentinels, and a NULL map),
   // grouped by type the way GPUResult holds them
   out->ncols = (int32_t)t.cols.size();
@@ -383,6 +586,13 @@ int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const g
     const DevCol& d = t.cols[c];
     out->types[c] = d.type;
     out->sequence[c] = base[d.type] + seen[d.type]++;
+    if (d.type == GHB_STRING) {
+      if ((st = download_string(P, d, t.rows, out, c))) {
+        ghb_plan_result_free(out);
+        return st;
+      }
+      continue;
+    }
     const size_t bytes = (size_t)std::max<int64_t>(t.rows, 1) * width_of(d.type);
     if (cudaMallocHost(&out->data[c], bytes) != cudaSuccess ||
         (d.is_null && cudaMallocHost((void**)&out->is_null[c], std::max<int64_t>(t.rows, 1)) != cudaSuccess)) {
@@ -400,13 +610,29 @@ int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const g
   return GHB_OK;
 }
 
+int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const ghb_plan_op* ops, int32_t nops,
+                     ghb_plan_result* out) {
+  CallScope cs(ctx, "run_plan", 0, true);
+  ghb_column hc[kPlanCols];
+  int32_t nc = 0;
+  int64_t rows = 0;
+  if (ghb_gtables_table(in, input, hc, kPlanCols, &nc, &rows) == GHB_OK) {
+    cs.rows(rows);
+    cs.bytes(cols_bytes(hc, nc));
+  }
+  return cs.done(ghb_run_plan_body(ctx, in, input, ops, nops, out));
+}
+
 int32_t ghb_plan_result_free(ghb_plan_result* r) {
   if (!r) return GHB_ERR_INVALID;
   for (int c = 0; c < GHB_MAX_RESULT_COLS; c++) {
     if (r->data[c]) cudaFreeHost(r->data[c]);
     if (r->is_null[c]) cudaFreeHost(r->is_null[c]);
+    if (r->str_bytes[c]) cudaFreeHost(r->str_bytes[c]);
     r->data[c] = nullptr;
     r->is_null[c] = nullptr;
+    r->str_bytes[c] = nullptr;
+    r->str_nbytes[c] = 0;
   }
   r->ncols = 0;
   r->rows = 0;

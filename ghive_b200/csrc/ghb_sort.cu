@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "ghb_ctx.hpp"
+#include "ghb_log.hpp"
 
 namespace ghb {
 
@@ -966,16 +967,19 @@ extern "C" int32_t ghb_sort(ghb_ctx* ctx, const ghb_column* keys, const int32_t*
                             int32_t npayload, ghb_out_column* out_keys, ghb_out_column* out_payload,
                             int32_t* out_rowid, const ghb_sort_cfg* cfg, void* stream) {
   if (!ctx) return GHB_ERR_INVALID;
-  scratch_reset(ctx);
+  CallScope cs(ctx, "sort", (cudaStream_t)stream);
   int64_t n = keys && nkeys > 0 ? keys[0].n : 0;
+  cs.rows(n);
+  cs.bytes(cols_bytes(keys, nkeys) + cols_bytes(payload, npayload));
+  scratch_reset(ctx);
   bool strings = false;
   for (int j = 0; keys && j < nkeys && j < kMaxSortKeys; j++) strings |= keys[j].type == GHB_STRING;
   const size_t extra = strings ? string_sort_scratch_bytes(keys, nkeys, n) : 0;
   int32_t st = scratch_reserve(ctx, sort_scratch_bytes(n) + extra, (cudaStream_t)stream);
-  if (st) return st;
+  if (st) return cs.done(st);
   if (strings)
-    return sort_with_strings(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys, out_payload,
-                             out_rowid, cfg, (cudaStream_t)stream);
-  return sort_impl(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys, out_payload,
-                   out_rowid, cfg, (cudaStream_t)stream);
+    return cs.done(sort_with_strings(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys,
+                                     out_payload, out_rowid, cfg, (cudaStream_t)stream));
+  return cs.done(sort_impl(ctx, keys, orders, null_orders, nkeys, payload, npayload, out_keys, out_payload,
+                           out_rowid, cfg, (cudaStream_t)stream));
 }

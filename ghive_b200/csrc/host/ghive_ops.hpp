@@ -18,8 +18,10 @@
 //     caller's buffers (the reference compacted them in place);
 //   - errors: functions returning a Table* return nullptr on failure, as the
 //     reference does, and the reason is last_error() (per thread);
-//   - joins are hash joins on one LONG or INT key between two tables (left =
-//     probe side, right = build side); N-way chains return nullptr.
+//   - joins are hash joins (left = probe side, right = build side): two
+//     tables on one LONG or INT key run on the pipelined host join; N-way
+//     chains, keys of several or STRING columns and semi joins run as one
+//     device plan (ghb_run_plan) whose intermediates stay on the device.
 // One device context per host thread is created on first use (device 0, or
 // the one set_device() names first).
 #pragma once
@@ -107,16 +109,32 @@ struct Column {
     data_ptr = std::calloc(n ? n : 1, detail::width(t));
   }
   Column(ColumnType t, uint32_t n, void* p) : data_ptr(p), type(t), row_num(n) {}
+  // A STRING column around caller memory: char_size bytes of UTF-8 text in
+  // chars and an int32 [start,end) pair per row in pairs (-1,-1: NULL).
+  Column(ColumnType t, uint32_t n, void* chars, void* pairs, uint32_t csize)
+      : data_ptr(chars), data_ptr_aux(pairs), type(t), row_num(n), char_size(csize) {}
+  // A STRING column owning copies of its bytes and pairs.
+  static Column* string_copy(uint32_t n, const void* chars, uint32_t nchars, const void* pairs) {
+    Column* c = new Column(STRING, n, std::malloc(nchars ? nchars : 1), std::malloc(n ? 8 * (size_t)n : 8), nchars);
+    c->owned = true;
+    if (nchars) std::memcpy(c->data_ptr, chars, nchars);
+    if (n) std::memcpy(c->data_ptr_aux, pairs, 8 * (size_t)n);
+    return c;
+  }
   Column(const Column&) = delete;
   Column& operator=(const Column&) = delete;
   ~Column() {
-    if (owned) std::free(data_ptr);
+    if (owned) {
+      std::free(data_ptr);
+      std::free(data_ptr_aux);
+    }
   }
   ghb_column desc() const {
     ghb_column c{};
     c.type = type;
     c.null_mode = GHB_NULLS_SENTINEL;
     c.data = data_ptr;
+    c.aux = data_ptr_aux;
     c.n = row_num;
     return c;
   }
@@ -306,12 +324,18 @@ class GroupByPredicate {
   }
 };
 
-// GHive's BaseJoinPredicate (BaseJoinPredicate.hpp:47-86) as a hash join:
-// tables[0] is the left (probe) side, tables[1] the right (build) side;
-// join_cols[i][0] is table i's key column, maintain_cols[i] the columns table
-// i contributes to the result (left columns first), join_types one entry
-// {type, {0, 1}}.  result_offsets receives, per result row, the left row and
-// the right row (-1 where an outer join found no match, or for a semi join).
+// GHive's BaseJoinPredicate (BaseJoinPredicate.hpp:47-86) as a hash join.
+// join_cols[i] are table i's key columns (the same count for every table),
+// maintain_cols[i] the columns table i contributes to the result, join_types
+// the chain's steps {type, {first, second}}: step 0 joins table 0 (the probe
+// side) with its second table, each later step joins the tuples so far, by
+// the key columns of the already joined table `first`, with table `second`
+// (SortMergeJoinPredicate.cu:138-454).  A semi join's table contributes no
+// columns.  The result holds the maintained columns of table 0, then of each
+// further non-semi table in step order (table 0 keeps column 0 when it names
+// none, BaseJoinPredicate.cu:13-19); result_offsets receives, per result row,
+// the row of each of those tables (-1 where an outer join found no match).
+// Result rows come in no particular order (the reference's in key order).
 class HashJoinPredicate {
  public:
   std::vector<std::vector<uint32_t>> join_cols;
@@ -322,12 +346,12 @@ class HashJoinPredicate {
   Table* process(const std::vector<Table*>& tables) {
     ghb_ctx* c = detail::ctx();
     if (!c) return nullptr;
-    detail::State& s = detail::state();
     if (tables.size() != 2 || join_types.size() != 1 || join_types[0].second != std::make_pair(0u, 1u) ||
-        join_cols.size() != 2 || join_cols[0].size() != 1 || join_cols[1].size() != 1) {
-      s.error = "the device join takes two tables and one key column each (N-way chains are not supported)";
-      return nullptr;
-    }
+        join_types[0].first == LEFT_SEMI_JOIN || join_cols.size() != 2 || join_cols[0].size() != 1 ||
+        join_cols[1].size() != 1 || join_cols[0][0] >= tables[0]->columns.size() ||
+        join_cols[1][0] >= tables[1]->columns.size() || tables[0]->columns[join_cols[0][0]]->type == STRING ||
+        tables[0]->columns[join_cols[0][0]]->type == DOUBLE)
+      return chain(tables);
     const Table* left = tables[0];
     const Table* right = tables[1];
     const ghb_column lkey = left->columns[join_cols[0][0]]->desc();
@@ -371,6 +395,163 @@ class HashJoinPredicate {
       return t;
     }
     return nullptr;
+  }
+
+ private:
+  // The general chain as one device plan: a GTables of the columns each table
+  // must bring (its maintained columns and the key columns of the steps that
+  // read it), each table with its row ids appended as an INT column; one
+  // JOIN_PROBE per step, the tuples so far as its probe side; a final
+  // projection to the maintained columns and the row ids.
+  Table* chain(const std::vector<Table*>& tables) {
+    ghb_ctx* c = detail::ctx();
+    detail::State& s = detail::state();
+    auto bad = [&](const std::string& m) -> Table* {
+      s.error = m;
+      return nullptr;
+    };
+    const size_t nt = tables.size();
+    if (nt < 2 || join_cols.size() != nt || join_types.empty())
+      return bad("a join takes two or more tables, key columns for each and at least one step");
+    for (size_t t = 0; t < nt; t++)
+      for (uint32_t k : join_cols[t])
+        if (k >= tables[t]->columns.size()) return bad("join key column out of range");
+    // the tables in the result, in order, and each table's columns on the device
+    std::vector<int> state(nt, 0);   // 1: joined, 2: semi-joined
+    state[0] = 1;
+    std::vector<size_t> result_tbl{0};
+    std::vector<std::vector<uint32_t>> need(nt);
+    auto add = [&](size_t t, uint32_t col) {
+      if (std::find(need[t].begin(), need[t].end(), col) == need[t].end()) need[t].push_back(col);
+    };
+    for (const auto& step : join_types) {
+      const uint32_t f = step.second.first, sc = step.second.second;
+      if (f >= nt || sc >= nt || state[f] != 1 || state[sc] != 0)
+        return bad("join step {" + std::to_string(f) + ", " + std::to_string(sc) +
+                   "}: the first table must be joined already and the second not");
+      if (join_cols[f].empty() || join_cols[f].size() != join_cols[sc].size())
+        return bad("join step: both tables need the same number of key columns");
+      if (step.first != INNER_JOIN && step.first != LEFT_OUTER_JOIN && step.first != LEFT_SEMI_JOIN)
+        return bad("join type " + std::to_string((int)step.first) + " is not run on the device");
+      for (uint32_t k : join_cols[f]) add(f, k);
+      for (uint32_t k : join_cols[sc]) add(sc, k);
+      state[sc] = step.first == LEFT_SEMI_JOIN ? 2 : 1;
+      if (step.first != LEFT_SEMI_JOIN) result_tbl.push_back(sc);
+    }
+    std::vector<std::vector<uint32_t>> keep(nt);
+    for (size_t i = 0; i < result_tbl.size(); i++) {
+      const size_t t = result_tbl[i];
+      keep[t] = t < maintain_cols.size() ? maintain_cols[t] : std::vector<uint32_t>{};
+      if (keep[t].empty() && i == 0) keep[t].push_back(0);
+      for (uint32_t col : keep[t]) {
+        if (col >= tables[t]->columns.size()) return bad("maintained column out of range");
+        add(t, col);
+      }
+    }
+    // the GTables: table t's columns need[t] then its row ids
+    std::vector<std::vector<int32_t>> types(nt), rowids(nt);
+    std::vector<int32_t> ncols(nt), rows(nt), keys(nt, 0);
+    std::vector<const char*> names(nt, "v");
+    std::vector<const void*> bufs[4], idx_bufs;
+    for (size_t t = 0; t < nt; t++) {
+      for (uint32_t col : need[t]) {
+        const Column* cl = tables[t]->columns[col];
+        if (cl->type < LONG || cl->type > STRING) return bad("DEPEND columns cannot be joined");
+        types[t].push_back((int32_t)cl->type);
+        bufs[cl->type].push_back(cl->data_ptr);
+        if (cl->type == STRING) idx_bufs.push_back(cl->data_ptr_aux);
+      }
+      rowids[t].resize(tables[t]->row_num);
+      for (uint32_t r = 0; r < tables[t]->row_num; r++) rowids[t][r] = (int32_t)r;
+      types[t].push_back(INT);
+      bufs[INT].push_back(rowids[t].data());
+      ncols[t] = (int32_t)types[t].size();
+      rows[t] = (int32_t)tables[t]->row_num;
+    }
+    std::vector<const int32_t*> type_ptrs(nt);
+    for (size_t t = 0; t < nt; t++) type_ptrs[t] = types[t].data();
+    ghb_gtables g{};
+    g.ntables = (int32_t)nt;
+    g.ncols = ncols.data();
+    g.types = type_ptrs.data();
+    g.row_cnt = rows.data();
+    g.key_cnt = keys.data();
+    g.vertex_name = names.data();
+    g.nlong = (int32_t)bufs[LONG].size();
+    g.long_cols = bufs[LONG].data();
+    g.ndouble = (int32_t)bufs[DOUBLE].size();
+    g.double_cols = bufs[DOUBLE].data();
+    g.nint = (int32_t)bufs[INT].size();
+    g.int_cols = bufs[INT].data();
+    g.nstring = (int32_t)bufs[STRING].size();
+    g.string_cols = bufs[STRING].data();
+    g.string_idx_cols = idx_bufs.data();
+    // the plan: the tuples so far as (table, GTables column) pairs
+    auto gcol = [&](size_t t, uint32_t col) {
+      return (int32_t)(std::find(need[t].begin(), need[t].end(), col) - need[t].begin());
+    };
+    std::vector<std::pair<size_t, int32_t>> acc;
+    for (int32_t j = 0; j < ncols[0]; j++) acc.push_back({0, j});
+    auto pos = [&](size_t t, int32_t j) {
+      return (int32_t)(std::find(acc.begin(), acc.end(), std::make_pair(t, j)) - acc.begin());
+    };
+    std::vector<std::vector<int32_t>> idx(join_types.size()), bkeep(join_types.size());
+    std::vector<ghb_plan_op> ops;
+    for (size_t i = 0; i < join_types.size(); i++) {
+      const uint32_t f = join_types[i].second.first, sc = join_types[i].second.second;
+      for (uint32_t k : join_cols[f]) idx[i].push_back(pos(f, gcol(f, k)));
+      for (uint32_t k : join_cols[sc]) idx[i].push_back(gcol(sc, k));
+      if (join_types[i].first != LEFT_SEMI_JOIN)
+        for (int32_t j = 0; j < ncols[sc]; j++) {
+          bkeep[i].push_back(j);
+          acc.push_back({sc, j});
+        }
+      ghb_plan_op op{};
+      op.op = GHB_OP_JOIN_PROBE;
+      op.join_type = (int32_t)join_types[i].first;
+      op.idx = idx[i].data();
+      op.nidx = (int32_t)idx[i].size();
+      op.build_table = (int32_t)sc;
+      op.nbuild_keep = (int32_t)bkeep[i].size();
+      op.build_keep = bkeep[i].data();
+      ops.push_back(op);
+    }
+    std::vector<int32_t> proj;
+    for (size_t t : result_tbl)
+      for (uint32_t col : keep[t]) proj.push_back(pos(t, gcol(t, col)));
+    for (size_t t : result_tbl) proj.push_back(pos(t, ncols[t] - 1));
+    ghb_plan_op last{};
+    last.op = GHB_OP_FILTER;
+    last.idx = proj.data();
+    last.nidx = (int32_t)proj.size();
+    ops.push_back(last);
+    ghb_plan_result res;
+    if (detail::fail(ghb_run_plan(c, &g, 0, ops.data(), (int32_t)ops.size(), &res))) return nullptr;
+    // the maintained columns (NULLs as sentinels), then the row ids
+    const int64_t n = res.rows;
+    Table* out = new Table();
+    out->row_num = (uint32_t)n;
+    const int nkeep = (int)proj.size() - (int)result_tbl.size();
+    for (int j = 0; j < nkeep; j++) {
+      const ColumnType t = (ColumnType)res.types[j];
+      if (t == STRING) {
+        out->columns.push_back(Column::string_copy((uint32_t)n, res.str_bytes[j], (uint32_t)res.str_nbytes[j],
+                                                   res.data[j]));
+        continue;
+      }
+      Column* col = new Column(t, (uint32_t)n);
+      if (n) std::memcpy(col->data_ptr, res.data[j], (size_t)n * detail::width(t));
+      out->columns.push_back(col);
+    }
+    result_offsets.assign((size_t)n * result_tbl.size(), -1);
+    for (size_t i = 0; i < result_tbl.size(); i++) {
+      const int32_t* ids = (const int32_t*)res.data[nkeep + i];
+      const uint8_t* nul = res.is_null[nkeep + i];
+      for (int64_t r = 0; r < n; r++)
+        if (!(nul && nul[r])) result_offsets[(size_t)r * result_tbl.size() + i] = ids[r];
+    }
+    ghb_plan_result_free(&res);
+    return out;
   }
 };
 

@@ -149,7 +149,8 @@ def _ops_array(ops):
 def run_plan(ctx, gtables, input_table, ops):
     """Runs the chain on the device; returns a dict shaped like GPUResult:
     long/double/int column lists, row count and sequence, plus `columns`
-    (the result columns in order, as (values, isnull) numpy pairs)."""
+    (the result columns in order, as (values, isnull) pairs; a STRING
+    column's values are a list of bytes, None for NULL)."""
     arr, keep = _ops_array(ops)
     res = abi.PlanResult()
     st = lib().ghb_run_plan(ctx.h, gtables.ptr, input_table, arr, len(ops), C.byref(res))
@@ -160,6 +161,14 @@ def run_plan(ctx, gtables, input_table, ops):
         n = res.rows
         for i in range(res.ncols):
             t = res.types[i]
+            if t == abi.STRING:   # pairs into the column's packed bytes -> bytes per row, None = NULL
+                pairs = np.ctypeslib.as_array(C.cast(res.data[i], C.POINTER(C.c_int32)),
+                                              shape=(2 * max(n, 1),))[:2 * n].reshape(-1, 2)
+                nb = res.str_nbytes[i]
+                blob = C.string_at(res.str_bytes[i], nb) if nb > 0 else b""
+                vals = [None if a < 0 else blob[a:b] for a, b in pairs.tolist()]
+                cols.append((vals, np.array([v is None for v in vals], dtype=bool)))
+                continue
             dt = abi.NP_DTYPE[t]
             vals = np.ctypeslib.as_array(C.cast(res.data[i], C.POINTER(np.ctypeslib.as_ctypes_type(dt))),
                                          shape=(max(n, 1),))[:n].copy()
@@ -169,11 +178,11 @@ def run_plan(ctx, gtables, input_table, ops):
             else:
                 nl = np.zeros(n, dtype=bool)
             cols.append((vals, nl))
-        by_type = {0: [], 1: [], 2: []}
+        by_type = {0: [], 1: [], 2: [], 3: []}
         for i in range(res.ncols):
             by_type[res.types[i]].append(cols[i][0])
         return {"columns": cols, "rows": n, "sequence": [res.sequence[i] for i in range(res.ncols)],
                 "longCols": by_type[0], "doubleCols": by_type[1], "intCols": by_type[2],
-                "types": [res.types[i] for i in range(res.ncols)]}
+                "stringCols": by_type[3], "types": [res.types[i] for i in range(res.ncols)]}
     finally:
         lib().ghb_plan_result_free(C.byref(res))

@@ -253,6 +253,13 @@ class Context:
         """Bound of this context's look-back waits (polls <= 0: the default)."""
         self._check(lib().ghb_ctx_set_spin_limit(self.h, int(polls)))
 
+    def set_log(self, path, level=1, peak_gbs=0.0):
+        """One JSON line per operator call of this context appended to `path`
+        (level 2 also times each call on the device and synchronises it);
+        path None closes the log."""
+        self._check(lib().ghb_ctx_set_log(self.h, None if path is None else str(path).encode(), int(level),
+                                          float(peak_gbs)))
+
     # ------------------------------------------------------------ device ops
     def filter(self, pred, cols, proj=None, capacity=None, stream=None, sync=True):
         """FilterPredicate::process + FilterOperator::clean_data on device columns.

@@ -225,6 +225,21 @@ int64_t ghb_kernel_launches(const ghb_ctx* ctx);
  * timeout path on purpose. */
 int32_t ghb_ctx_set_spin_limit(ghb_ctx* ctx, int32_t polls);
 
+/* Per-call tracing.  Every operator entry point opens an NVTX range named for
+ * the operator (seen by Nsight tools when one is attached).  With a log open,
+ * each call of this context also appends one JSON line to `path`:
+ *   level 1: {"op", "device", "rows", "bytes", "host_us", "status"}: rows and
+ *            the algorithmic input bytes of the call, and its host-side time
+ *            (the enqueue of an asynchronous call; all of a host-buffer or
+ *            plan call);
+ *   level 2: the call is bracketed by events on its stream and waited for,
+ *            adding "device_us", "gbs" and, with peak_gbs > 0,
+ *            "roofline_frac" = gbs / peak_gbs.  For measurement only: it
+ *            synchronises every call and must not be used under stream capture.
+ * path NULL or level 0 closes the log.  ghb_ctx_create opens one when the
+ * environment sets GHB_LOG=<path> (GHB_LOG_LEVEL, GHB_LOG_PEAK_GBS). */
+int32_t ghb_ctx_set_log(ghb_ctx* ctx, const char* path, int32_t level, double peak_gbs);
+
 /* ---- filter (F1) -------------------------------------------------------
  * Replaces FilterPredicate::process (FilterPredicate.cu:434-571) followed by
  * FilterOperator::clean_data (FilterOperator.cu:36-93): evaluates the
@@ -279,7 +294,9 @@ int32_t ghb_filter_groupby(ghb_ctx* ctx, const ghb_predicate* pred,
  * build_payload columns, which must stay valid until the table is freed.
  * The table stays resident on the device until ghb_join_table_free, so one
  * build serves many probes (a broadcast map-join small table).  NULL build
- * keys are not inserted; NULL probe keys never match. */
+ * keys are not inserted; NULL probe keys never match.  At most
+ * GHB_MAX_JOIN_PAYLOAD build payloads (and as many probe payloads per probe). */
+#define GHB_MAX_JOIN_PAYLOAD 16
 int32_t ghb_join_build(ghb_ctx* ctx, const ghb_column* build_key,
                        const ghb_column* build_payload, int32_t n_build_payload,
                        const ghb_join_cfg* cfg, ghb_join_table** out,
@@ -551,13 +568,16 @@ int32_t ghb_gtables_table(const ghb_gtables* in, int32_t table, ghb_column* cols
 typedef struct ghb_plan_op {
   int32_t op;                  /* GHB_OP_FILTER / GROUPBY / JOIN_PROBE / SORT */
   int32_t join_type;           /* JOIN_PROBE                                   */
-  const ghb_predicate* pred;   /* FILTER                                       */
+  const ghb_predicate* pred;   /* FILTER (NULL: a projection alone, which
+                                  selects columns without copying them)       */
   const int32_t* idx;          /* FILTER: projection (NULL = all columns);
                                   GROUPBY: key columns; SORT: key columns;
                                   JOIN_PROBE: the k probe key columns, then
                                   the k build key columns of the build table
                                   (k > 1: the tuples are packed into one key,
-                                  fixed-width columns, 63 bits at most)        */
+                                  63 bits at most; a STRING key column of both
+                                  sides is first mapped to ids equal exactly
+                                  when the strings are)                        */
   int32_t nidx;
   int32_t naggs;               /* GROUPBY                                      */
   const ghb_agg_desc* aggs;
@@ -574,8 +594,11 @@ typedef struct ghb_plan_op {
  * (GPUResult.java:29-39, built at ghive_JNIInterface.cu:217-340): column i
  * has types[i], data[i] (NULLs as GHive's sentinels) and is_null[i]
  * (NULL: no NULL map), and sequence[i] is its index in the concatenation
- * long || double || int || string of GPUResult's arrays.  The arrays are
- * pinned host memory owned by the library until ghb_plan_result_free. */
+ * long || double || int || string of GPUResult's arrays.  A STRING column's
+ * data[i] is its int32 [start,end) pairs (-1,-1 = NULL) into str_bytes[i],
+ * its rows' UTF-8 bytes packed in row order (str_nbytes[i] of them); it has
+ * no NULL map.  The arrays are pinned host memory owned by the library until
+ * ghb_plan_result_free. */
 typedef struct ghb_plan_result {
   int32_t ncols;
   int32_t types[GHB_MAX_RESULT_COLS];
@@ -584,6 +607,8 @@ typedef struct ghb_plan_result {
   int32_t sequence[GHB_MAX_RESULT_COLS];
   int64_t rows;
   int32_t n_long, n_double, n_int, n_string;
+  uint8_t* str_bytes[GHB_MAX_RESULT_COLS];
+  int64_t str_nbytes[GHB_MAX_RESULT_COLS];
 } ghb_plan_result;
 
 /* Runs `nops` operators on input table `input` of `in`: the table's columns
@@ -591,7 +616,11 @@ typedef struct ghb_plan_result {
  * as the next one's input (GHive copied each operator's input in and output
  * back, FilterOperator.cu:53-89, GroupByPredicate.cu:39-91), a JOIN_PROBE
  * builds its hash table from another input table, and only the final table
- * is copied back into `out`.  Synchronous; the context's own stream. */
+ * is copied back into `out`.  STRING columns (stringCols with their
+ * stringIdxCols) travel as their pairs into bytes copied once: they may be
+ * predicate leaves and projections, group-by and sort keys, join keys and
+ * payloads of either side, not aggregate inputs.  Synchronous; the
+ * context's own stream. */
 int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input,
                      const ghb_plan_op* ops, int32_t nops, ghb_plan_result* out);
 int32_t ghb_plan_result_free(ghb_plan_result* result);

@@ -163,11 +163,141 @@ static void test_join() {
     CHECK(offs);
     delete r;
   }
-  HashJoinPredicate three;
-  three.join_cols = {{0}, {0}, {0}};
-  three.join_types = {{INNER_JOIN, {0u, 1u}}, {INNER_JOIN, {0u, 2u}}};
-  CHECK(three.process({left, right, right}) == nullptr && !last_error().empty());
+  // a three-table chain: left joins right on its key, then the tuples join a
+  // third table by the right table's key (join_cols[1] serves both steps),
+  // LEFT OUTER: right keys without a third row keep their tuple with NULLs
+  {
+    const uint32_t n3 = 400;
+    Table* third = new Table();
+    Column* tk = new Column(LONG, n3);
+    Column* tv = new Column(LONG, n3);
+    for (uint32_t i = 0; i < n3; i++) {
+      tk->as<int64_t>()[i] = (int64_t)(2 * i);   // the even right keys below 800
+      tv->as<int64_t>()[i] = (int64_t)i * 11 - 5;
+    }
+    third->columns = {tk, tv};
+    third->row_num = n3;
+    HashJoinPredicate three;
+    three.join_cols = {{0}, {0}, {0}};
+    three.maintain_cols = {{1}, {1}, {1}};
+    three.join_types = {{INNER_JOIN, {0u, 1u}}, {LEFT_OUTER_JOIN, {1u, 2u}}};
+    Table* r = three.process({left, right, third});
+    CHECK(r != nullptr);
+    if (r) {
+      std::multiset<std::tuple<int32_t, int64_t, int64_t, int32_t, int32_t, int32_t>> expect, got;
+      for (uint32_t i = 0; i < nl; i++) {
+        const int64_t key = lk->as<int64_t>()[i];
+        if (key == kLongNull || key >= (int64_t)nr) continue;
+        const bool t3 = key % 2 == 0 && key < 2 * (int64_t)n3;
+        expect.insert(std::make_tuple((int32_t)i, rv->as<int64_t>()[key], t3 ? tv->as<int64_t>()[key / 2] : kLongNull,
+                                      (int32_t)i, (int32_t)key, t3 ? (int32_t)(key / 2) : -1));
+      }
+      CHECK(r->columns.size() == 3 && three.result_offsets.size() == 3 * (size_t)r->row_num);
+      for (uint32_t i = 0; r->columns.size() == 3 && i < r->row_num; i++)
+        got.insert(std::make_tuple(r->columns[0]->as<int32_t>()[i], r->columns[1]->as<int64_t>()[i],
+                                   r->columns[2]->as<int64_t>()[i], three.result_offsets[3 * i],
+                                   three.result_offsets[3 * i + 1], three.result_offsets[3 * i + 2]));
+      CHECK(got == expect);
+      delete r;
+    }
+    delete third;
+  }
+  // a semi join: the right table contributes no columns and no offsets
+  {
+    HashJoinPredicate semi;
+    semi.join_cols = {{0}, {0}};
+    semi.maintain_cols = {{1, 0}, {1}};
+    semi.join_types = {{LEFT_SEMI_JOIN, {0u, 1u}}};
+    Table* r = semi.process({left, right});
+    CHECK(r != nullptr);
+    if (r) {
+      std::multiset<int32_t> expect, got;
+      for (uint32_t i = 0; i < nl; i++) {
+        const int64_t key = lk->as<int64_t>()[i];
+        if (key != kLongNull && key < (int64_t)nr) expect.insert((int32_t)i);
+      }
+      bool ok = r->columns.size() == 2 && semi.result_offsets.size() == (size_t)r->row_num;
+      for (uint32_t i = 0; ok && i < r->row_num; i++) {
+        got.insert(r->columns[0]->as<int32_t>()[i]);
+        ok = semi.result_offsets[i] == r->columns[0]->as<int32_t>()[i] &&
+             r->columns[1]->as<int64_t>()[i] == lk->as<int64_t>()[semi.result_offsets[i]];
+      }
+      CHECK(ok && got == expect);
+      delete r;
+    }
+  }
+  // a step that reads a table not joined yet is refused
+  HashJoinPredicate wrong;
+  wrong.join_cols = {{0}, {0}, {0}};
+  wrong.join_types = {{INNER_JOIN, {0u, 1u}}, {INNER_JOIN, {2u, 1u}}};
+  CHECK(wrong.process({left, right, right}) == nullptr && !last_error().empty());
   delete left;
+  delete right;
+}
+
+// A join on a STRING key column (with NULL keys) that keeps a STRING column
+// of the build side: the strings come back as their own bytes and pairs.
+static void test_string_join() {
+  const char* names[] = {"ALGERIA", "ARGENTINA", "BRAZIL", "CANADA", "EGYPT", "", "\xc3\x89TATS"};
+  const uint32_t nn = 7, nl = 5000;
+  std::string lchars;
+  std::vector<int32_t> lpairs;
+  std::mt19937_64 g(5);
+  std::vector<int> pick(nl);
+  for (uint32_t i = 0; i < nl; i++) {
+    pick[i] = (int)(g() % (nn + 2)) - 1;   // -1: NULL, nn: a name no build row has
+    if (pick[i] < 0) {
+      lpairs.insert(lpairs.end(), {-1, -1});
+      continue;
+    }
+    const std::string v = pick[i] < (int)nn ? names[pick[i]] : "NOWHERE";
+    lpairs.push_back((int32_t)lchars.size());
+    lchars += v;
+    lpairs.push_back((int32_t)lchars.size());
+  }
+  std::string rchars;
+  std::vector<int32_t> rpairs, apairs;
+  std::string achars;
+  for (uint32_t i = 0; i < nn; i++) {
+    rpairs.push_back((int32_t)rchars.size());
+    rchars += names[i];
+    rpairs.push_back((int32_t)rchars.size());
+    const std::string a = std::string("region-") + std::to_string(i % 3);
+    apairs.push_back((int32_t)achars.size());
+    achars += a;
+    apairs.push_back((int32_t)achars.size());
+  }
+  Table* left = new Table();
+  left->columns = {new Column(STRING, nl, (void*)lchars.data(), lpairs.data(), (uint32_t)lchars.size())};
+  left->row_num = nl;
+  Table* right = new Table();
+  right->columns = {new Column(STRING, nn, (void*)rchars.data(), rpairs.data(), (uint32_t)rchars.size()),
+                    new Column(STRING, nn, (void*)achars.data(), apairs.data(), (uint32_t)achars.size())};
+  right->row_num = nn;
+  HashJoinPredicate j;
+  j.join_cols = {{0}, {0}};
+  j.maintain_cols = {{0}, {1}};
+  j.join_types = {{INNER_JOIN, {0u, 1u}}};
+  Table* r = j.process({left, right});
+  CHECK(r != nullptr);
+  if (r) {
+    auto str = [](const Column* c, uint32_t i) {
+      const int32_t* p = (const int32_t*)c->data_ptr_aux;
+      return std::string((const char*)c->data_ptr + p[2 * i], p[2 * i + 1] - p[2 * i]);
+    };
+    std::multiset<std::pair<std::string, std::string>> expect, got;
+    for (uint32_t i = 0; i < nl; i++)
+      if (pick[i] >= 0 && pick[i] < (int)nn)
+        expect.insert({names[pick[i]], std::string("region-") + std::to_string(pick[i] % 3)});
+    bool ok = r->columns.size() == 2 && r->columns[0]->type == STRING && r->columns[1]->type == STRING;
+    for (uint32_t i = 0; ok && i < r->row_num; i++) {
+      got.insert({str(r->columns[0], i), str(r->columns[1], i)});
+      ok = str(r->columns[0], i) == names[pick[j.result_offsets[2 * i]]];
+    }
+    CHECK(ok && got == expect);
+    delete r;
+  }
+  delete left;   // the columns wrap the strings above and own nothing
   delete right;
 }
 
@@ -212,6 +342,7 @@ int main() {
   test_filter();
   test_groupby();
   test_join();
+  test_string_join();
   test_sort();
   if (failures) {
     std::printf("%d checks failed\n", failures);

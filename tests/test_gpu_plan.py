@@ -145,3 +145,87 @@ def test_three_table_chain_with_two_column_keys(ctx):
     (q, _), (rg, _), (cnt, _), (sm, _) = r["columns"]
     assert list(zip(q.tolist(), rg.tolist())) == keys
     assert cnt.tolist() == [exp[k][0] for k in keys] and sm.tolist() == [exp[k][1] for k in keys]
+
+
+def _strings(vals):
+    """A GTables string column from a list of bytes (None = NULL): the bytes
+    packed in row order and int32 [start,end) pairs, -1,-1 for NULL."""
+    blob, pairs, at = bytearray(), [], 0
+    for v in vals:
+        if v is None:
+            pairs += [-1, -1]
+            continue
+        blob += v
+        pairs += [at, at + len(v)]
+        at += len(v)
+    return ("string", bytes(blob), np.array(pairs, dtype=np.int32))
+
+
+def test_string_columns_through_filter_join_groupby_sort(ctx):
+    """STRING columns on the whole chain: a predicate on a STRING column, a
+    join on a STRING key keeping a STRING attribute of the build side, then
+    GROUP BY (attribute, city) and ORDER BY both; the strings come back
+    packed with their pairs the way GPUResult's String[][] is filled."""
+    g = np.random.default_rng(94)
+    n = 200_000
+    cities = [b"AMSTERDAM", b"BERLIN", b"CAIRO", b"CALGARY", b"DELHI", b"", b"\xc3\xa9VORA"]
+    cats = [b"MFGR#%d" % i for i in range(1, 41)]
+    city = [None if x < 0 else cities[x] for x in g.integers(-1, len(cities), n).tolist()]
+    # category keys: NULLs, the 40 categories, and some no dimension row has
+    cat = [None if x < 0 else (cats[x] if x < len(cats) else b"NOPE%d" % x)
+           for x in g.integers(-1, len(cats) + 5, n).tolist()]
+    rev = g.integers(1, 1000, n, dtype=np.int64)
+    dcat = cats[:35]                                        # 5 categories have no dimension row
+    brand = [b"BRAND-%d" % (i % 7) if i % 11 else None for i in range(35)]
+    w = np.arange(35, dtype=np.int32) * 3 - 20
+    gt = GTables([("Map 1", 0, [_strings(city), _strings(cat), rev]),
+                  ("Map 2", 1, [_strings(dcat), _strings(brand), w])])
+    pred = abi.Pred.leaf(abi.FILTER_GE, 0, a="C")           # city >= 'C' (bytes, unsigned)
+    aggs = [(abi.CNT, -1), (abi.SUM, 2), (abi.SUM, 4)]
+    r = run_plan(ctx, gt, 0, [op_filter(pred), op_join(1, 1, 0, build_keep=[1, 2]),   # city cat rev brand w
+                              op_groupby([3, 0], aggs, max_groups=4096), op_sort([0, 1])])
+    dim = {c: (b, int(x)) for c, b, x in zip(dcat, brand, w.tolist())}
+    exp = {}
+    for c, k, v in zip(city, cat, rev.tolist()):
+        if c is None or c < b"C" or k is None or k not in dim:
+            continue
+        b, x = dim[k]
+        key = (b, c)
+        e = exp.get(key, [0, 0, 0])
+        e[0] += 1
+        e[1] += v
+        e[2] += x
+        exp[key] = e
+    # Hive's order: NULLs first ascending, then bytes unsigned, shorter first on a tie
+    keys = sorted(exp, key=lambda t: tuple((0, b"") if x is None else (1, x) for x in t))
+    assert r["rows"] == len(keys)
+    assert r["types"] == [abi.STRING, abi.STRING, abi.LONG, abi.LONG, abi.LONG]
+    (gb, gbn), (gc, _), (cnt, _), (s1, _), (s2, _) = r["columns"]
+    assert list(zip(gb, gc)) == keys
+    assert gbn.tolist() == [k[0] is None for k in keys]
+    assert cnt.tolist() == [exp[k][0] for k in keys]
+    assert s1.tolist() == [exp[k][1] for k in keys] and s2.tolist() == [exp[k][2] for k in keys]
+    assert r["sequence"] == [3, 4, 0, 1, 2] and len(r["stringCols"]) == 2
+
+
+def test_string_join_keys_of_two_columns_and_outer_misses(ctx):
+    """A LEFT OUTER join on (STRING, INT) keys: a probe row without a match
+    keeps its columns and gets NULL build columns, a STRING one included."""
+    g = np.random.default_rng(95)
+    n = 50_000
+    names = [b"n%03d" % i for i in range(60)]
+    pk1 = [names[x] if x >= 0 else None for x in g.integers(-1, 60, n).tolist()]
+    pk2 = g.integers(0, 4, n, dtype=np.int32)
+    bk1 = names[:50] * 3
+    bk2 = np.repeat(np.arange(3, dtype=np.int32), 50)
+    battr = [b"attr-" + x + b"-%d" % y for x, y in zip(bk1, bk2.tolist())]
+    gt = GTables([("Map 1", 0, [_strings(pk1), pk2]), ("Map 2", 2, [_strings(bk1), bk2, _strings(battr)])])
+    r = run_plan(ctx, gt, 0, [op_join([0, 1], 1, [0, 1], build_keep=[2], join_type=abi.LEFT_OUTER_JOIN),
+                              op_sort([0, 1])])
+    look = {(a, b): c for a, b, c in zip(bk1, bk2.tolist(), battr)}
+    rows = [(a, b, None if a is None else look.get((a, b))) for a, b in zip(pk1, pk2.tolist())]
+    rows.sort(key=lambda t: ((0, b"") if t[0] is None else (1, t[0]), t[1]))   # stable, like the sort
+    assert r["rows"] == n
+    (s, _), (i, _), (a, an) = r["columns"]
+    assert list(zip(s, i.tolist(), a)) == rows
+    assert an.tolist() == [t[2] is None for t in rows]
