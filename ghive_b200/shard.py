@@ -1,10 +1,10 @@
 """Host side of running the operators on several GPUs (one rank per GPU).
 
   filter, group-by  each rank takes a contiguous row range (shard_range);
-                    group-by ranks compute mergeable partial aggregates
-                    (AVG travels as SUM + COUNT) and the partials are merged
-                    on one rank (merge_groupby), the all-gather form that suits
-                    small group counts;
+                    group-by ranks compute mergeable partial aggregates on
+                    the device (AVG travels as SUM + COUNT), exchange them by
+                    the hash of their key (one all-to-all per column) and
+                    merge them with the device group-by (groupby_sharded);
   join              the build side is replicated, each rank probes its probe
                     row range; probe row ids are offset by the range start;
   sort              sample sort (sort_sharded): splitters from an all-gathered
@@ -40,68 +40,90 @@ def partial_aggs(aggs):
     return part, where
 
 
-def merge_groupby(parts, aggs, has_key=True):
-    """Merges per-rank partial group-by results.
+def merge_aggs(aggs, first=1):
+    """The aggregates that merge partial_aggs(aggs)[0]'s columns: partial j,
+    column first + j of a table (key, partial 0, partial 1, ...), is summed
+    (SUM, COUNT) or reduced by MIN / MAX."""
+    part, _ = partial_aggs(aggs)
+    return [(abi.SUM if t in (abi.SUM, abi.CNT) else t, first + j) for j, (t, _c) in enumerate(part)]
 
-    parts: per rank (key, vals), key = (values, isnull) or None, vals = list of
-    (values, isnull) for partial_aggs(aggs)[0].  Returns (key, vals) for
-    `aggs`, groups ordered by key (NULL first)."""
-    _, where = partial_aggs(aggs)
-    if has_key:
-        kv = np.concatenate([p[0][0] for p in parts])
-        kn = np.concatenate([np.asarray(p[0][1], bool) for p in parts])
-        ukey = np.where(kn, 0, kv)
-        # NULL keys form their own group, ordered first
-        order = np.lexsort((ukey, ~kn))
-        kv, kn, ukey = kv[order], kn[order], ukey[order]
-        new = np.ones(len(kv), bool)
-        new[1:] = (ukey[1:] != ukey[:-1]) | (kn[1:] != kn[:-1])
-        gid = np.cumsum(new) - 1
-        ng = int(gid[-1]) + 1 if len(gid) else 0
-        key = (kv[new], kn[new])
-    else:
-        order = np.arange(len(parts))
-        gid = np.zeros(len(parts), np.int64)
-        ng = 1
-        key = None
 
-    def col(j):
-        v = np.concatenate([p[1][j][0] for p in parts])[order]
-        n = np.concatenate([np.asarray(p[1][j][1], bool) for p in parts])[order]
-        return v, n
+def groupby_sharded(cols, key_col, aggs, local_groupby, pred=None, group=None):
+    """Filter + GROUP BY over row-sharded columns, one rank per GPU.
 
+    Each rank aggregates its own rows into partial aggregates (local_groupby,
+    the device operator; AVG travels as SUM + COUNT), sends each partial row
+    to the rank that owns its key (the key's 64-bit mix modulo the world size;
+    NULL keys to rank 0) with one all-to-all per column, and merges what it
+    receives with a second local_groupby over the partial rows (SUM of sums
+    and counts, MIN of minima, MAX of maxima).  AVG is the merged SUM over the
+    merged COUNT.  The ranks end up with disjoint sets of groups.
+
+    local_groupby(pred, cols, keys, aggs) -> ((key values, key isnull),
+    [(values, isnull) per aggregate]) with torch tensors on this rank's
+    device (isnull a bool tensor, or None when no row is NULL).
+    key_col None is a global aggregate: every rank's partial row goes to rank
+    0, which returns the one result row (the others return none).
+    Returns (key or None, [(values, isnull) per aggregate of `aggs`])."""
+    import torch
+    import torch.distributed as dist
+
+    from .workloads import mix64_torch
+
+    part, where = partial_aggs(aggs)
+    keyed = key_col is not None
+    key, vals = local_groupby(pred, cols, [key_col] if keyed else [], part)
+    first = vals[0][0] if vals else key[0]
+    dev = first.device
+    g = len(first)
+
+    def nulls(nl):
+        return torch.zeros(g, dtype=torch.bool, device=dev) if nl is None else nl.to(torch.bool)
+
+    columns = ([(key[0], nulls(key[1]))] if keyed else []) + [(v, nulls(n)) for v, n in vals]
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    if world > 1:
+        if keyed:
+            kv = key[0]
+            bits = kv.view(torch.int64) if kv.element_size() == 8 else kv.to(torch.int64)
+            owner = torch.remainder(mix64_torch(bits), world)
+            owner = torch.where(columns[0][1], torch.zeros_like(owner), owner)
+        else:   # a global aggregate: every partial row goes to rank 0
+            owner = torch.zeros(g, dtype=torch.int64, device=dev)
+        order = torch.argsort(owner, stable=True)
+        send = torch.bincount(owner, minlength=world)
+        recv = torch.empty_like(send)
+        dist.all_to_all_single(recv, send, group=group)
+        send_l, recv_l = send.tolist(), recv.tolist()
+        moved = []
+        for v, n in columns:
+            pair = []
+            for t in (v[order].contiguous(), n[order].to(torch.uint8).contiguous()):
+                out = torch.empty(sum(recv_l), dtype=t.dtype, device=dev)
+                dist.all_to_all_single(out, t, recv_l, send_l, group=group)
+                pair.append(out)
+            moved.append((pair[0], pair[1].to(torch.bool)))
+        columns = moved
+    # the owner's merge: GROUP BY the key over the partial rows
+    mkey, mvals = local_groupby(None, columns, [0] if keyed else [], merge_aggs(aggs, 1 if keyed else 0))
+    ng = len(mvals[0][0]) if mvals else len(mkey[0])
     out = []
-    for (t, c), w in zip(aggs, where):
-        v, n = col(w[0])
-        if t in (abi.SUM, abi.CNT, abi.AVG):
-            s = np.zeros(ng, dtype=v.dtype)
-            seen = np.zeros(ng, bool)
-            if v.dtype.kind == "f":
-                np.add.at(s, gid[~n], v[~n])
-            else:
-                # int64 sums wrap like Hive's
-                np.add.at(s.view(np.uint64), gid[~n], v[~n].view(np.uint64))
-            np.logical_or.at(seen, gid[~n], True)
-            if t == abi.AVG:
-                cv, cn = col(w[1])
-                cnt = np.zeros(ng, np.int64)
-                np.add.at(cnt, gid[~cn], cv[~cn])
-                avg = np.where(cnt > 0, s / np.maximum(cnt, 1), 0.0)
-                out.append((avg, cnt == 0))
-            elif t == abi.CNT:
-                out.append((s, np.zeros(ng, bool)))
-            else:
-                out.append((s, ~seen))
+    for (t, _c), w in zip(aggs, where):
+        v, n = mvals[w[0]]
+        n = torch.zeros(ng, dtype=torch.bool, device=v.device) if n is None else n.to(torch.bool)
+        if t == abi.AVG:
+            cnt, _ = mvals[w[1]]
+            empty = cnt == 0
+            avg = torch.where(empty, torch.zeros_like(v, dtype=torch.float64),
+                              v.to(torch.float64) / torch.clamp(cnt, min=1).to(torch.float64))
+            out.append((avg, empty))
+        elif t == abi.CNT:
+            out.append((v, torch.zeros(ng, dtype=torch.bool, device=v.device)))
         else:
-            fill = np.inf if v.dtype.kind == "f" else np.iinfo(v.dtype).max
-            if t == abi.MAX:
-                fill = -np.inf if v.dtype.kind == "f" else np.iinfo(v.dtype).min
-            r = np.full(ng, fill, dtype=v.dtype)
-            (np.minimum if t == abi.MIN else np.maximum).at(r, gid[~n], v[~n])
-            seen = np.zeros(ng, bool)
-            np.logical_or.at(seen, gid[~n], True)
-            out.append((r, ~seen))
-    return key, out
+            out.append((v, n))
+    if not keyed and world > 1 and dist.get_rank(group) != 0:
+        return None, [(v[:0], n[:0]) for v, n in out]   # rank 0 holds the one row
+    return (mkey if keyed else None), out
 
 
 # ------------------------------------------------------------ sample sort

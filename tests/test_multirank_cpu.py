@@ -24,19 +24,37 @@ def _port():
         return s.getsockname()[1]
 
 
-def _groupby_rank(rank, world, port, q):
-    import torch.distributed as dist
+def _oracle_local_groupby(pred, cols, keys, aggs):
+    """One rank's group-by over its columns (torch CPU tensors or (values,
+    isnull) pairs): the CPU oracle here, the device operator on a GPU."""
+    import torch
 
     from oracle import oracle
+
+    def np_col(c):
+        return (c[0].numpy(), c[1].numpy().astype(bool)) if isinstance(c, tuple) else c.numpy()
+    k, v = oracle.filter_groupby(pred, [np_col(c) for c in cols], keys, aggs)
+    key = (torch.from_numpy(k[0][0]), torch.from_numpy(k[0][1])) if keys else None
+    return key, [(torch.from_numpy(a), torch.from_numpy(b)) for a, b in v]
+
+
+def _groupby_rank(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         cols = workloads.fact_table(200_003, seed_idx=51, groups=700)
         lo, hi = shard.shard_range(len(cols[0]), rank, world)
-        part, _ = shard.partial_aggs(workloads.AGGS_FACT)
-        k, v = oracle.filter_groupby(workloads.fact_predicate(), [c[lo:hi] for c in cols], [0], part)
+        mine = [torch.from_numpy(c[lo:hi]) for c in cols]
+        key, vals = shard.groupby_sharded(mine, 0, workloads.AGGS_FACT, _oracle_local_groupby,
+                                          pred=workloads.fact_predicate())
+        _, gvals = shard.groupby_sharded(mine, None, [(abi.SUM, 1), (abi.MIN, 3), (abi.AVG, 2)],
+                                         _oracle_local_groupby)
+        res = ((key[0].numpy(), key[1].numpy()), [(v.numpy(), n.numpy()) for v, n in vals],
+               [(v.numpy(), n.numpy()) for v, n in gvals])
         gathered = [None] * world
-        dist.all_gather_object(gathered, (k[0], v))
+        dist.all_gather_object(gathered, res)
         if rank == 0:
             q.put(gathered)
         dist.barrier()
@@ -140,19 +158,36 @@ def test_shard_ranges_cover_rows_once():
             assert max(h - l for l, h in got) - min(h - l for l, h in got) <= 1
 
 
-def test_sharded_groupby_merges_to_the_whole():
-    from oracle import oracle
-    gathered = _spawn(_groupby_rank)
-    key, vals = shard.merge_groupby([(k, v) for k, v in gathered], workloads.AGGS_FACT)
-    cols = workloads.fact_table(200_003, seed_idx=51, groups=700)
-    ek, ev = oracle.filter_groupby(workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT)
-    assert np.array_equal(key[0], ek[0][0]) and np.array_equal(key[1], ek[0][1])
-    for j, ((gv, gn), (xv, xn)) in enumerate(zip(vals, ev)):
+def _check_cols(got, exp):
+    for j, ((gv, gn), (xv, xn)) in enumerate(zip(got, exp)):
         assert np.array_equal(gn, xn), j
         if xv.dtype.kind == "f":
             assert np.all(np.abs(gv[~gn] - xv[~xn]) <= REL_TOL * np.abs(xv[~xn])), j
         else:
             assert np.array_equal(gv[~gn].astype(xv.dtype), xv[~xn]), j
+
+
+def test_sharded_groupby_merges_to_the_whole():
+    """Two ranks aggregate their halves, exchange the partial rows by the
+    hash of their key and merge them: the union of the ranks' groups is the
+    oracle's result over all rows, each group on exactly one rank; the global
+    aggregate's one row is on rank 0."""
+    from oracle import oracle
+    gathered = _spawn(_groupby_rank)
+    kv = np.concatenate([g[0][0] for g in gathered])
+    kn = np.concatenate([g[0][1] for g in gathered])
+    vals = [(np.concatenate([g[1][j][0] for g in gathered]), np.concatenate([g[1][j][1] for g in gathered]))
+            for j in range(len(workloads.AGGS_FACT))]
+    assert all(len(g[0][0]) > 0 for g in gathered)    # both ranks own groups
+    order = np.lexsort((np.where(kn, 0, kv), ~kn))
+    cols = workloads.fact_table(200_003, seed_idx=51, groups=700)
+    ek, ev = oracle.filter_groupby(workloads.fact_predicate(), cols, [0], workloads.AGGS_FACT)
+    assert np.array_equal(kv[order], ek[0][0]) and np.array_equal(kn[order], ek[0][1])
+    _check_cols([(v[order], n[order]) for v, n in vals], ev)
+    gaggs = [(abi.SUM, 1), (abi.MIN, 3), (abi.AVG, 2)]
+    _, gv = oracle.filter_groupby(None, cols, [], gaggs)
+    assert len(gathered[0][2][0][0]) == 1 and len(gathered[1][2][0][0]) == 0
+    _check_cols(gathered[0][2], gv)
 
 
 def test_sharded_join_probe_unions_to_the_whole():
@@ -196,20 +231,6 @@ def test_order_image_is_monotone():
     img = shard.order_image(torch.from_numpy(iv), None, True, False).numpy()
     o = np.argsort(-iv, kind="stable")
     assert np.all(np.diff(img[o]) >= 0)
-
-
-def test_global_aggregate_partials_merge():
-    parts = []
-    g = np.random.default_rng(3)
-    allv = []
-    for _ in range(3):
-        v = g.integers(-10, 10, 100).astype(np.int64)
-        allv.append(v)
-        parts.append((None, [(np.array([v.sum()]), np.array([False])),
-                             (np.array([v.min()]), np.array([False]))]))
-    _, vals = shard.merge_groupby(parts, [(abi.SUM, 0), (abi.MIN, 0)], has_key=False)
-    a = np.concatenate(allv)
-    assert vals[0][0][0] == a.sum() and vals[1][0][0] == a.min()
 
 
 if __name__ == "__main__":
