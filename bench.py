@@ -531,11 +531,16 @@ def bench_sort(ctx, args, dev, stream, peak, peak_kind):
     for zipf in (False, True):
         d, k, rowid = workloads.sort_table(N_SORT, zipf=zipf, seed_idx=2)
         dd, dk, dr = (torch.from_numpy(x).to(dev) for x in (d, k, rowid))
+        # the outputs (d, k, row id; the inputs hold no NULLs, so no NULL maps)
+        # made once, as the join's are
+        from ghive_b200.ops import _Outs
+        souts = (_Outs([abi.INT, abi.LONG], N_SORT, dev, with_nulls=False),
+                 _Outs([abi.INT], N_SORT, dev, with_nulls=False))
         for _ in range(max(1, args.warmup)):
-            ctx.sort([dd, dk], payload=[dr], sync=False)
+            ctx.sort([dd, dk], payload=[dr], sync=False, outs=souts)
         ctx.sync()
         l0 = ctx.launches
-        ctx.sort([dd, dk], payload=[dr], sync=False)
+        ctx.sort([dd, dk], payload=[dr], sync=False, outs=souts)
         ctx.sync()
         # the sort launches a min/max and a histogram kernel, then one kernel
         # per executed radix pass
@@ -544,7 +549,7 @@ def bench_sort(ctx, args, dev, stream, peak, peak_kind):
         for _ in range(max(3, min(args.steps, 10))):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            ctx.sort([dd, dk], payload=[dr], sync=False)
+            ctx.sort([dd, dk], payload=[dr], sync=False, outs=souts)
             b.record(stream)
             times.append((a, b))
         ctx.sync()
@@ -959,7 +964,7 @@ def run_profile_case(case, reps):
         d, k, r = workloads.sort_table(20_000_000, seed_idx=2)
         dd, dk, dr = (torch.from_numpy(x).to(dev) for x in (d, k, r))
         for _ in range(reps):
-            ctx.sort([dd, dk], payload=[dr])
+            ctx.sort([dd, dk], payload=[dr], with_nulls=False)
         print("sorted")
     elif case == "batch":
         specs = workloads.batched_specs(64, seed_idx=3, max_rows=2_000_000)

@@ -104,28 +104,61 @@ struct MinMaxParams {
 
 __global__ void __launch_bounds__(256) sort_minmax_kernel(MinMaxParams p) {
   constexpr int U = 4;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int j = 0; j < p.K.nkeys; j++) {
     const KeyField& f = p.K.k[j];
     unsigned long long mn = ~0ull, mx = 0, anynull = 0;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < p.n; base += U * stride) {
-      int64_t raw[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        int64_t r = base + u * stride;
-        raw[u] = r < p.n ? ld_raw(f.col, r) : 0;
+    auto fold = [&](int64_t raw, int64_t r) {
+      if (f.col.null_mode != GHB_NULLS_NONE && raw_is_null(f.col, raw, r)) {
+        anynull = 1;
+        return;
       }
+      uint64_t img = key_image(f.col, raw);
+      if (f.desc) img = ~img;
+      mn = min(mn, (unsigned long long)img);
+      mx = max(mx, (unsigned long long)img);
+    };
+    // 16-byte loads, U of them in flight per thread (a column read once,
+    // evict-first); rows past the last whole vector, and columns with a NULL
+    // map or an unaligned base, one value at a time
+    int64_t done = 0;
+    if (f.col.null_mode != GHB_NULLS_BYTEMAP && ((uintptr_t)f.col.data & 15) == 0) {
+      if (f.col.type == GHB_INT) {
+        const int4* v = (const int4*)f.col.data;
+        const int64_t nv = p.n / 4;
+        for (int64_t b = tid; b < nv; b += U * stride) {
+          int4 x[U];
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        int64_t r = base + u * stride;
-        if (r >= p.n) continue;
-        if (f.col.null_mode != GHB_NULLS_NONE && raw_is_null(f.col, raw[u], r)) { anynull = 1; continue; }
-        uint64_t img = key_image(f.col, raw[u]);
-        if (f.desc) img = ~img;
-        mn = min(mn, (unsigned long long)img);
-        mx = max(mx, (unsigned long long)img);
+          for (int u = 0; u < U; u++) x[u] = b + u * stride < nv ? __ldcs(v + b + u * stride) : make_int4(0, 0, 0, 0);
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            if (b + u * stride >= nv) continue;
+            fold(x[u].x, 0);
+            fold(x[u].y, 0);
+            fold(x[u].z, 0);
+            fold(x[u].w, 0);
+          }
+        }
+        done = nv * 4;
+      } else {
+        const longlong2* v = (const longlong2*)f.col.data;
+        const int64_t nv = p.n / 2;
+        for (int64_t b = tid; b < nv; b += U * stride) {
+          longlong2 x[U];
+#pragma unroll
+          for (int u = 0; u < U; u++) x[u] = b + u * stride < nv ? __ldcs(v + b + u * stride) : make_longlong2(0, 0);
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            if (b + u * stride >= nv) continue;
+            fold(x[u].x, 0);
+            fold(x[u].y, 0);
+          }
+        }
+        done = nv * 2;
       }
     }
+    for (int64_t r = done + tid; r < p.n; r += stride) fold(ld_raw(f.col, r), r);
     for (int o = 16; o > 0; o >>= 1) {
       mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
       mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));

@@ -390,11 +390,17 @@ class Context:
                 "build": ob.rows(m), "probe": op.rows(m)}
 
     def sort(self, keys, orders=None, null_orders=None, payload=(), rowid=False, stream=None,
-             sync=True):
+             sync=True, with_nulls=True, outs=None):
+        """ORDER BY on device columns.  with_nulls=False leaves out the
+        outputs' NULL maps (NULLs then carry their sentinels); outs = (key
+        outputs, payload outputs) reuses output columns made earlier."""
         ks, ps = _Cols(keys), _Cols(payload)
         n = ks[0].n
-        ok = _Outs([ks[j].type for j in range(ks.n)], n, self.torch_device)
-        op = _Outs([ps[j].type for j in range(ps.n)], n, self.torch_device)
+        if outs is not None:
+            ok, op = outs
+        else:
+            ok = _Outs([ks[j].type for j in range(ks.n)], n, self.torch_device, with_nulls=with_nulls)
+            op = _Outs([ps[j].type for j in range(ps.n)], n, self.torch_device, with_nulls=with_nulls)
         rid = torch.empty(max(1, n), dtype=torch.int32, device=self.torch_device) if rowid else None
         o = (C.c_int32 * ks.n)(*(orders or [abi.ASC] * ks.n))
         no = (C.c_int32 * ks.n)(*(null_orders or [abi.NULLS_DEFAULT] * ks.n))

@@ -28,15 +28,19 @@ def shard_range(n, rank, world):
 
 def partial_aggs(aggs):
     """The per-rank aggregates for `aggs` and, per original aggregate, the
-    indices of its partials: AVG(c) becomes SUM(c) and COUNT(c)."""
+    indices of its partials: AVG(c) becomes SUM(c) and COUNT(c).  A partial
+    two aggregates need (SUM(c) for both SUM(c) and AVG(c)) is computed once."""
     part, where = [], []
+
+    def index(a):
+        if a not in part:
+            part.append(a)
+        return part.index(a)
     for t, c in aggs:
         if t == abi.AVG:
-            where.append((len(part), len(part) + 1))
-            part += [(abi.SUM, c), (abi.CNT, c)]
+            where.append((index((abi.SUM, c)), index((abi.CNT, c))))
         else:
-            where.append((len(part),))
-            part.append((t, c))
+            where.append((index((t, c)),))
     return part, where
 
 
@@ -104,8 +108,14 @@ def groupby_sharded(cols, key_col, aggs, local_groupby, pred=None, group=None):
                 pair.append(out)
             moved.append((pair[0], pair[1].to(torch.bool)))
         columns = moved
-    # the owner's merge: GROUP BY the key over the partial rows
-    mkey, mvals = local_groupby(None, columns, [0] if keyed else [], merge_aggs(aggs, 1 if keyed else 0))
+    # the owner's merge: GROUP BY the key over the partial rows (a COUNT
+    # partial is never NULL: it goes without a NULL map, so its merge needs
+    # no non-NULL count)
+    off = 1 if keyed else 0
+    for j, (t, _c) in enumerate(part):
+        if t == abi.CNT:
+            columns[off + j] = columns[off + j][0]
+    mkey, mvals = local_groupby(None, columns, [0] if keyed else [], merge_aggs(aggs, off))
     ng = len(mvals[0][0]) if mvals else len(mkey[0])
     out = []
     for (t, _c), w in zip(aggs, where):
