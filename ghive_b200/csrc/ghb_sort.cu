@@ -228,15 +228,74 @@ struct HistParams {
   int32_t vals_wide;         // values are 64-bit (else 32-bit)
   int32_t carry_rowid;       // value = row index (else the single payload's raw bits)
   ghb_column pay_src;
+  int32_t vec;               // every column read has 16-byte aligned data and no NULL map
 };
+
+// Rows r..r+3 (r a multiple of 4) of a column with 16-byte aligned data, as
+// raw 64-bit values, by 16-byte loads read once.
+__device__ __forceinline__ void load4(const ghb_column& c, int64_t r, int64_t raw[4]) {
+  if (c.type == GHB_INT) {
+    const int4 x = __ldcs((const int4*)c.data + r / 4);
+    raw[0] = x.x;
+    raw[1] = x.y;
+    raw[2] = x.z;
+    raw[3] = x.w;
+  } else {
+    const longlong2* q = (const longlong2*)c.data + r / 2;
+    const longlong2 a = __ldcs(q), b = __ldcs(q + 1);
+    raw[0] = a.x;
+    raw[1] = a.y;
+    raw[2] = b.x;
+    raw[3] = b.y;
+  }
+}
 
 __global__ void __launch_bounds__(256) sort_hist_kernel(HistParams p) {
   constexpr int U = 4;
   __shared__ uint32_t sh[kMaxPasses][kBins];
   for (int i = threadIdx.x; i < kMaxPasses * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < p.n; base += U * stride) {
+  // four consecutive rows per thread by 16-byte loads and stores, then the
+  // rows past the last group of four (or all rows) one at a time
+  int64_t done = 0;
+  if (p.vec) {
+    const int64_t ng = p.n / 4;
+    for (int64_t g = tid; g < ng; g += stride) {
+      const int64_t r = g * 4;
+      uint64_t k[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int i = 0; i < kMaxSub; i++) {
+        if (i >= p.seg.n) break;
+        const SubPlan& sp = p.sub[i];
+        int64_t raw[4];
+        load4(sp.col, r, raw);
+#pragma unroll
+        for (int u = 0; u < 4; u++) k[u] |= sub_bits_plan(sp, raw[u], r + u);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        for (int q = 0; q < p.npasses; q++) atomicAdd(&sh[q][(k[u] >> (q * kDigitBits)) & (kBins - 1)], 1u);
+      if (p.keys_out) {
+        ulonglong2* ko = (ulonglong2*)(p.keys_out + r);
+        __stcs(ko, make_ulonglong2(k[0], k[1]));
+        __stcs(ko + 1, make_ulonglong2(k[2], k[3]));
+        int64_t v[4] = {r, r + 1, r + 2, r + 3};
+        if (!p.carry_rowid) load4(p.pay_src, r, v);
+        if (p.vals_wide) {
+          ulonglong2* vo = (ulonglong2*)p.vals_out + r / 2;
+          __stcs(vo, make_ulonglong2((unsigned long long)v[0], (unsigned long long)v[1]));
+          __stcs(vo + 1, make_ulonglong2((unsigned long long)v[2], (unsigned long long)v[3]));
+        } else {
+          __stcs((uint4*)p.vals_out + r / 4,
+                 make_uint4((unsigned)v[0], (unsigned)v[1], (unsigned)v[2], (unsigned)v[3]));
+        }
+      }
+    }
+    done = ng * 4;
+  }
+  for (int64_t base = done + tid; base < p.n; base += U * stride) {
     uint64_t k[U];
 #pragma unroll
     for (int u = 0; u < U; u++) k[u] = 0;
@@ -339,22 +398,9 @@ __device__ __forceinline__ void gather_write(const PassParams& p, int64_t row, i
   }
 }
 
-// Unpacks a one-segment key (and the carried value) to output position `pos`.
-// The key loop has constant indices (unrolled over the most keys), so the
-// per-key fields are read straight from the parameter space.
-__device__ __forceinline__ void decode_write(const PassParams& p, uint64_t k, uint64_t v, int64_t pos) {
-#pragma unroll
-  for (int j = 0; j < kMaxSortKeys; j++) {
-    if (j >= p.K.nkeys) break;
-    const KeyField& kf = p.K.k[j];
-    const int vb = p.dec_vbits[j];
-    const uint64_t field = vb == 0 ? 0 : (k >> p.dec_vshift[j]) & (vb >= 64 ? ~0ull : ((1ull << vb) - 1));
-    const bool null = p.dec_fshift[j] >= 0 && (((k >> p.dec_fshift[j]) & 1ull) == 0) == (bool)kf.nulls_first;
-    uint64_t u = field + kf.umin;
-    if (kf.desc) u = ~u;
-    int64_t raw = kf.col.type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(u) : (int64_t)(u ^ 0x8000000000000000ull);
-    write_raw(p.out_keys[j], pos, kf.col.type, raw, null);
-  }
+// The carried value of a decoded row: its row index (row id output and
+// payloads gathered by it), or the single payload itself.
+__device__ __forceinline__ void decode_value(const PassParams& p, uint64_t v, int64_t pos) {
   if (p.carry_rowid) {
     int64_t row = (int64_t)v;
     if (p.out_rowid) p.out_rowid[pos] = (int32_t)row;
@@ -532,13 +578,40 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
     __syncthreads();
     // write runs: element i of the reordered tile goes to gbase[d] + (i - bexcl[d])
     const int64_t tile_n = min((int64_t)kSortTile, p.n - tile * kSortTile);
+    if (DST == kDstDecode) {
+      // one key column at a time, its decoding parameters held in registers,
+      // then the carried values
+      for (int j = 0; j < p.K.nkeys; j++) {
+        const KeyField& kf = p.K.k[j];
+        const int vb = p.dec_vbits[j], vs = p.dec_vshift[j], fs = p.dec_fshift[j];
+        const uint64_t vmask = vb == 0 ? 0 : (vb >= 64 ? ~0ull : ((1ull << vb) - 1));
+        const uint64_t umin = kf.umin;
+        const bool desc = kf.desc, nf = kf.nulls_first;
+        const int type = kf.col.type;
+        const ghb_out_column o = p.out_keys[j];
+        for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
+          const uint64_t k = s_keys[i];
+          const uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
+          const int64_t pos = (int64_t)(s_gbase[dk] + (i - s_bexcl[dk]));
+          const bool null = fs >= 0 && (((k >> fs) & 1ull) == 0) == nf;
+          uint64_t u = (vb == 0 ? 0 : (k >> vs) & vmask) + umin;
+          if (desc) u = ~u;
+          const int64_t raw = type == GHB_DOUBLE ? (int64_t)unflip_f64_bits(u) : (int64_t)(u ^ 0x8000000000000000ull);
+          write_raw(o, pos, type, raw, null);
+        }
+      }
+      for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
+        const uint64_t k = s_keys[i];
+        const uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
+        const int64_t pos = (int64_t)(s_gbase[dk] + (i - s_bexcl[dk]));
+        decode_value(p, (uint64_t)s_vals[i], pos);
+      }
+    } else
     for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
       uint64_t k = s_keys[i];
       uint32_t dk = (uint32_t)(k >> p.shift) & (kBins - 1);
       int64_t pos = (int64_t)(s_gbase[dk] + (i - s_bexcl[dk]));
-      if (DST == kDstDecode) {
-        decode_write(p, k, (uint64_t)s_vals[i], pos);
-      } else if (DST == kDstGather) {
+      if (DST == kDstGather) {
         gather_write(p, (int64_t)s_vals[i], pos);
       } else {
         __stcs((unsigned long long*)p.keys_out + pos, (unsigned long long)k);
@@ -802,7 +875,15 @@ int32_t sort_impl(ghb_ctx* ctx, const ghb_column* keys, const int32_t* orders,
     hp.vals_wide = wide ? 1 : 0;
     hp.carry_rowid = carry_rowid ? 1 : 0;
     hp.pay_src = carry_rowid ? ghb_column{} : payload[0];
-    sort_hist_kernel<<<std::min(grid, ctx->num_sms * 4), 256, 0, stream>>>(hp);
+    // 16-byte loads and stores when every column read allows them
+    auto vec_ok = [](const ghb_column& c) {
+      return c.null_mode != GHB_NULLS_BYTEMAP && ((uintptr_t)c.data & 15) == 0;
+    };
+    hp.vec = 1;
+    for (int i = 0; i < segs[s].n; i++) hp.vec &= vec_ok(hp.sub[i].col) ? 1 : 0;
+    if (!carry_rowid) hp.vec &= vec_ok(hp.pay_src) ? 1 : 0;
+    if (hp.keys_out && (((uintptr_t)hp.keys_out | (uintptr_t)hp.vals_out) & 15)) hp.vec = 0;
+    sort_hist_kernel<<<std::min(grid, ctx->num_sms * 8), 256, 0, stream>>>(hp);
     GHB_LAUNCH_CHECK(ctx);
   }
   std::vector<uint32_t> hist((size_t)segs.size() * kMaxPasses * kBins, 0);
