@@ -340,6 +340,7 @@ def run_ours(args, world, rank, local):
 
     lines = []
     if world == 1 and not args.headline_only:
+        lines.append(bench_filter(ctx, args, dev, stream, peak, peak_kind))
         lines.append(bench_groupby(ctx, args, dev, stream, peak, peak_kind))
         lines.append(bench_join_hashed(ctx, args, dev, stream, peak, peak_kind))
         lines.append(bench_sort(ctx, args, dev, stream, peak, peak_kind))
@@ -405,6 +406,69 @@ def _double_errors(gpu_keys, gpu_aggs, ok, comp, out_types):
     return {"results": int(e.size), "max_rel": float(e.max()) if e.size else None,
             "median_rel": float(np.median(e)) if e.size else None,
             "reference": "FP64 Neumaier compensated sum per group (CPU oracle)"}
+
+
+def bench_filter(ctx, args, dev, stream, peak, peak_kind):
+    """The filter alone on the fact table: d < 1263 over 6M rows, the four
+    columns of each passing row written out in order."""
+    import torch
+
+    from ghive_b200 import abi, workloads
+    from ghive_b200.ops import _Outs
+    cols = workloads.fact_table(N_FACT, seed_idx=0)
+    dcols = [torch.from_numpy(c).to(dev) for c in cols]
+    pred = workloads.fact_predicate()
+    types = [abi.INT, abi.LONG, abi.DOUBLE, abi.INT]
+    outs = _Outs(types, N_FACT, dev, with_nulls=False)
+    flush = torch.zeros(64 << 20, dtype=torch.float32, device=dev)  # 256 MB
+    for _ in range(args.warmup):
+        ctx.filter(pred, dcols, outs=outs, sync=False)
+    ctx.sync()
+    times = []
+    for _ in range(max(args.steps, 10)):
+        flush_l2(flush)
+        torch.cuda._sleep(300_000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _, d_rows = ctx.filter(pred, dcols, outs=outs, sync=False)
+        b.record(stream)
+        times.append((a, b))
+    ctx.sync()
+    rows = int(d_rows.item())
+    ms = statistics.median(x.elapsed_time(y) for x, y in times)
+    nbytes = N_FACT * 24 + rows * 24
+    # e2e: pinned host columns through ghb_filter_host
+    hcols = [pinned(c) for c in cols]
+    ctx.filter_host(pred, hcols)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        ctx.filter_host(pred, hcols)
+    e2e_ms = (time.perf_counter() - t0) / 5 * 1e3
+    out = {"op": "filter",
+           "workload": "filter d<1263 over the 6M-row fact table (k i32, qty i64, price f64, d i32), "
+                       "the passing rows' four columns written in order",
+           "value": N_FACT / (ms / 1e3), "unit": "rows/s", "ms": ms, "rows_out": rows,
+           "roofline": roofline(nbytes, ms, peak, peak_kind,
+                                kernel="filter_kernel (predicate, ballots, look-back, gather)",
+                                l2="flushed before each launch"),
+           "e2e": {"value": N_FACT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+                   "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)),
+                   "d2h_bytes_per_step": int(rows * 24 + 8),
+                   "api": "ghb_filter_host (pinned host columns; outputs allocated per call)"}}
+    if not args.no_cpu:
+        from oracle import oracle
+        import numpy as np
+
+        def cpu():
+            sel = oracle.filter_rows(pred, cols)
+            return [np.take(c, sel) for c in cols]
+        t1, _ = timed_cpu(cpu)
+        out["cpu_baseline"] = {"value": N_FACT / t1, "unit": "rows/s", "cores": 1, "kind": "port",
+                               "sample": "the whole 6M-row workload: Hive's filter restated in C++ "
+                                         "(selected rows), then the projected columns gathered"}
+    del dcols, flush, outs
+    torch.cuda.empty_cache()
+    return out
 
 
 def bench_groupby(ctx, args, dev, stream, peak, peak_kind):
@@ -934,6 +998,7 @@ def run_profile_case(case, reps):
     the operator run `reps` times so a capture can skip the first, cold
     launch), for ncu captures:
 
+      filter   filter d < 1263 over the 6M-row fact table, four columns out
       groupby  filter d < 1263 + GROUP BY k over the 6M-row fact table
       gbcnt    the same table, COUNT(*) only
       join     1.5M-key build, 20M-row probe, int64 + double build payloads
@@ -958,6 +1023,11 @@ def run_profile_case(case, reps):
         for _ in range(reps):
             ctx.join_probe(t, df, abi.INNER_JOIN, capacity=20_000_000, rowids=False, outs=outs)
         print("rows", int(outs[4].item()))
+    elif case == "filter":
+        cols = [torch.from_numpy(c).to(dev) for c in workloads.fact_table(N_FACT, seed_idx=0)]
+        for _ in range(reps):
+            _, k = ctx.filter(workloads.fact_predicate(), cols, with_nulls=False)
+        print("rows", k)
     elif case in ("groupby", "gbcnt"):
         cols = [torch.from_numpy(c).to(dev) for c in workloads.fact_table(N_FACT, seed_idx=0)]
         aggs = workloads.AGGS_FACT if case == "groupby" else [(abi.CNT, -1)]

@@ -59,7 +59,10 @@ __device__ __forceinline__ void copy_value(const ghb_column& c, const ghb_out_co
   }
 }
 
-__global__ void __launch_bounds__(kFiltThreads) filter_kernel(FilterParams p) {
+// The parameters stay in the constant bank (__grid_constant__): the string
+// leaves' out-of-line compare takes references into them, which would
+// otherwise copy the whole parameter block to every thread's stack.
+__global__ void __launch_bounds__(kFiltThreads) filter_kernel(const __grid_constant__ FilterParams p) {
   __shared__ int64_t s_tile;
   __shared__ uint32_t s_warp_cnt[kFiltItems][kFiltThreads / 32];
   __shared__ uint32_t s_warp_off[kFiltItems][kFiltThreads / 32];

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(TH) join_count_direct_kernel(ProbeParams p) {
 // TH threads x IT rows per thread = one chunk (kChunk rows) per iteration.
 // Four 256-thread CTAs per SM (64 registers): more key and table loads in flight.
 template <int TH, int IT, bool KEY_INT, bool NULLABLE>
-__global__ void __launch_bounds__(TH, 1024 / TH) join_count_kernel(ProbeParams p) {
+__global__ void __launch_bounds__(TH, TH == 512 ? 2 : TH == 256 ? 4 : 1) join_count_kernel(ProbeParams p) {
   constexpr int kJThreads = TH, kJItems = IT;
   static_assert(TH * IT == kChunk, "a CTA iteration covers one chunk");
   const int lane = threadIdx.x & 31;

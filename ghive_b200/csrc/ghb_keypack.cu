@@ -191,7 +191,9 @@ __global__ void __launch_bounds__(256) string_rep_kernel(ghb_column c, const int
   }
 }
 
-__global__ void __launch_bounds__(256) predicate_pass_kernel(PredProg prog, ColSet cs, int64_t n, int32_t* pass) {
+__global__ void __launch_bounds__(256) predicate_pass_kernel(const __grid_constant__ PredProg prog,
+                                                              const __grid_constant__ ColSet cs, int64_t n,
+                                                              int32_t* pass) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
     pass[r] = eval_pred(prog, cs, r) ? 1 : 0;
 }

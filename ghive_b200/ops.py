@@ -261,15 +261,19 @@ class Context:
                                           float(peak_gbs)))
 
     # ------------------------------------------------------------ device ops
-    def filter(self, pred, cols, proj=None, capacity=None, stream=None, sync=True):
+    def filter(self, pred, cols, proj=None, capacity=None, stream=None, sync=True, with_nulls=True,
+               outs=None):
         """FilterPredicate::process + FilterOperator::clean_data on device columns.
+        with_nulls=False leaves out the outputs' NULL maps; outs reuses output
+        columns made earlier (an _Outs of the projected types).
 
         Returns ([(values, isnull)] per projected column, row count tensor or int)."""
         cs = _Cols(cols)
         n = cs[0].n if cs.n else 0
         proj = list(range(cs.n)) if proj is None else list(proj)
         cap = n if capacity is None else capacity
-        outs = _Outs([cs[j].type for j in proj], cap, self.torch_device)
+        if outs is None:
+            outs = _Outs([cs[j].type for j in proj], cap, self.torch_device, with_nulls=with_nulls)
         pa = (C.c_int32 * max(1, len(proj)))(*proj)
         d_rows = torch.zeros(1, dtype=torch.int64, device=self.torch_device)
         pp, keep = _pred(pred)
