@@ -201,6 +201,11 @@ int32_t string_rep_rows(ghb_ctx* ctx, const ghb_column& c, const int32_t* pass, 
 // component is NULL and matches nothing).  GHB_ERR_UNSUPPORTED past 63 bits.
 int32_t keypack_join(ghb_ctx* ctx, const ghb_column* a, const ghb_column* b, int32_t nkeys, int64_t* a_packed,
                      uint8_t* a_null, int64_t* b_packed, uint8_t* b_null, cudaStream_t stream);
+// Exclusive prefix sums of n int64 counts, in place; their total to the
+// device word *d_total.  One CTA for a few thousand counts, else tiles of
+// 1024 claimed in order with decoupled look-back (bounded by the context's
+// spin limit).
+int32_t scan_counts(ghb_ctx* ctx, int64_t* counts, int64_t n, int64_t* d_total, cudaStream_t stream);
 // pass[r] = 1 when row r passes the predicate program, else 0.
 int32_t predicate_pass(ghb_ctx* ctx, const PredProg& prog, const ghb_column* cols, int32_t ncols, int64_t n,
                        int32_t* pass, cudaStream_t stream);

@@ -946,6 +946,28 @@ size_t join_probe_scratch_bytes(int64_t n) {
          (((size_t)std::max<int64_t>(nchunks, 1) * 16 * 8 + 255) & ~(size_t)255) + 512;
 }
 
+int32_t scan_counts(ghb_ctx* ctx, int64_t* counts, int64_t n, int64_t* d_total, cudaStream_t stream) {
+  if (n <= 4096) {
+    join_scan_kernel<<<1, 1024, 0, stream>>>(counts, n, d_total);
+  } else {
+    ScanParams sp;
+    sp.counts = counts;
+    sp.n = n;
+    sp.ntiles = (n + 1023) / 1024;
+    sp.d_total = d_total;
+    const int32_t st = lookback_prepare(ctx, sp.ntiles, &sp.epoch, stream);
+    if (st) return st;
+    sp.lb = ctx->lb_status;
+    sp.counters = ctx->d_counters;
+    sp.status = ctx->d_status;
+    sp.spin_limit = ctx->spin_limit;
+    const int sgrid = (int)std::min<int64_t>(sp.ntiles, (int64_t)ctx->num_sms);
+    join_scan_lb_kernel<<<sgrid, 1024, 0, stream>>>(sp);
+  }
+  GHB_LAUNCH_CHECK(ctx);
+  return GHB_OK;
+}
+
 int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column* probe_key,
                         int32_t join_type, ghb_out_column* out_build, const ghb_column* probe_payload,
                         int32_t npp, ghb_out_column* out_probe, int32_t* out_probe_rowid,
@@ -1043,23 +1065,7 @@ int32_t join_probe_impl(ghb_ctx* ctx, const ghb_join_table* t, const ghb_column*
   grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   count_direct<<<grid, threads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
-  if (nunits <= 4096) {
-    join_scan_kernel<<<1, 1024, 0, stream>>>(p.chunk_count, nunits, d_out_rows);
-  } else {
-    ScanParams sp;
-    sp.counts = p.chunk_count;
-    sp.n = nunits;
-    sp.ntiles = (nunits + 1023) / 1024;
-    sp.d_total = d_out_rows;
-    if ((st = lookback_prepare(ctx, sp.ntiles, &sp.epoch, stream))) return st;
-    sp.lb = ctx->lb_status;
-    sp.counters = ctx->d_counters;
-    sp.status = ctx->d_status;
-    sp.spin_limit = ctx->spin_limit;
-    const int sgrid = (int)std::min<int64_t>(sp.ntiles, (int64_t)ctx->num_sms);
-    join_scan_lb_kernel<<<sgrid, 1024, 0, stream>>>(sp);
-  }
-  GHB_LAUNCH_CHECK(ctx);
+  if ((st = scan_counts(ctx, p.chunk_count, nunits, d_out_rows, stream))) return st;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, write_kernel, threads, 0));
   grid = (int)std::min<int64_t>(p.nchunks, (int64_t)ctx->num_sms * std::max(1, per_sm));
   write_kernel<<<grid, threads, 0, stream>>>(p);
