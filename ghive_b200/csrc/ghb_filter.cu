@@ -76,6 +76,16 @@ __global__ void __launch_bounds__(kFiltThreads) filter_kernel(const __grid_const
     const int64_t tile = s_tile;
     if (tile >= p.ntiles) break;
     const int64_t base = tile * kFiltTile;
+    // the projected columns of a whole tile start toward L2 while the
+    // predicate is evaluated and the tile's offset looked up, so the copies
+    // after the look-back read L2
+    if (threadIdx.x < p.nproj && base + kFiltTile <= p.n) {
+      const ghb_column& c = p.cols.c[p.proj[threadIdx.x]];
+      const int w = c.type == GHB_INT ? 4 : 8;
+      const void* src = c.type == GHB_STRING ? (const void*)((const int2*)c.aux + base)
+                                             : (const void*)((const char*)c.data + base * w);
+      if (((uintptr_t)src & 15) == 0) bulk_prefetch_l2(src, (uint32_t)(kFiltTile * w));
+    }
 
     unsigned ballots[kFiltItems];
 #pragma unroll
