@@ -441,6 +441,13 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
       // key or row index read from that input addresses anything
       if (*(volatile int32_t*)p.dev_status == kDevTimeout) t = p.ntiles;
       s_tile = t;
+      // the tile about one round of claims ahead starts toward L2, so the
+      // CTA that claims it finds its keys and values there
+      const int64_t ahead = t + gridDim.x;
+      if (SRC == kSrcPacked && (ahead + 1) * kSortTile <= p.n) {
+        bulk_prefetch_l2((const unsigned long long*)p.keys_in + ahead * kSortTile, kSortTile * 8);
+        bulk_prefetch_l2(vals_in + ahead * kSortTile, kSortTile * (uint32_t)sizeof(V));
+      }
     }
     for (int i = threadIdx.x; i < (kSortThreads / 32) * kBins; i += kSortThreads) {
       (&s_whist[0][0])[i] = 0;
