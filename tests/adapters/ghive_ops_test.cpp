@@ -338,12 +338,67 @@ static void test_sort() {
   delete t;
 }
 
-int main() {
+// GHive's own N-way join case (JoinPredicateTest.cu), read from a text file
+// the test driver writes from the committed fixture: the tables (one LONG
+// key column each), the chain's steps, and the expected result_offsets.
+// The offsets are compared as a multiset of per-row tuples (the reference's
+// come in key order, these in no particular order).
+static void test_golden_chain(const char* path) {
+  FILE* f = std::fopen(path, "r");
+  CHECK(f != nullptr);
+  if (!f) return;
+  int nt = 0;
+  CHECK(std::fscanf(f, "%d", &nt) == 1);
+  std::vector<Table*> tables;
+  for (int t = 0; t < nt; t++) {
+    int n = 0;
+    CHECK(std::fscanf(f, "%d", &n) == 1);
+    Column* c = new Column(LONG, (uint32_t)n);
+    for (int i = 0; i < n; i++) CHECK(std::fscanf(f, "%ld", &c->as<int64_t>()[i]) == 1);
+    Table* tb = new Table();
+    tb->columns = {c};
+    tb->row_num = (uint32_t)n;
+    tables.push_back(tb);
+  }
+  HashJoinPredicate j;
+  j.join_cols.assign(nt, {0});
+  j.maintain_cols.assign(nt, {0});
+  int ns = 0;
+  CHECK(std::fscanf(f, "%d", &ns) == 1);
+  for (int i = 0; i < ns; i++) {
+    int type = 0;
+    unsigned a = 0, b = 0;
+    CHECK(std::fscanf(f, "%d %u %u", &type, &a, &b) == 3);
+    j.join_types.push_back({(BaseJoinType)type, {a, b}});
+  }
+  int ne = 0;
+  CHECK(std::fscanf(f, "%d", &ne) == 1);
+  std::vector<int32_t> expect(ne);
+  for (int i = 0; i < ne; i++) CHECK(std::fscanf(f, "%d", &expect[i]) == 1);
+  std::fclose(f);
+  Table* r = j.process(tables);
+  CHECK(r != nullptr);
+  if (r) {
+    const size_t w = j.result_offsets.size() / std::max<size_t>(1, r->row_num);
+    CHECK(w > 0 && expect.size() % w == 0);
+    std::multiset<std::vector<int32_t>> got, exp;
+    for (size_t i = 0; w && i + w <= j.result_offsets.size(); i += w)
+      got.insert(std::vector<int32_t>(j.result_offsets.begin() + i, j.result_offsets.begin() + i + w));
+    for (size_t i = 0; w && i + w <= expect.size(); i += w)
+      exp.insert(std::vector<int32_t>(expect.begin() + i, expect.begin() + i + w));
+    CHECK(got == exp);
+    delete r;
+  }
+  for (Table* t : tables) delete t;
+}
+
+int main(int argc, char** argv) {
   test_filter();
   test_groupby();
   test_join();
   test_string_join();
   test_sort();
+  if (argc > 1) test_golden_chain(argv[1]);
   if (failures) {
     std::printf("%d checks failed\n", failures);
     return 1;
