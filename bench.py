@@ -450,7 +450,8 @@ def bench_filter(ctx, args, dev, stream, peak, peak_kind):
            "value": N_FACT / (ms / 1e3), "unit": "rows/s", "ms": ms, "rows_out": rows,
            "roofline": roofline(nbytes, ms, peak, peak_kind,
                                 kernel="filter_kernel (predicate, ballots, look-back, gather)",
-                                l2="flushed before each launch"),
+                                l2="flushed before each launch",
+                                traffic=profile_traffic("filter_fact6M.md")),
            "e2e": {"value": N_FACT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                    "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)),
                    "d2h_bytes_per_step": int(rows * 24 + 8),
