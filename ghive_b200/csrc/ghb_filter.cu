@@ -101,19 +101,29 @@ __global__ void __launch_bounds__(kFiltThreads) filter_kernel(const __grid_const
     __syncthreads();
     // exclusive scan over (item, warp) in row order, by warp 0
     if (warp == 0) {
-      constexpr int kSlots = kFiltItems * (kFiltThreads / 32);  // 64
-      uint32_t a = ((uint32_t*)s_warp_cnt)[2 * lane];
-      uint32_t b = ((uint32_t*)s_warp_cnt)[2 * lane + 1];
-      uint32_t pair = a + b, incl = pair;
+      // each lane scans kPer consecutive (item, warp) slots
+      constexpr int kSlots = kFiltItems * (kFiltThreads / 32);
+      constexpr int kPer = kSlots / 32;
+      static_assert(kSlots % 32 == 0, "whole slots per lane");
+      uint32_t v[kPer];
+      uint32_t mine = 0;
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        v[q] = ((uint32_t*)s_warp_cnt)[kPer * lane + q];
+        mine += v[q];
+      }
+      uint32_t incl = mine;
       for (int o = 1; o < 32; o <<= 1) {
         uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
       }
-      uint32_t excl = incl - pair;
-      ((uint32_t*)s_warp_off)[2 * lane] = excl;
-      ((uint32_t*)s_warp_off)[2 * lane + 1] = excl + a;
+      uint32_t run = incl - mine;
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        ((uint32_t*)s_warp_off)[kPer * lane + q] = run;
+        run += v[q];
+      }
       uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-      static_assert(kSlots == 64, "scan assumes 64 (item, warp) slots");
       uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, total, p.status, p.spin_limit);
       if (lane == 0) {
         s_tile_excl = ex;

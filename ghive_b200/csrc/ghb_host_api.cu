@@ -55,7 +55,7 @@ int32_t stage_in(ghb_ctx* ctx, const ghb_column* h, int32_t n, std::vector<ghb_c
     if (st) return st;
     if (h[i].n > 0) {
       if (!h[i].data) return set_error(ctx, GHB_ERR_INVALID, "column %d: data is NULL", i);
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(p, h[i].data, col_bytes(h[i]), cudaMemcpyHostToDevice, s));
+      if ((st = copy_h2d(ctx, p, h[i].data, col_bytes(h[i]), s))) return st;
     }
     d[i].data = p;
     if (h[i].null_mode == GHB_NULLS_BYTEMAP && h[i].n > 0) {
@@ -63,7 +63,7 @@ int32_t stage_in(ghb_ctx* ctx, const ghb_column* h, int32_t n, std::vector<ghb_c
       void* q = nullptr;
       st = scratch_alloc(ctx, (size_t)h[i].n, &q, s);
       if (st) return st;
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(q, h[i].is_null, (size_t)h[i].n, cudaMemcpyHostToDevice, s));
+      if ((st = copy_h2d(ctx, q, h[i].is_null, (size_t)h[i].n, s))) return st;
       d[i].is_null = (const uint8_t*)q;
     }
   }

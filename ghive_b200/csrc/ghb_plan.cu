@@ -172,8 +172,8 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
       if (st) return st;
       d.bytes = (const uint8_t*)bytes;
       d.nbytes = nb;
-      if (rows > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.data, pairs, rows * 8, cudaMemcpyHostToDevice, P.s));
-      if (nb > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(bytes, h[c].data, nb, cudaMemcpyHostToDevice, P.s));
+      if (rows > 0 && (st = copy_h2d(P.ctx, d.data, pairs, rows * 8, P.s))) return st;
+      if (nb > 0 && (st = copy_h2d(P.ctx, bytes, h[c].data, nb, P.s))) return st;
       continue;
     }
     DevCol& d = t->cols[c];
@@ -183,11 +183,11 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
     if (st) return st;
     if (rows > 0) {
       if (!h[c].data) return set_error(P.ctx, GHB_ERR_INVALID, "column %d: data is NULL", c);
-      GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.data, h[c].data, rows * width_of(d.type), cudaMemcpyHostToDevice, P.s));
+      if ((st = copy_h2d(P.ctx, d.data, h[c].data, rows * width_of(d.type), P.s))) return st;
     }
     if (h[c].null_mode == GHB_NULLS_BYTEMAP) {
       if ((st = P.alloc((size_t)std::max<int64_t>(rows, 1), (void**)&d.is_null))) return st;
-      if (rows > 0) GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d.is_null, h[c].is_null, rows, cudaMemcpyHostToDevice, P.s));
+      if (rows > 0 && (st = copy_h2d(P.ctx, d.is_null, h[c].is_null, rows, P.s))) return st;
     }
   }
   return GHB_OK;
