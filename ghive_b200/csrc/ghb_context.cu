@@ -9,7 +9,6 @@
 #include <cstring>
 #include <map>
 #include <mutex>
-#include <thread>
 
 #include "ghb_ctx.hpp"
 
@@ -101,48 +100,6 @@ int32_t scratch_alloc(ghb_ctx* ctx, size_t bytes, void** out, cudaStream_t strea
   }
   *out = ctx->scratch + off;
   ctx->scratch_used = off + bytes;
-  return GHB_OK;
-}
-
-constexpr size_t kStageChunk = 16u << 20;   // bytes of one staging buffer
-
-int32_t copy_h2d(ghb_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream) {
-  if (bytes == 0) return GHB_OK;
-  cudaPointerAttributes attr;
-  if (cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost) {
-    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
-    return GHB_OK;
-  }
-  cudaGetLastError();
-  if (bytes < (1u << 20)) {   // small: the driver's own staging
-    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
-    return GHB_OK;
-  }
-  for (int b = 0; b < 2; b++) {
-    if (!ctx->stage[b] && cudaMallocHost(&ctx->stage[b], kStageChunk) != cudaSuccess) {
-      cudaGetLastError();
-      ctx->stage[b] = nullptr;
-      return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned staging memory");
-    }
-    if (!ctx->stage_ev[b]) GHB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ctx->stage_ev[b], cudaEventDisableTiming));
-  }
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int nthreads = (int)std::min(4u, std::max(1u, hw / 2));
-  int b = 0;
-  for (size_t off = 0; off < bytes; off += kStageChunk, b ^= 1) {
-    const size_t len = std::min(kStageChunk, bytes - off);
-    GHB_CUDA_TRY(ctx, cudaEventSynchronize(ctx->stage_ev[b]));   // its previous copy is done
-    char* to = (char*)ctx->stage[b];
-    const char* from = (const char*)src + off;
-    const size_t part = (len / nthreads + 63) & ~(size_t)63;
-    std::vector<std::thread> helpers;
-    for (int t = 1; t < nthreads && (size_t)t * part < len; t++)
-      helpers.emplace_back([=] { std::memcpy(to + t * part, from + t * part, std::min(part, len - t * part)); });
-    std::memcpy(to, from, std::min(part, len));
-    for (std::thread& h : helpers) h.join();
-    GHB_CUDA_TRY(ctx, cudaMemcpyAsync((char*)dst + off, to, len, cudaMemcpyHostToDevice, stream));
-    GHB_CUDA_TRY(ctx, cudaEventRecord(ctx->stage_ev[b], stream));
-  }
   return GHB_OK;
 }
 
@@ -350,10 +307,11 @@ int32_t ghb_ctx_destroy(ghb_ctx* ctx) {
   if (ctx->lb_status) cudaFree(ctx->lb_status);
   if (ctx->gb_table) cudaFree(ctx->gb_table);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
-  for (int b = 0; b < 2; b++) {
-    if (ctx->stage[b]) cudaFreeHost(ctx->stage[b]);
-    if (ctx->stage_ev[b]) cudaEventDestroy(ctx->stage_ev[b]);
-  }
+  for (int l = 0; l < kStageLanes; l++)
+    for (int b = 0; b < 2; b++) {
+      if (ctx->stage[l][b]) cudaFreeHost(ctx->stage[l][b]);
+      if (ctx->stage_ev[l][b]) cudaEventDestroy(ctx->stage_ev[l][b]);
+    }
   for (cudaStream_t& hs : ctx->hstream)
     if (hs) cudaStreamDestroy(hs);
   for (auto& row : ctx->hev)

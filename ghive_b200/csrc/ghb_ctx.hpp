@@ -20,6 +20,11 @@
 #include "../../include/ghive_b200.h"
 #include "ghb_internal.cuh"
 
+namespace ghb {
+constexpr int kStageLanes = 4;                // host threads of a staged copy at most
+constexpr size_t kStagePiece = 8u << 20;      // bytes of one staging buffer
+}  // namespace ghb
+
 struct ghb_ctx {
   int device = 0;
   int num_sms = 148;
@@ -66,10 +71,10 @@ struct ghb_ctx {
   // default pool).
   cudaMemPool_t pool = nullptr;
 
-  // pinned staging of pageable host inputs (copy_h2d): two buffers and the
-  // events that say their last copy to the device is done
-  void* stage[2] = {nullptr, nullptr};
-  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  // pinned staging of pageable host memory (ghb_copy.cu): two buffers per
+  // lane and the events that say their last copy is done
+  void* stage[ghb::kStageLanes][2] = {};
+  cudaEvent_t stage_ev[ghb::kStageLanes][2] = {};
 
   // per-call JSON log (ghb_ctx_set_log): the file, its level, the peak the
   // roofline fraction divides by (0: none), and level 2's events
@@ -206,13 +211,21 @@ int32_t string_rep_rows(ghb_ctx* ctx, const ghb_column& c, const int32_t* pass, 
 // component is NULL and matches nothing).  GHB_ERR_UNSUPPORTED past 63 bits.
 int32_t keypack_join(ghb_ctx* ctx, const ghb_column* a, const ghb_column* b, int32_t nkeys, int64_t* a_packed,
                      uint8_t* a_null, int64_t* b_packed, uint8_t* b_null, cudaStream_t stream);
-// Copies `bytes` of host memory to the device on `stream`.  Pinned or
-// registered memory goes by one asynchronous copy; pageable memory (a JVM
-// direct buffer) through two pinned staging buffers: the host copies the
-// next chunk into one, split over a few threads, while the previous chunk's
-// copy to the device runs from the other.  The source may be reused when it
-// returns.
+// Copies between host memory and the device (ghb_copy.cu).  Pinned or
+// registered host memory goes by one asynchronous copy; pageable memory (a
+// JVM direct buffer) through pinned staging buffers in up to kStageLanes
+// host threads, each overlapping the host copy of one piece with the DMA of
+// the previous one.  copy_h2d_many returns once the sources may be reused
+// (the copies are queued on `stream`); copy_d2h_many returns with the data
+// in host memory.
+struct CopyTask {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+int32_t copy_h2d_many(ghb_ctx* ctx, const std::vector<CopyTask>& tasks, cudaStream_t stream);
 int32_t copy_h2d(ghb_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream);
+int32_t copy_d2h_many(ghb_ctx* ctx, const std::vector<CopyTask>& tasks, cudaStream_t stream);
 // Exclusive prefix sums of n int64 counts, in place; their total to the
 // device word *d_total.  One CTA for a few thousand counts, else tiles of
 // 1024 claimed in order with decoupled look-back (bounded by the context's

@@ -47,6 +47,7 @@ size_t out_bytes(const ghb_out_column& o, int64_t cap) {
 int32_t stage_in(ghb_ctx* ctx, const ghb_column* h, int32_t n, std::vector<ghb_column>& d,
                  cudaStream_t s) {
   d.assign(h, h + n);
+  std::vector<CopyTask> copies;
   for (int i = 0; i < n; i++) {
     if (h[i].type == GHB_STRING)
       return set_error(ctx, GHB_ERR_UNSUPPORTED, "STRING columns are not on the device path");
@@ -55,7 +56,7 @@ int32_t stage_in(ghb_ctx* ctx, const ghb_column* h, int32_t n, std::vector<ghb_c
     if (st) return st;
     if (h[i].n > 0) {
       if (!h[i].data) return set_error(ctx, GHB_ERR_INVALID, "column %d: data is NULL", i);
-      if ((st = copy_h2d(ctx, p, h[i].data, col_bytes(h[i]), s))) return st;
+      copies.push_back({p, h[i].data, col_bytes(h[i])});
     }
     d[i].data = p;
     if (h[i].null_mode == GHB_NULLS_BYTEMAP && h[i].n > 0) {
@@ -63,11 +64,11 @@ int32_t stage_in(ghb_ctx* ctx, const ghb_column* h, int32_t n, std::vector<ghb_c
       void* q = nullptr;
       st = scratch_alloc(ctx, (size_t)h[i].n, &q, s);
       if (st) return st;
-      if ((st = copy_h2d(ctx, q, h[i].is_null, (size_t)h[i].n, s))) return st;
+      copies.push_back({q, h[i].is_null, (size_t)h[i].n});
       d[i].is_null = (const uint8_t*)q;
     }
   }
-  return GHB_OK;
+  return copy_h2d_many(ctx, copies, s);
 }
 
 int32_t stage_out(ghb_ctx* ctx, const ghb_out_column* h, int32_t n, int64_t cap,

@@ -150,6 +150,7 @@ ghb_out_column payload_out(const ghb_out_column& o) {
 int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTable* t) {
   t->rows = rows;
   t->cols.assign(ncols, DevCol{});
+  std::vector<CopyTask> copies;   // every column's copies, issued together
   for (int c = 0; c < ncols; c++) {
     if (h[c].type == GHB_STRING) {
       // the pairs, and the bytes up to the largest end a non-NULL row uses
@@ -172,8 +173,8 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
       if (st) return st;
       d.bytes = (const uint8_t*)bytes;
       d.nbytes = nb;
-      if (rows > 0 && (st = copy_h2d(P.ctx, d.data, pairs, rows * 8, P.s))) return st;
-      if (nb > 0 && (st = copy_h2d(P.ctx, bytes, h[c].data, nb, P.s))) return st;
+      if (rows > 0) copies.push_back({d.data, pairs, (size_t)rows * 8});
+      if (nb > 0) copies.push_back({bytes, h[c].data, (size_t)nb});
       continue;
     }
     DevCol& d = t->cols[c];
@@ -183,14 +184,14 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
     if (st) return st;
     if (rows > 0) {
       if (!h[c].data) return set_error(P.ctx, GHB_ERR_INVALID, "column %d: data is NULL", c);
-      if ((st = copy_h2d(P.ctx, d.data, h[c].data, rows * width_of(d.type), P.s))) return st;
+      copies.push_back({d.data, h[c].data, (size_t)rows * width_of(d.type)});
     }
     if (h[c].null_mode == GHB_NULLS_BYTEMAP) {
       if ((st = P.alloc((size_t)std::max<int64_t>(rows, 1), (void**)&d.is_null))) return st;
-      if (rows > 0 && (st = copy_h2d(P.ctx, d.is_null, h[c].is_null, rows, P.s))) return st;
+      if (rows > 0) copies.push_back({d.is_null, h[c].is_null, (size_t)rows});
     }
   }
-  return GHB_OK;
+  return copy_h2d_many(P.ctx, copies, P.s);
 }
 
 std::vector<ghb_column> descs(const DevTable& t) {
@@ -465,10 +466,8 @@ int32_t run_sort(Plan& P, const ghb_plan_op& op, DevTable& t) {
 // (GPUResult builds each row's String from its [start,end)).
 int32_t download_string(Plan& P, const DevCol& d, int64_t rows, ghb_plan_result* out, int c) {
   std::vector<int2> from((size_t)std::max<int64_t>(rows, 1)), to((size_t)std::max<int64_t>(rows, 1));
-  if (rows > 0) {
-    GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(from.data(), d.data, rows * 8, cudaMemcpyDeviceToHost, P.s));
-    GHB_CUDA_TRY(P.ctx, cudaStreamSynchronize(P.s));
-  }
+  int32_t st;
+  if (rows > 0 && (st = copy_d2h_many(P.ctx, {CopyTask{from.data(), d.data, (size_t)rows * 8}}, P.s))) return st;
   int64_t total = 0;
   for (int64_t r = 0; r < rows; r++) {
     if (from[r].x < 0) {
@@ -479,26 +478,22 @@ int32_t download_string(Plan& P, const DevCol& d, int64_t rows, ghb_plan_result*
     total += from[r].y - from[r].x;
     if (total >= INT32_MAX) return set_error(P.ctx, GHB_ERR_UNSUPPORTED, "result column %d: 2^31 bytes of strings", c);
   }
-  if (cudaMallocHost(&out->data[c], (size_t)std::max<int64_t>(rows, 1) * 8) != cudaSuccess ||
-      cudaMallocHost((void**)&out->str_bytes[c], (size_t)std::max<int64_t>(total, 1)) != cudaSuccess) {
-    cudaGetLastError();
-    return set_error(P.ctx, GHB_ERR_OOM, "cannot allocate pinned host memory for the result");
-  }
+  out->data[c] = std::malloc((size_t)std::max<int64_t>(rows, 1) * 8);
+  out->str_bytes[c] = (uint8_t*)std::malloc((size_t)std::max<int64_t>(total, 1));
+  if (!out->data[c] || !out->str_bytes[c]) return set_error(P.ctx, GHB_ERR_OOM, "cannot allocate host memory for the result");
   std::memcpy(out->data[c], to.data(), (size_t)rows * 8);
   out->str_nbytes[c] = total;
   if (total == 0) return GHB_OK;
   void *d_to = nullptr, *d_bytes = nullptr;
-  int32_t st = P.alloc((size_t)rows * 8, &d_to);
+  st = P.alloc((size_t)rows * 8, &d_to);
   if (!st) st = P.alloc((size_t)total, &d_bytes);
   if (st) return st;
-  GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(d_to, to.data(), rows * 8, cudaMemcpyHostToDevice, P.s));
+  if ((st = copy_h2d(P.ctx, d_to, to.data(), (size_t)rows * 8, P.s))) return st;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, (int64_t)P.ctx->num_sms * 8));
   gather_string_bytes_kernel<<<grid, 256, 0, P.s>>>(d.bytes, (const int2*)d.data, (const int2*)d_to, rows,
                                                     (uint8_t*)d_bytes);
   GHB_LAUNCH_CHECK(P.ctx);
-  GHB_CUDA_TRY(P.ctx, cudaMemcpyAsync(out->str_bytes[c], d_bytes, total, cudaMemcpyDeviceToHost, P.s));
-  GHB_CUDA_TRY(P.ctx, cudaStreamSynchronize(P.s));   // `to` is host memory the copy reads
-  return GHB_OK;
+  return copy_d2h_many(P.ctx, {CopyTask{out->str_bytes[c], d_bytes, (size_t)total}}, P.s);
 }
 
 }  // namespace
@@ -555,7 +550,14 @@ static int32_t ghb_run_plan_body(ghb_ctx* ctx, const ghb_gtables* in, int32_t in
   if (!ctx->hstream[1]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[1], cudaStreamNonBlocking));
   Plan P{ctx, ctx->hstream[1], {}};
   DevTable t;
-  int32_t st = upload(P, hc, nc, rows, &t);
+  int32_t st;
+  {
+    CallScope cs(ctx, "plan_upload", P.s, true);
+    cs.rows(rows);
+    cs.bytes(cols_bytes(hc, nc));
+    st = cs.done(upload(P, hc, nc, rows, &t));
+    if (!st) st = cs.done(ghb_sync(ctx, P.s));
+  }
   if (st) return st;
   for (int i = 0; i < nops && !st; i++) {
     switch (ops[i].op) {
@@ -570,6 +572,8 @@ static int32_t ghb_run_plan_body(ghb_ctx* ctx, const ghb_gtables* in, int32_t in
   if ((int)t.cols.size() > GHB_MAX_RESULT_COLS)
     return set_error(ctx, GHB_ERR_UNSUPPORTED, "result of %zu columns (at most %d)", t.cols.size(),
                      GHB_MAX_RESULT_COLS);
+  CallScope dl(ctx, "plan_download", P.s, true);
+  dl.rows(t.rows);
   // the result: host columns (NULLs as GHive's sentinels, and a NULL map),
   // grouped by type the way GPUResult holds them
   out->ncols = (int32_t)t.cols.size();
@@ -582,6 +586,7 @@ static int32_t ghb_run_plan_body(ghb_ctx* ctx, const ghb_gtables* in, int32_t in
   out->n_string = count[GHB_STRING];
   const int32_t base[4] = {0, count[0], count[0] + count[1], count[0] + count[1] + count[2]};
   int32_t seen[4] = {0, 0, 0, 0};
+  std::vector<CopyTask> copies;   // every fixed-width column's copies, issued together
   for (int c = 0; c < out->ncols; c++) {
     const DevCol& d = t.cols[c];
     out->types[c] = d.type;
@@ -594,19 +599,21 @@ static int32_t ghb_run_plan_body(ghb_ctx* ctx, const ghb_gtables* in, int32_t in
       continue;
     }
     const size_t bytes = (size_t)std::max<int64_t>(t.rows, 1) * width_of(d.type);
-    if (cudaMallocHost(&out->data[c], bytes) != cudaSuccess ||
-        (d.is_null && cudaMallocHost((void**)&out->is_null[c], std::max<int64_t>(t.rows, 1)) != cudaSuccess)) {
-      cudaGetLastError();
+    out->data[c] = std::malloc(bytes);
+    if (d.is_null) out->is_null[c] = (uint8_t*)std::malloc((size_t)std::max<int64_t>(t.rows, 1));
+    if (!out->data[c] || (d.is_null && !out->is_null[c])) {
       ghb_plan_result_free(out);
-      return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned host memory for the result");
+      return set_error(ctx, GHB_ERR_OOM, "cannot allocate host memory for the result");
     }
     if (t.rows > 0) {
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out->data[c], d.data, t.rows * width_of(d.type), cudaMemcpyDeviceToHost, P.s));
-      if (d.is_null)
-        GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out->is_null[c], d.is_null, t.rows, cudaMemcpyDeviceToHost, P.s));
+      copies.push_back({out->data[c], d.data, (size_t)t.rows * width_of(d.type)});
+      if (d.is_null) copies.push_back({out->is_null[c], d.is_null, (size_t)t.rows});
     }
   }
-  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(P.s));
+  if ((st = copy_d2h_many(ctx, copies, P.s))) {
+    ghb_plan_result_free(out);
+    return st;
+  }
   return GHB_OK;
 }
 
@@ -626,9 +633,9 @@ int32_t ghb_run_plan(ghb_ctx* ctx, const ghb_gtables* in, int32_t input, const g
 int32_t ghb_plan_result_free(ghb_plan_result* r) {
   if (!r) return GHB_ERR_INVALID;
   for (int c = 0; c < GHB_MAX_RESULT_COLS; c++) {
-    if (r->data[c]) cudaFreeHost(r->data[c]);
-    if (r->is_null[c]) cudaFreeHost(r->is_null[c]);
-    if (r->str_bytes[c]) cudaFreeHost(r->str_bytes[c]);
+    std::free(r->data[c]);
+    std::free(r->is_null[c]);
+    std::free(r->str_bytes[c]);
     r->data[c] = nullptr;
     r->is_null[c] = nullptr;
     r->str_bytes[c] = nullptr;

@@ -597,7 +597,7 @@ typedef struct ghb_plan_op {
  * long || double || int || string of GPUResult's arrays.  A STRING column's
  * data[i] is its int32 [start,end) pairs (-1,-1 = NULL) into str_bytes[i],
  * its rows' UTF-8 bytes packed in row order (str_nbytes[i] of them); it has
- * no NULL map.  The arrays are pinned host memory owned by the library until
+ * no NULL map.  The arrays are host memory owned by the library until
  * ghb_plan_result_free. */
 typedef struct ghb_plan_result {
   int32_t ncols;
