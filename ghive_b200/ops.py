@@ -415,12 +415,12 @@ class Context:
         return ok.rows(n), op.rows(n), (None if rid is None else rid[:n])
 
     # -------------------------------------------------------------- host ops
-    def filter_host(self, pred, cols, proj=None, capacity=None):
+    def filter_host(self, pred, cols, proj=None, capacity=None, outs=None):
         cs = _Cols(cols)
         n = cs[0].n if cs.n else 0
         proj = list(range(cs.n)) if proj is None else list(proj)
         cap = n if capacity is None else capacity
-        outs = _Outs([cs[j].type for j in proj], cap)
+        outs = outs or _Outs([cs[j].type for j in proj], cap)
         pa = (C.c_int32 * max(1, len(proj)))(*proj)
         rows = C.c_int64()
         pp, keep = _pred(pred)
