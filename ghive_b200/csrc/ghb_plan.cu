@@ -158,8 +158,7 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
       d.type = GHB_STRING;
       d.null_mode = GHB_NULLS_SENTINEL;
       const int2* pairs = (const int2*)h[c].aux;
-      if (rows > 0 && (!pairs || !h[c].data))
-        return set_error(P.ctx, GHB_ERR_INVALID, "column %d: STRING without its bytes or index", c);
+      if (rows > 0 && !pairs) return set_error(P.ctx, GHB_ERR_INVALID, "column %d: STRING without its index", c);
       int64_t nb = 0;
       for (int64_t r = 0; r < rows; r++)
         if (pairs[r].x >= 0) {
@@ -167,6 +166,7 @@ int32_t upload(Plan& P, const ghb_column* h, int32_t ncols, int64_t rows, DevTab
             return set_error(P.ctx, GHB_ERR_INVALID, "column %d row %lld: end before start", c, (long long)r);
           nb = std::max<int64_t>(nb, pairs[r].y);
         }
+      if (nb > 0 && !h[c].data) return set_error(P.ctx, GHB_ERR_INVALID, "column %d: STRING without its bytes", c);
       int32_t st = P.alloc((size_t)std::max<int64_t>(rows, 1) * 8, &d.data);
       void* bytes = nullptr;
       if (!st) st = P.alloc((size_t)std::max<int64_t>(nb, 1), &bytes);

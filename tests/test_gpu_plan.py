@@ -229,3 +229,30 @@ def test_string_join_keys_of_two_columns_and_outer_misses(ctx):
     (s, _), (i, _), (a, an) = r["columns"]
     assert list(zip(s, i.tolist(), a)) == rows
     assert an.tolist() == [t[2] is None for t in rows]
+
+
+def test_plans_over_empty_tables_and_empty_intermediates(ctx):
+    """Edge cases the chain must carry: an input table of no rows, a build
+    table of no rows, a filter that passes nothing before a GROUP BY (no
+    groups) and a global aggregate over nothing (one row: COUNT 0, SUM NULL),
+    and a STRING column of only NULLs through a join and a sort."""
+    e64, e32 = np.array([], dtype=np.int64), np.array([], dtype=np.int32)
+    gt = GTables([("Map 1", 0, [e64, e32]), ("Map 2", 0, [np.arange(5, dtype=np.int64)])])
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0), op_sort([1])])
+    assert r["rows"] == 0 and r["types"] == [abi.INT, abi.LONG]      # the sort key first
+    keys = np.arange(100, dtype=np.int64)
+    gt = GTables([("Map 1", 0, [keys, np.ones(100, dtype=np.int32)]), ("Map 2", 0, [e64, e32])])
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0, build_keep=[1], join_type=abi.LEFT_OUTER_JOIN)])
+    assert r["rows"] == 100 and r["columns"][2][1].all()            # every build column NULL
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0)])
+    assert r["rows"] == 0
+    never = abi.Pred.leaf(abi.FILTER_LT, 0, a=-1)
+    r = run_plan(ctx, gt, 0, [op_filter(never), op_groupby([1], [(abi.CNT, -1), (abi.SUM, 0)])])
+    assert r["rows"] == 0
+    r = run_plan(ctx, gt, 0, [op_filter(never), op_groupby([], [(abi.CNT, -1), (abi.SUM, 0)])])
+    assert r["rows"] == 1 and r["columns"][0][0][0] == 0 and r["columns"][1][1][0]
+    nulls = _strings([None] * 50)
+    gt = GTables([("Map 1", 0, [nulls, np.arange(50, dtype=np.int64)]), ("Map 2", 0, [_strings([b"a", None])])])
+    r = run_plan(ctx, gt, 0, [op_join(0, 1, 0, join_type=abi.LEFT_OUTER_JOIN), op_sort([1], orders=[abi.DESC])])
+    assert r["rows"] == 50 and all(v is None for v in r["columns"][1][0])
+    assert r["columns"][0][0].tolist() == list(range(49, -1, -1))
