@@ -67,7 +67,9 @@ def groupby_sharded(cols, key_col, aggs, local_groupby, pred=None, group=None):
     [(values, isnull) per aggregate]) with torch tensors on this rank's
     device (isnull a bool tensor, or None when no row is NULL).
     key_col None is a global aggregate: every rank's partial row goes to rank
-    0, which returns the one result row (the others return none).
+    0, which returns the one result row (the others return none).  The key
+    is a fixed-width column (a STRING key's [start,end) pairs point into
+    its own rank's bytes and do not travel).
     Returns (key or None, [(values, isnull) per aggregate of `aggs`])."""
     import torch
     import torch.distributed as dist
