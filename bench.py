@@ -461,13 +461,25 @@ def bench_filter(ctx, args, dev, stream, peak, peak_kind):
         from oracle import oracle
         import numpy as np
 
-        def cpu():
-            sel = oracle.filter_rows(pred, cols)
-            return [np.take(c, sel) for c in cols]
-        t1, _ = timed_cpu(cpu)
-        out["cpu_baseline"] = {"value": N_FACT / t1, "unit": "rows/s", "cores": 1, "kind": "port",
+        from concurrent.futures import ThreadPoolExecutor
+
+        def cpu_range(lo, hi):
+            part = [c[lo:hi] for c in cols]
+            sel = oracle.filter_rows(pred, part)
+            return [np.take(c, sel) for c in part]
+        t1, _ = timed_cpu(lambda: cpu_range(0, N_FACT))
+        threads = host_threads()
+        bounds = [(N_FACT * i // threads, N_FACT * (i + 1) // threads) for i in range(threads)]
+
+        def cpu_all():
+            with ThreadPoolExecutor(threads) as ex:
+                return list(ex.map(lambda b: cpu_range(*b), bounds))
+        tn, _ = timed_cpu(cpu_all)
+        out["cpu_baseline"] = {"value": N_FACT / tn, "unit": "rows/s", "cores": threads, "kind": "port",
+                               "t1_value": N_FACT / t1,
                                "sample": "the whole 6M-row workload: Hive's filter restated in C++ "
-                                         "(selected rows), then the projected columns gathered"}
+                                         "(selected rows), then the projected columns gathered; "
+                                         "T=all: row ranges, one per thread"}
     del dcols, flush, outs
     torch.cuda.empty_cache()
     return out
@@ -788,6 +800,12 @@ def bench_batched(ctx, args, dev, stream, peak, peak_kind, count=512):
         with ThreadPoolExecutor(threads) as ex:
             res = list(ex.map(one, range(len(sample))))
         dt = time.perf_counter() - t0
+        # T=1: the first eight of those instances one after the other
+        t0 = time.perf_counter()
+        for j in range(8):
+            one(j)
+        dt1 = time.perf_counter() - t0
+        rows1 = sum(specs[sample[j]]["rows"] for j in range(8))
         errs = []
         types = [abi.LONG, abi.LONG, abi.DOUBLE, abi.DOUBLE, abi.INT, abi.INT]
         for j, i in enumerate(sample):
@@ -796,10 +814,11 @@ def bench_batched(ctx, args, dev, stream, peak, peak_kind, count=512):
             if e["results"]:
                 errs.append((e["max_rel"], e["results"]))
         out["cpu_baseline"] = {"value": srows / dt, "unit": "rows/s", "cores": threads,
-                               "kind": "port",
+                               "kind": "port", "t1_value": rows1 / dt1,
                                "sample": "instances 0-63 (%d rows), one sequential Hive group-by "
-                                         "restatement per instance over a %d-thread pool"
-                                         % (srows, threads)}
+                                         "restatement per instance over a %d-thread pool; T=1: "
+                                         "instances 0-7 (%d rows) one after the other"
+                                         % (srows, threads, rows1)}
         out["double_error_vs_compensated_sum"] = {
             "results": int(sum(n for _, n in errs)),
             "max_rel": max(m for m, _ in errs) if errs else None,
