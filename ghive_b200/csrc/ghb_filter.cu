@@ -6,12 +6,14 @@
 // FilterOperator.cu:36-93: thrust::reduce + thrust::copy_if of row indices,
 // D2H of the indices, then a host gather over every column, in place).
 //
-// One kernel: each CTA claims tiles of rows in launch order, evaluates the
-// whole predicate tree in registers, turns the per-row results into warp
-// ballots, scans the popcounts across the CTA, gets the tile's global output
-// offset by decoupled look-back over earlier tiles, and copies the projected
+// One kernel: each CTA claims ranges of rows (whole tiles, about one range
+// per resident CTA) in launch order, evaluates the whole predicate tree in
+// registers, keeps the per-row results as warp ballots in shared memory,
+// scans their popcounts across the range, gets the range's global output
+// offset by decoupled look-back over earlier ranges, and copies the projected
 // columns of the selected rows to their final positions.  No bitmap or index
-// list is materialised; the output keeps input order (Hive's selected[]).
+// list goes to global memory; the output keeps input order (Hive's
+// selected[]).
 #include <algorithm>
 
 #include "ghb_ctx.hpp"
@@ -22,6 +24,9 @@ namespace ghb {
 constexpr int kFiltThreads = 256;
 constexpr int kFiltItems = 8;   // rows per thread per tile
 constexpr int kFiltTile = kFiltThreads * kFiltItems;
+constexpr int kFiltWarps = kFiltThreads / 32;
+constexpr int kFiltWords = kFiltItems * kFiltWarps;   // ballot words of one tile
+constexpr int kFiltMaxTiles = 16;                     // tiles of one claimed range
 constexpr int kMaxProj = kMaxCols;
 
 struct FilterParams {
@@ -31,119 +36,182 @@ struct FilterParams {
   int32_t proj[kMaxProj];
   ghb_out_column out[kMaxProj];
   int64_t n;
-  int64_t ntiles;
+  int64_t range_rows;            // rows of a claimed range: whole tiles, at most kFiltMaxTiles
+  int64_t nranges;
   int64_t cap;
   int64_t* d_out_rows;
   uint64_t* lb;
   uint32_t epoch;
-  unsigned long long* counters;  // [0] next tile, [1] finished CTAs
+  unsigned long long* counters;  // [0] next range, [1] finished CTAs
   int32_t* status;
   int32_t spin_limit;            // look-back polls before GHB_ERR_TIMEOUT
 };
 
-__device__ __forceinline__ void copy_value(const ghb_column& c, const ghb_out_column& o, int64_t row,
-                                           int64_t pos) {
-  if (c.type == GHB_STRING) {
-    // a STRING output row is the input row's [start,end) into the same bytes
-    const int2 ix = __ldg((const int2*)c.aux + row);
-    ((int2*)o.data)[pos] = ix;
-    if (o.is_null) o.is_null[pos] = ix.x < 0 ? 1 : 0;
+// Copies column c's value of the selected rows row0 + k * kFiltThreads (bit
+// `lane` of word b[k]) to output row pos[k]: every load of the tile is issued
+// before its stores.
+__device__ __forceinline__ void copy_rows(const ghb_column& c, const ghb_out_column& o, int64_t row0,
+                                          const bool (&live)[kFiltItems], const int64_t (&pos)[kFiltItems]) {
+  if (c.type == GHB_INT) {
+    int32_t v[kFiltItems];
+#pragma unroll
+    for (int k = 0; k < kFiltItems; k++)
+      if (live[k]) v[k] = __ldcs((const int*)c.data + row0 + k * kFiltThreads);
+#pragma unroll
+    for (int k = 0; k < kFiltItems; k++)
+      if (live[k]) ((int32_t*)o.data)[pos[k]] = v[k];
+    if (o.is_null) {
+#pragma unroll
+      for (int k = 0; k < kFiltItems; k++)
+        if (live[k]) o.is_null[pos[k]] = raw_is_null(c, (int64_t)v[k], row0 + k * kFiltThreads) ? 1 : 0;
+    }
     return;
   }
-  if (c.type == GHB_INT) ((int32_t*)o.data)[pos] = __ldg((const int32_t*)c.data + row);
-  else ((long long*)o.data)[pos] = __ldg((const long long*)c.data + row);
+  // LONG, DOUBLE bits, or a STRING row's [start,end) pair into the same bytes
+  const long long* src = c.type == GHB_STRING ? (const long long*)c.aux : (const long long*)c.data;
+  long long v[kFiltItems];
+#pragma unroll
+  for (int k = 0; k < kFiltItems; k++)
+    if (live[k]) v[k] = __ldcs(src + row0 + k * kFiltThreads);
+#pragma unroll
+  for (int k = 0; k < kFiltItems; k++)
+    if (live[k]) ((long long*)o.data)[pos[k]] = v[k];
   if (o.is_null) {
-    bool null = false;
-    if (c.null_mode != GHB_NULLS_NONE) null = raw_is_null(c, ld_raw(c, row), row);
-    o.is_null[pos] = null ? 1 : 0;
+#pragma unroll
+    for (int k = 0; k < kFiltItems; k++) {
+      if (!live[k]) continue;
+      const bool null = c.type == GHB_STRING ? (int32_t)(v[k] & 0xffffffff) < 0
+                                             : raw_is_null(c, (int64_t)v[k], row0 + k * kFiltThreads);
+      o.is_null[pos[k]] = null ? 1 : 0;
+    }
   }
 }
 
-// The parameters stay in the constant bank (__grid_constant__): the string
-// leaves' out-of-line compare takes references into them, which would
-// otherwise copy the whole parameter block to every thread's stack.
+// Each CTA claims ranges of rows in launch order.  Per range: the predicate
+// tree of every row, kept as warp ballots in shared memory; one scan of the
+// ballots' counts; the range's global output offset by decoupled look-back
+// over earlier ranges (one per range, so a range's writes do not wait per
+// tile); then the projected columns of the selected rows, every load of a
+// tile's column issued before its stores.  The parameters stay in the
+// constant bank (__grid_constant__): the string leaves' out-of-line compare
+// takes references into them, which would otherwise copy the whole parameter
+// block to every thread's stack.
 __global__ void __launch_bounds__(kFiltThreads) filter_kernel(const __grid_constant__ FilterParams p) {
-  __shared__ int64_t s_tile;
-  __shared__ uint32_t s_warp_cnt[kFiltItems][kFiltThreads / 32];
-  __shared__ uint32_t s_warp_off[kFiltItems][kFiltThreads / 32];
-  __shared__ uint64_t s_tile_excl;
+  constexpr int kWords = kFiltMaxTiles * kFiltWords;
+  constexpr int kPer = kWords / kFiltThreads;
+  static_assert(kWords % kFiltThreads == 0, "whole ballot words per thread");
+  __shared__ int64_t s_range;
+  __shared__ uint32_t s_mask[kWords];   // ballot words in row order: (tile, item, warp)
+  __shared__ uint32_t s_off[kWords];    // each word's first output row within the range
+  __shared__ uint32_t s_wsum[kFiltWarps];
+  __shared__ uint64_t s_excl;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
+  const bool leaf1 = p.pred.n_nodes == 1 && p.pred.nodes[0].col2 < 0 &&
+                     p.cols.c[p.pred.nodes[0].col].type != GHB_STRING;
 
   while (true) {
-    claim_tile(&p.counters[0], &s_tile);
-    const int64_t tile = s_tile;
-    if (tile >= p.ntiles) break;
-    const int64_t base = tile * kFiltTile;
-    // the projected columns of a whole tile start toward L2 while the
-    // predicate is evaluated and the tile's offset looked up, so the copies
-    // after the look-back read L2
-    if (threadIdx.x < p.nproj && base + kFiltTile <= p.n) {
-      const ghb_column& c = p.cols.c[p.proj[threadIdx.x]];
-      const int w = c.type == GHB_INT ? 4 : 8;
-      const void* src = c.type == GHB_STRING ? (const void*)((const int2*)c.aux + base)
-                                             : (const void*)((const char*)c.data + base * w);
-      if (((uintptr_t)src & 15) == 0) bulk_prefetch_l2(src, (uint32_t)(kFiltTile * w));
-    }
-
-    unsigned ballots[kFiltItems];
+    claim_tile(&p.counters[0], &s_range);
+    const int64_t r = s_range;
+    if (r >= p.nranges) break;
+    const int64_t base = r * p.range_rows;
+    const int64_t end = min(p.n, base + p.range_rows);
+    const int tiles = (int)((end - base + kFiltTile - 1) / kFiltTile);
+    for (int t = 0; t < tiles; t++) {
+      const int64_t row0 = base + (int64_t)t * kFiltTile + threadIdx.x;
+      unsigned ballots[kFiltItems];
+      if (leaf1) {
+        // one leaf on a fixed-width column: the tile's values are loaded
+        // before any is compared
+        const ghb_pred_node& nd = p.pred.nodes[0];
+        const ghb_column& c = p.cols.c[nd.col];
+        int64_t x[kFiltItems];
 #pragma unroll
-    for (int k = 0; k < kFiltItems; k++) {
-      int64_t row = base + (int64_t)k * kFiltThreads + threadIdx.x;
-      bool pass = row < p.n && eval_pred(p.pred, p.cols, row);
-      ballots[k] = __ballot_sync(0xffffffffu, pass);
-    }
-    if (lane == 0) {
+        for (int k = 0; k < kFiltItems; k++) {
+          const int64_t row = row0 + k * kFiltThreads;
+          x[k] = row < end ? ld_raw(c, row) : 0;
+        }
 #pragma unroll
-      for (int k = 0; k < kFiltItems; k++) s_warp_cnt[k][warp] = __popc(ballots[k]);
-    }
-    __syncthreads();
-    // exclusive scan over (item, warp) in row order, by warp 0
-    if (warp == 0) {
-      // each lane scans kPer consecutive (item, warp) slots
-      constexpr int kSlots = kFiltItems * (kFiltThreads / 32);
-      constexpr int kPer = kSlots / 32;
-      static_assert(kSlots % 32 == 0, "whole slots per lane");
-      uint32_t v[kPer];
-      uint32_t mine = 0;
+        for (int k = 0; k < kFiltItems; k++) {
+          const int64_t row = row0 + k * kFiltThreads;
+          ballots[k] = __ballot_sync(0xffffffffu, row < end && leaf_on_raw(nd, c, x[k], row));
+        }
+      } else {
 #pragma unroll
-      for (int q = 0; q < kPer; q++) {
-        v[q] = ((uint32_t*)s_warp_cnt)[kPer * lane + q];
-        mine += v[q];
+        for (int k = 0; k < kFiltItems; k++) {
+          const int64_t row = row0 + k * kFiltThreads;
+          ballots[k] = __ballot_sync(0xffffffffu, row < end && eval_pred(p.pred, p.cols, row));
+        }
       }
-      uint32_t incl = mine;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      uint32_t run = incl - mine;
-#pragma unroll
-      for (int q = 0; q < kPer; q++) {
-        ((uint32_t*)s_warp_off)[kPer * lane + q] = run;
-        run += v[q];
-      }
-      uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-      uint64_t ex = lookback_exclusive(p.lb, p.epoch, tile, total, p.status, p.spin_limit);
       if (lane == 0) {
-        s_tile_excl = ex;
-        if (tile == p.ntiles - 1) *p.d_out_rows = (int64_t)(ex + total);
-      }
-    }
-    __syncthreads();
-    const uint64_t tile_excl = s_tile_excl;
 #pragma unroll
-    for (int k = 0; k < kFiltItems; k++) {
-      if (!((ballots[k] >> lane) & 1u)) continue;
-      int64_t row = base + (int64_t)k * kFiltThreads + threadIdx.x;
-      int64_t pos = (int64_t)(tile_excl + s_warp_off[k][warp] + __popc(ballots[k] & lt_mask));
-      if (pos >= p.cap) {
-        raise_status(p.status, kDevCapacity);
-        continue;
+        for (int k = 0; k < kFiltItems; k++) s_mask[(t * kFiltItems + k) * kFiltWarps + warp] = ballots[k];
       }
-      for (int j = 0; j < p.nproj; j++) copy_value(p.cols.c[p.proj[j]], p.out[j], row, pos);
     }
     __syncthreads();
+    // exclusive scan of the words' counts in row order: kPer consecutive
+    // words per thread, then across the warps
+    const int nwords = tiles * kFiltWords;
+    uint32_t cnt[kPer];
+    uint32_t mine = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const int w = threadIdx.x * kPer + q;
+      cnt[q] = w < nwords ? __popc(s_mask[w]) : 0;
+      mine += cnt[q];
+    }
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t ws = lane < kFiltWarps ? s_wsum[lane] : 0;
+      uint32_t wi = ws;
+#pragma unroll
+      for (int o = 1; o < kFiltWarps; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += v;
+      }
+      const uint32_t total = __shfl_sync(0xffffffffu, wi, kFiltWarps - 1);
+      const uint64_t ex = lookback_exclusive(p.lb, p.epoch, r, total, p.status, p.spin_limit);
+      if (lane < kFiltWarps) s_wsum[lane] = wi - ws;
+      if (lane == 0) {
+        s_excl = ex;
+        if (r == p.nranges - 1) *p.d_out_rows = (int64_t)(ex + total);
+        if ((int64_t)(ex + total) > p.cap) raise_status(p.status, kDevCapacity);
+      }
+    }
+    __syncthreads();
+    uint32_t run = s_wsum[warp] + incl - mine;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const int w = threadIdx.x * kPer + q;
+      if (w < nwords) s_off[w] = run;
+      run += cnt[q];
+    }
+    __syncthreads();
+    const uint64_t rex = s_excl;
+    if (p.nproj > 0) {
+      for (int t = 0; t < tiles; t++) {
+        bool live[kFiltItems];
+        int64_t pos[kFiltItems];
+#pragma unroll
+        for (int k = 0; k < kFiltItems; k++) {
+          const int w = (t * kFiltItems + k) * kFiltWarps + warp;
+          const unsigned b = s_mask[w];
+          pos[k] = (int64_t)(rex + s_off[w] + __popc(b & lt_mask));
+          live[k] = ((b >> lane) & 1u) && pos[k] < p.cap;
+        }
+        const int64_t row0 = base + (int64_t)t * kFiltTile + threadIdx.x;
+        for (int j = 0; j < p.nproj; j++) copy_rows(p.cols.c[p.proj[j]], p.out[j], row0, live, pos);
+      }
+    }
+    __syncthreads();   // the next range reuses the ballots and offsets
   }
   claim_finish(p.counters);
 }
@@ -177,22 +245,27 @@ int32_t filter_impl(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* c
   p.cols.n = ncols;
   p.nproj = nproj;
   p.n = n;
-  p.ntiles = (n + kFiltTile - 1) / kFiltTile;
   p.cap = out_capacity;
   p.d_out_rows = d_out_rows;
   p.status = ctx->d_status;
   p.counters = ctx->d_counters;
   p.spin_limit = ctx->spin_limit;
-  if (p.ntiles == 0) {
+  if (n == 0) {
     GHB_CUDA_TRY(ctx, cudaMemsetAsync(d_out_rows, 0, sizeof(int64_t), stream));
     return GHB_OK;
   }
-  st = lookback_prepare(ctx, p.ntiles, &p.epoch, stream);
-  if (st) return st;
-  p.lb = ctx->lb_status;
   int per_sm = 0;
   GHB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, filter_kernel, kFiltThreads, 0));
-  int grid = (int)std::min<int64_t>(p.ntiles, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  const int64_t slots = (int64_t)ctx->num_sms * std::max(1, per_sm);
+  // one range per resident CTA where the rows allow, in whole tiles
+  const int64_t ntiles = (n + kFiltTile - 1) / kFiltTile;
+  const int64_t per = std::min<int64_t>(kFiltMaxTiles, std::max<int64_t>(1, (ntiles + slots - 1) / slots));
+  p.range_rows = per * kFiltTile;
+  p.nranges = (ntiles + per - 1) / per;
+  st = lookback_prepare(ctx, p.nranges, &p.epoch, stream);
+  if (st) return st;
+  p.lb = ctx->lb_status;
+  int grid = (int)std::min<int64_t>(p.nranges, slots);
   filter_kernel<<<grid, kFiltThreads, 0, stream>>>(p);
   GHB_LAUNCH_CHECK(ctx);
   return GHB_OK;

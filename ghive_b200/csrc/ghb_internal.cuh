@@ -141,6 +141,18 @@ static __device__ __noinline__ bool eval_str_leaf(const PredProg& p, const ghb_p
   return false;
 }
 
+// A leaf against literals on a fixed-width column c, given row i's raw value x.
+__device__ __forceinline__ bool leaf_on_raw(const ghb_pred_node& nd, const ghb_column& c, int64_t x, int64_t i) {
+  if (raw_is_null(c, x, i)) return false;
+  if (nd.mode == GHB_FILTER_NOT_NULL) return true;
+  if (c.type == GHB_DOUBLE || nd.lit_is_double) {
+    double a = nd.lit_is_double ? nd.lit_d[0] : (double)nd.lit_i[0];
+    double b = nd.lit_is_double ? nd.lit_d[1] : (double)nd.lit_i[1];
+    return cmp_mode<double>(nd.mode, raw_to_f64(c.type, x), a, b);
+  }
+  return cmp_mode<int64_t>(nd.mode, x, nd.lit_i[0], nd.lit_i[1]);
+}
+
 // One leaf of FilterPredicate (FilterPredicate.hpp:119-385 functors, with
 // Hive's NULL rule: a NULL operand never passes).
 __device__ __forceinline__ bool eval_leaf(const PredProg& p, const ghb_pred_node& nd, const ColSet& cs,
@@ -148,22 +160,16 @@ __device__ __forceinline__ bool eval_leaf(const PredProg& p, const ghb_pred_node
   const ghb_column& c = cs.c[nd.col];
   if (p.has_str && c.type == GHB_STRING) return eval_str_leaf(p, nd, cs, i);
   int64_t x = ld_raw(c, i);
+  if (nd.col2 < 0) return leaf_on_raw(nd, c, x, i);
+  // against another column of the same row
   if (raw_is_null(c, x, i)) return false;
   if (nd.mode == GHB_FILTER_NOT_NULL) return true;
-  if (nd.col2 >= 0) {
-    const ghb_column& c2 = cs.c[nd.col2];
-    int64_t y = ld_raw(c2, i);
-    if (raw_is_null(c2, y, i)) return false;
-    if (c.type == GHB_DOUBLE || c2.type == GHB_DOUBLE)
-      return cmp_mode<double>(nd.mode, raw_to_f64(c.type, x), raw_to_f64(c2.type, y), 0.0);
-    return cmp_mode<int64_t>(nd.mode, x, y, 0);
-  }
-  if (c.type == GHB_DOUBLE || nd.lit_is_double) {
-    double a = nd.lit_is_double ? nd.lit_d[0] : (double)nd.lit_i[0];
-    double b = nd.lit_is_double ? nd.lit_d[1] : (double)nd.lit_i[1];
-    return cmp_mode<double>(nd.mode, raw_to_f64(c.type, x), a, b);
-  }
-  return cmp_mode<int64_t>(nd.mode, x, nd.lit_i[0], nd.lit_i[1]);
+  const ghb_column& c2 = cs.c[nd.col2];
+  int64_t y = ld_raw(c2, i);
+  if (raw_is_null(c2, y, i)) return false;
+  if (c.type == GHB_DOUBLE || c2.type == GHB_DOUBLE)
+    return cmp_mode<double>(nd.mode, raw_to_f64(c.type, x), raw_to_f64(c2.type, y), 0.0);
+  return cmp_mode<int64_t>(nd.mode, x, y, 0);
 }
 
 // Evaluates the whole tree for row i.  The program is in post-order, so each
