@@ -218,6 +218,15 @@ def run_reference(args, world, rank):
 
 
 # ----------------------------------------------------------------- GPU arm
+def filter_host_chunks(n):
+    """Chunks of ghb_filter_host's pipelined path over n pinned rows (one
+    int64 row count comes back per chunk): about n/12 rows each, whole
+    2048-row tiles between 512Ki and 8Mi rows; below two chunks, one call."""
+    c = min(8 << 20, max(512 << 10, (n + 11) // 12))
+    c = (c + 2047) // 2048 * 2048
+    return (n + c - 1) // c if n >= 2 * c else 1
+
+
 def pinned(a):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -450,12 +459,13 @@ def bench_filter(ctx, args, dev, stream, peak, peak_kind):
                        "the passing rows' four columns written in order",
            "value": N_FACT / (ms / 1e3), "unit": "rows/s", "ms": ms, "rows_out": rows,
            "roofline": roofline(nbytes, ms, peak, peak_kind,
-                                kernel="filter_kernel (predicate, ballots, look-back, gather)",
+                                kernel="filter_kernel (per range of tiles: predicate ballots, one look-back, "
+                                       "the projected columns' selected rows)",
                                 l2="flushed before each launch",
                                 traffic=profile_traffic("filter_fact6M.md")),
            "e2e": {"value": N_FACT / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                    "h2d_bytes_per_step": int(sum(c.nbytes for c in cols)),
-                   "d2h_bytes_per_step": int(rows * 24 + 8),
+                   "d2h_bytes_per_step": int(rows * 24 + 8 * filter_host_chunks(N_FACT)),
                    "api": "ghb_filter_host (pinned host columns and outputs)"}}
     if not args.no_cpu:
         from oracle import oracle

@@ -14,9 +14,6 @@
 #include "ghb_ctx.hpp"
 
 namespace ghb {
-namespace {
-
-constexpr size_t kSmallCopy = 1u << 20;   // below this the driver's own staging
 
 bool host_pinned(const void* p) {
   cudaPointerAttributes attr;
@@ -24,6 +21,10 @@ bool host_pinned(const void* p) {
   cudaGetLastError();
   return pinned;
 }
+
+namespace {
+
+constexpr size_t kSmallCopy = 1u << 20;   // below this the driver's own staging
 
 int32_t ensure_staging(ghb_ctx* ctx) {
   for (int l = 0; l < kStageLanes; l++)

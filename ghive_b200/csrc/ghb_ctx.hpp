@@ -226,6 +226,8 @@ struct CopyTask {
 int32_t copy_h2d_many(ghb_ctx* ctx, const std::vector<CopyTask>& tasks, cudaStream_t stream);
 int32_t copy_h2d(ghb_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream);
 int32_t copy_d2h_many(ghb_ctx* ctx, const std::vector<CopyTask>& tasks, cudaStream_t stream);
+// True when p is pinned (or registered) host memory.
+bool host_pinned(const void* p);
 // Exclusive prefix sums of n int64 counts, in place; their total to the
 // device word *d_total.  One CTA for a few thousand counts, else tiles of
 // 1024 claimed in order with decoupled look-back (bounded by the context's

@@ -110,6 +110,167 @@ int32_t read_count(ghb_ctx* ctx, const int64_t* d_count, int64_t* out, cudaStrea
   return st;
 }
 
+// The context's three host-path streams (copy in, kernels, copy out) and
+// their per-buffer events, made on first use.
+int32_t host_streams(ghb_ctx* ctx) {
+  for (int i = 0; i < 3; i++)
+    if (!ctx->hstream[i]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[i], cudaStreamNonBlocking));
+  for (auto& row : ctx->hev)
+    for (cudaEvent_t& e : row)
+      if (!e) GHB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return GHB_OK;
+}
+
+// At least `bytes` of pinned host memory at ctx->pinned.
+int32_t ensure_pinned(ghb_ctx* ctx, size_t bytes) {
+  if (ctx->pinned_bytes >= bytes) return GHB_OK;
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  ctx->pinned = nullptr;
+  ctx->pinned_bytes = 0;
+  if (cudaMallocHost(&ctx->pinned, std::max<size_t>(bytes, 4096)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned host memory");
+  }
+  ctx->pinned_bytes = std::max<size_t>(bytes, 4096);
+  return GHB_OK;
+}
+
+// Rows of one chunk of the pipelined filter: about a twelfth of the input
+// (so the first chunk's copy, which nothing overlaps, is short), in whole
+// 2048-row tiles, between 512Ki and 8Mi rows.
+int64_t filter_chunk_rows(int64_t n) {
+  const int64_t c = std::min<int64_t>(8 << 20, std::max<int64_t>(512 << 10, (n + 11) / 12));
+  return (c + 2047) / 2048 * 2048;
+}
+
+// True when every buffer the filter reads or writes on the host is pinned,
+// so its copies can run asynchronously chunk by chunk.
+bool filter_host_pinned(const ghb_column* cols, int32_t ncols, const ghb_out_column* out, int32_t nproj) {
+  for (int i = 0; i < ncols; i++) {
+    if (!cols[i].data || !host_pinned(cols[i].data)) return false;
+    if (cols[i].null_mode == GHB_NULLS_BYTEMAP && (!cols[i].is_null || !host_pinned(cols[i].is_null))) return false;
+  }
+  for (int j = 0; j < nproj; j++) {
+    if (!out[j].data || !host_pinned(out[j].data)) return false;
+    if (out[j].is_null && !host_pinned(out[j].is_null)) return false;
+  }
+  return true;
+}
+// The filter over pinned host columns, in chunks of rows through three
+// streams: a chunk's columns are copied in while the one before is filtered
+// and the one before that is copied out, so the copies in both directions
+// overlap each other and the kernels.  Each chunk is filtered into one of
+// two device output buffers (a chunk's output is at most its rows); its row
+// count comes back before its copy-out is issued, and the chunks' outputs
+// are appended in chunk order, which is the filter's row order.
+int32_t filter_host_chunked(ghb_ctx* ctx, const ghb_predicate* pred, const ghb_column* cols, int32_t ncols,
+                            const int32_t* proj, int32_t nproj, ghb_out_column* out, int64_t out_capacity,
+                            int64_t n, int64_t* out_rows) {
+  int32_t st = host_streams(ctx);
+  if (st) return st;
+  cudaStream_t s_in = ctx->hstream[0], s_k = ctx->hstream[1], s_out = ctx->hstream[2];
+  // the calling thread's legacy default stream may hold work on these buffers
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(0));
+  const int64_t chunk = filter_chunk_rows(n);
+  const int64_t nchunks = (n + chunk - 1) / chunk;
+  size_t need = 4096;
+  for (int i = 0; i < ncols; i++) {
+    need += 2 * (align256((size_t)chunk * type_width(cols[i].type)) + 256);
+    if (cols[i].null_mode == GHB_NULLS_BYTEMAP) need += 2 * (align256((size_t)chunk) + 256);
+  }
+  for (int j = 0; j < nproj; j++) need += 2 * (out_bytes(out[j], chunk) + 512);
+  if ((st = scratch_reserve(ctx, need, s_in))) return st;
+  if ((st = ensure_pinned(ctx, (size_t)nchunks * 8))) return st;
+  int64_t* h_rows = (int64_t*)ctx->pinned;   // each chunk's row count
+  struct Slot {
+    std::vector<ghb_column> in;
+    std::vector<ghb_out_column> out;
+    int64_t* d_rows = nullptr;
+  } slot[2];
+  for (int b = 0; b < 2; b++) {
+    Slot& sl = slot[b];
+    sl.in.assign(cols, cols + ncols);
+    for (int i = 0; i < ncols; i++) {
+      void* q = nullptr;
+      if ((st = scratch_alloc(ctx, std::max<size_t>((size_t)chunk * type_width(cols[i].type), 16), &q, s_in)))
+        return st;
+      sl.in[i].data = q;
+      if (cols[i].null_mode == GHB_NULLS_BYTEMAP) {
+        if ((st = scratch_alloc(ctx, std::max<size_t>((size_t)chunk, 16), &q, s_in))) return st;
+        sl.in[i].is_null = (const uint8_t*)q;
+      }
+    }
+    if ((st = stage_out(ctx, out, nproj, chunk, sl.out, s_in))) return st;
+    if ((st = scratch_alloc(ctx, 8, (void**)&sl.d_rows, s_in))) return st;
+  }
+  cudaEvent_t* ev_in = ctx->hev[0];     // chunk copied in (per buffer)
+  cudaEvent_t* ev_filt = ctx->hev[1];   // chunk filtered: its input buffer is free
+  cudaEvent_t* ev_rows = ctx->hev[2];   // chunk's row count on the host side
+  cudaEvent_t* ev_out = ctx->hev[3];    // chunk copied out: its output buffer is free
+  auto fail = [&](int32_t code) {
+    cudaStreamSynchronize(s_in);
+    cudaStreamSynchronize(s_k);
+    cudaStreamSynchronize(s_out);
+    return code;
+  };
+  int64_t total = 0, written = 0;
+  auto copy_out = [&](int64_t c) -> int32_t {
+    const int b = (int)(c & 1);
+    const Slot& sl = slot[b];
+    GHB_CUDA_TRY(ctx, cudaEventSynchronize(ev_rows[b]));
+    const int64_t rows = h_rows[c];
+    total += rows;
+    const int64_t r = std::max<int64_t>(0, std::min<int64_t>(rows, out_capacity - written));
+    GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_out, ev_rows[b], 0));
+    for (int j = 0; j < nproj && r > 0; j++) {
+      const size_t w = type_width(out[j].type);
+      GHB_CUDA_TRY(ctx, cudaMemcpyAsync((char*)out[j].data + written * w, sl.out[j].data, r * w,
+                                        cudaMemcpyDeviceToHost, s_out));
+      if (out[j].is_null)
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync(out[j].is_null + written, sl.out[j].is_null, r, cudaMemcpyDeviceToHost,
+                                          s_out));
+    }
+    written += r;
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_out[b], s_out));
+    return GHB_OK;
+  };
+  for (int64_t c = 0; c < nchunks; c++) {
+    const int b = (int)(c & 1);
+    Slot& sl = slot[b];
+    const int64_t r0 = c * chunk, rows = std::min<int64_t>(chunk, n - r0);
+    // copy in, once the filter of chunk c - 2 has read this buffer
+    if (c >= 2) GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_in, ev_filt[b], 0));
+    for (int i = 0; i < ncols; i++) {
+      const size_t w = type_width(cols[i].type);
+      sl.in[i].n = rows;
+      GHB_CUDA_TRY(ctx, cudaMemcpyAsync((void*)sl.in[i].data, (const char*)cols[i].data + r0 * w, rows * w,
+                                        cudaMemcpyHostToDevice, s_in));
+      if (cols[i].null_mode == GHB_NULLS_BYTEMAP)
+        GHB_CUDA_TRY(ctx, cudaMemcpyAsync((void*)sl.in[i].is_null, cols[i].is_null + r0, rows,
+                                          cudaMemcpyHostToDevice, s_in));
+    }
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_in[b], s_in));
+    // filter, once the chunk is in and chunk c - 2's output has been copied out
+    GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, ev_in[b], 0));
+    if (c >= 2) GHB_CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, ev_out[b], 0));
+    st = filter_impl(ctx, pred, sl.in.data(), ncols, proj, nproj, sl.out.data(), rows, sl.d_rows, s_k);
+    if (st) return fail(st);
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_filt[b], s_k));
+    GHB_CUDA_TRY(ctx, cudaMemcpyAsync(&h_rows[c], sl.d_rows, 8, cudaMemcpyDeviceToHost, s_k));
+    GHB_CUDA_TRY(ctx, cudaEventRecord(ev_rows[b], s_k));
+    // the previous chunk's output goes out while this one is filtered
+    if (c >= 1 && (st = copy_out(c - 1))) return fail(st);
+  }
+  if (nchunks >= 1 && (st = copy_out(nchunks - 1))) return fail(st);
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s_out));
+  GHB_CUDA_TRY(ctx, cudaStreamSynchronize(s_in));
+  st = ghb_sync(ctx, s_k);   // device status of every chunk's kernel
+  *out_rows = total;
+  if (st) return st;
+  if (total > out_capacity) return set_error(ctx, GHB_ERR_CAPACITY, "output or table capacity exceeded");
+  return GHB_OK;
+}
+
 }  // namespace
 }  // namespace ghb
 
@@ -128,6 +289,11 @@ static int32_t ghb_filter_host_body(ghb_ctx* ctx, const ghb_predicate* pred, con
   if (st) return st;
   if (nproj < 0 || nproj > kMaxCols || (nproj > 0 && (!proj || !out)))
     return set_error(ctx, GHB_ERR_INVALID, "bad projection list");
+  if (out_capacity < 0) return set_error(ctx, GHB_ERR_INVALID, "negative out_capacity");
+  for (int j = 0; j < nproj; j++)
+    if (proj[j] < 0 || proj[j] >= ncols) return set_error(ctx, GHB_ERR_INVALID, "projection %d out of range", j);
+  if (n >= 2 * filter_chunk_rows(n) && filter_host_pinned(cols, ncols, out, nproj))
+    return filter_host_chunked(ctx, pred, cols, ncols, proj, nproj, out, out_capacity, n, out_rows);
   size_t need = 4096 + align256(8);
   for (int i = 0; i < ncols; i++) need += in_bytes(cols[i]) + 256;
   for (int j = 0; j < nproj; j++) need += out_bytes(out[j], out_capacity) + 512;
@@ -226,12 +392,8 @@ static int32_t ghb_hash_join_host_body(ghb_ctx* ctx, const ghb_column* build_key
     if (probe_payload[j].n != n)
       return set_error(ctx, GHB_ERR_INVALID, "probe payload %d row count differs from the key", j);
   if (n >= (int64_t)INT32_MAX) return set_error(ctx, GHB_ERR_UNSUPPORTED, "probe of 2^31 rows or more");
-  int32_t st;
-  for (int i = 0; i < 3; i++)
-    if (!ctx->hstream[i]) GHB_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->hstream[i], cudaStreamNonBlocking));
-  for (auto& row : ctx->hev)
-    for (cudaEvent_t& e : row)
-      if (!e) GHB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  int32_t st = host_streams(ctx);
+  if (st) return st;
   cudaStream_t s_in = ctx->hstream[0], s_k = ctx->hstream[1], s_out = ctx->hstream[2];
   // the calling thread's legacy default stream may hold work on these
   // buffers: start after it
@@ -297,17 +459,9 @@ static int32_t ghb_hash_join_host_body(ghb_ctx* ctx, const ghb_column* build_key
     int64_t* d_rows = nullptr;
   } slot[2];
   int64_t* h_rows = nullptr;   // pinned: each chunk's row count
-  size_t hneed = (size_t)std::max<int64_t>(nchunks, 1) * 8;
-  if (ctx->pinned_bytes < hneed) {
-    if (ctx->pinned) cudaFreeHost(ctx->pinned);
-    ctx->pinned = nullptr;
-    ctx->pinned_bytes = 0;
-    if (cudaMallocHost(&ctx->pinned, std::max<size_t>(hneed, 4096)) != cudaSuccess) {
-      cudaGetLastError();
-      ghb_join_table_free(ctx, t);
-      return set_error(ctx, GHB_ERR_OOM, "cannot allocate pinned host memory");
-    }
-    ctx->pinned_bytes = std::max<size_t>(hneed, 4096);
+  if ((st = ensure_pinned(ctx, (size_t)std::max<int64_t>(nchunks, 1) * 8))) {
+    ghb_join_table_free(ctx, t);
+    return st;
   }
   h_rows = (int64_t*)ctx->pinned;
   auto fail = [&](int32_t code) {

@@ -630,6 +630,12 @@ int32_t ghb_plan_result_free(ghb_plan_result* result);
  * These copy the inputs in, run the operator, copy the result out and
  * synchronise, like one GHive operator call on host `Column`s.  The row
  * count is returned through the host int64 *out_rows. */
+/* With every host buffer pinned (or registered) and two chunks of rows or
+ * more (about n/12 rows each, 512Ki to 8Mi), the filter runs in chunks whose
+ * copies in and out overlap each other and the kernels; the output is the
+ * same.  An output capacity below the row count returns GHB_ERR_CAPACITY
+ * with the full count in *out_rows (the first out_capacity rows may have
+ * been written). */
 int32_t ghb_filter_host(ghb_ctx* ctx, const ghb_predicate* pred,
                         const ghb_column* cols, int32_t ncols,
                         const int32_t* proj, int32_t nproj,

@@ -493,6 +493,58 @@ def test_host_entry_points_match_device(ctx):
     assert np.array_equal(opp[0][0], rowid[perm]) and np.array_equal(okk[1][0], k2[perm])
 
 
+def _pin(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+
+def _pinned_outs(types, cap):
+    import torch
+    from ghive_b200.ops import _Outs
+    o = _Outs(types, cap, None)
+    keep = []
+    for j, t in enumerate(types):
+        buf = torch.from_numpy(np.empty(max(1, cap), dtype=abi.NP_DTYPE[t])).pin_memory()
+        nb = torch.empty(max(1, cap), dtype=torch.uint8).pin_memory()
+        o.cols[j] = (buf.numpy(), nb.numpy())
+        o.arr[j].data, o.arr[j].is_null = buf.data_ptr(), nb.data_ptr()
+        keep += [buf, nb]
+    o._pinned = keep
+    return o
+
+
+def test_filter_host_pinned_chunks(ctx):
+    """Pinned host columns of 3.3M rows take the chunked host path (chunks
+    copied in, filtered and copied out on three streams): the same rows in
+    the same order as the oracle, a BYTEMAP input's NULLs carried, an
+    output capacity below the row count refused with the full count, and
+    pageable columns (one copy in, one out) giving the same rows."""
+    from ghive_b200._lib import GhbError
+    g = np.random.default_rng(43)
+    n = 3_300_001
+    a = g.integers(0, 2526, n, dtype=np.int32)
+    b = g.integers(-(1 << 40), 1 << 40, n, dtype=np.int64)
+    bnull = g.random(n) < 0.1
+    c = g.random(n)
+    pred = abi.Pred.or_(abi.Pred.leaf(abi.FILTER_LT, 0, a=700), abi.Pred.leaf(abi.FILTER_GT, 2, a=0.9))
+    sel = oracle.filter_rows(pred, [a, (b, bnull), c])
+    types = [abi.INT, abi.LONG, abi.DOUBLE]
+    for cols in ([_pin(a), (_pin(b), _pin(bnull.astype(np.uint8))), _pin(c)], [a, (b, bnull), c]):
+        outs = _pinned_outs(types, n)
+        got, k = ctx.filter_host(pred, cols, outs=outs)
+        assert k == len(sel)
+        assert np.array_equal(got[0][0], a[sel]) and np.array_equal(got[1][0], b[sel])
+        assert np.array_equal(got[2][0].view(np.uint8), c[sel].view(np.uint8))
+        assert np.array_equal(got[1][1], bnull[sel]) and not got[0][1].any()
+    cap = len(sel) // 2
+    with pytest.raises(GhbError) as e:
+        ctx.filter_host(pred, [_pin(a), (_pin(b), _pin(bnull.astype(np.uint8))), _pin(c)], capacity=cap,
+                        outs=_pinned_outs(types, cap))
+    assert e.value.code == abi.ERR_CAPACITY
+    outs, k = ctx.filter_host(pred, [a, (b, bnull), c], proj=[2])
+    assert k == len(sel) and np.array_equal(outs[0][0].view(np.uint8), c[sel].view(np.uint8))
+
+
 @pytest.mark.parametrize("max_groups", [8, 1000])
 def test_groupby_narrow_shared_accumulators(ctx, max_groups):
     """The specialised fold keeps COUNT as u32, integer SUM as a u32 pair with
