@@ -1,7 +1,8 @@
 """GPU parity at the benchmark workloads' own sizes, through the same calls
 the benchmark times.
 
-- filter + GROUP BY over the 6M-row fact table (1000 groups);
+- filter + GROUP BY over the 6M-row fact table (1000 groups), with native
+  widths and with every integer 8 bytes wide (Hive's layout);
 - the inner hash join of 1.5M unique build keys with a 60M-row probe, with
   the benchmark's output set (probe row id, int64 and double build payloads,
   no build row ids): the lean write pass.  Once with the dense surrogate keys
@@ -61,6 +62,22 @@ def test_fact_table_filter_groupby_6M(ctx):
     errs = compare_groupby(host_cols(gk), host_cols(ga), ok, oa, _types(cols, aggs), comp)
     s = error_summary(errs)
     print("fact table 6M: double SUM/AVG error vs compensated sum", s)
+    assert s["results"] == 2000 and s["max_rel"] <= REL_TOL
+
+
+def test_fact_table_hive_layout_6M(ctx):
+    """The same query with every integer column 8 bytes wide, as Hive's
+    LongColumnVector holds them (k and d widened to int64): LONG keys and
+    LONG MIN/MAX."""
+    k, qty, price, d = workloads.fact_table(6_000_000, seed_idx=0)
+    cols = [k.astype(np.int64), qty, price, d.astype(np.int64)]
+    pred, aggs = workloads.fact_predicate(), workloads.AGGS_FACT
+    ok, oa, comp = oracle.filter_groupby(pred, cols, [0], aggs, cap=1000, with_comp=True)
+    gk, ga, g = ctx.filter_groupby(pred, [dev(c) for c in cols], [0], aggs, capacity=1000,
+                                   max_groups=1000)
+    assert g == 1000
+    errs = compare_groupby(host_cols(gk), host_cols(ga), ok, oa, _types(cols, aggs), comp)
+    s = error_summary(errs)
     assert s["results"] == 2000 and s["max_rel"] <= REL_TOL
 
 
