@@ -416,8 +416,10 @@ __device__ __forceinline__ void decode_value(const PassParams& p, uint64_t v, in
   }
 }
 
+// Three CTAs per SM: the registers are held to 80 (a few bytes spill), and
+// three CTAs' shared memory fits an SM.
 template <typename V, int SRC, int DST>
-__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(PassParams p) {
+__global__ void __launch_bounds__(kSortThreads, 3) sort_pass_kernel(PassParams p) {
   __shared__ uint32_t s_whist[kSortThreads / 32][kBins];  // per-warp counts, then exclusive over warps
   __shared__ uint32_t s_bexcl[kBins];                      // block-local exclusive offset per digit
   __shared__ uint64_t s_gbase[kBins];                      // global destination of each digit's run
