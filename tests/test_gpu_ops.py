@@ -130,6 +130,34 @@ def test_filter_ghive_golden_rows(ctx):
     assert rows == [tuple(r) for r in case["expected_rows"]]
 
 
+def test_filter_ranges_of_several_tiles(ctx):
+    """5M rows: each CTA claims a range of several 2048-row tiles (one
+    look-back per range), the last range and tile partial.  A one-leaf
+    predicate (values loaded before the compares), a tree over a NULL-mapped
+    column, and a capacity that runs out inside a range: the rows below it
+    are written, the error carries the full count."""
+    from ghive_b200._lib import GhbError
+    g = np.random.default_rng(8)
+    n = 5_000_003
+    a = g.integers(0, 2526, n, dtype=np.int32)
+    b = g.integers(-(1 << 40), 1 << 40, n, dtype=np.int64)
+    bnull = g.random(n) < 0.1
+    c = g.random(n)
+    _check_filter(ctx, abi.Pred.leaf(abi.FILTER_LT, 0, a=1263), [a, (b, bnull), c])
+    tree = abi.Pred.and_(abi.Pred.leaf(abi.FILTER_GE, 1, a=0),
+                         abi.Pred.or_(abi.Pred.leaf(abi.FILTER_LT, 2, a=0.3), abi.Pred.leaf(abi.FILTER_EQ, 0, a=7)))
+    _check_filter(ctx, tree, [a, (b, bnull), c])
+    sel = oracle.filter_rows(tree, [a, (b, bnull), c])
+    cap = len(sel) // 3
+    from ghive_b200.ops import _Outs
+    outs = _Outs([abi.INT, abi.LONG, abi.DOUBLE], cap, "cuda:0")
+    with pytest.raises(GhbError) as e:
+        ctx.filter(tree, [dev(a), (dev(b), dev(bnull.astype(np.uint8))), dev(c)], capacity=cap, outs=outs)
+    assert e.value.code == abi.ERR_CAPACITY
+    got = outs.rows(cap)
+    assert np.array_equal(host(got[0][0]), a[sel[:cap]]) and np.array_equal(host(got[1][0]), b[sel[:cap]])
+
+
 def test_filter_capacity_error_reports_required_rows(ctx):
     from ghive_b200._lib import GhbError
     n = 10_000
