@@ -1054,6 +1054,9 @@ def run_profile_case(case, reps):
       filter   filter d < 1263 over the 6M-row fact table, four columns out
       groupby  filter d < 1263 + GROUP BY k over the 6M-row fact table
       gbcnt    the same table, COUNT(*) only
+      gbrows   GROUP BY k over 1 and then 6M rows of that table: COUNT(*) with
+               no predicate, then the filter and the fact aggregates (the
+               cost of a call against its rows)
       join     1.5M-key build, 20M-row probe, int64 + double build payloads
       joinhash the same with the keys spread over the int64 range (hashed table)
       sort     ORDER BY (d int32, k int64) with an int32 row id, 20M rows
@@ -1087,6 +1090,14 @@ def run_profile_case(case, reps):
         for _ in range(reps):
             _, _, g = ctx.filter_groupby(workloads.fact_predicate(), cols, [0], aggs, capacity=1000,
                                          max_groups=1000)
+        print("groups", g)
+    elif case == "gbrows":
+        big = [torch.from_numpy(c).to(dev) for c in workloads.fact_table(N_FACT, seed_idx=0)]
+        for n in (1, N_FACT):
+            cols = [c[:n] for c in big]
+            for pred, aggs in ((None, [(abi.CNT, -1)]), (workloads.fact_predicate(), workloads.AGGS_FACT)):
+                for _ in range(reps):
+                    _, _, g = ctx.filter_groupby(pred, cols, [0], aggs, capacity=1000, max_groups=1000)
         print("groups", g)
     elif case == "sort":
         d, k, r = workloads.sort_table(20_000_000, seed_idx=2)
